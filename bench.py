@@ -1,0 +1,309 @@
+"""Benchmark of the B200 ensemble forecast step: member-steps/s at 256^2, FP32.
+
+Workload (one "step" = one RK4 time step of every member): 2048 members per GPU at N=256,
+complex64 compact spectra, nu=2.5e-4, dt=2.5e-4, Kolmogorov forcing 0.1 sin(4y) and
+Euler-Maruyama noise sigma=0.05 on 1<=|k|<=4 (Philox, in-kernel), seeded Gaussian-random-field
+initial vorticity (unit enstrophy).  The ensemble state plus stage buffers (~2.5 GB) is far
+larger than L2 (126 MB), so every step streams from HBM.
+
+Legs:
+  value        device-resident throughput (CUDA events on the library's stream, max over ranks)
+  e2e          the same step through the C ABI with the whole ensemble state copied
+               host->device (pinned) before and device->host after every step
+  roofline     dominant kernel: algorithmic bytes per launch / mean launch duration
+  cpu_baseline the reference's own CPU solver (oracle/_ref, hzl::ensemble on all host
+               threads) on a bounded sample of the same grid size
+
+`--impl reference` times only the reference CPU path (rank 0; other ranks exit 0).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N = 256
+MEMBERS = 2048
+NU = 2.5e-4
+DT = 2.5e-4
+SIGMA = 0.05
+SEED = 42
+METRIC = "ensemble member-steps/s at 256^2"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference_sample(n: int, seconds_target: float = 15.0):
+    """Times the reference's own CPU path (hzl::ensemble: Solver::step per member on
+    std::jthread workers, src/inference.cpp:555-590) on all host threads; bounded sample."""
+    from oracle.oracle import Reference, host_cores, params6
+    ref = Reference()
+    threads = host_cores()
+    p = params6(NU, 0.1, 0.2, 0.5, 2, 3)   # reference physics (OU forcing); same FFT cost
+    # calibrate with one member-step per thread, then size the sample to ~seconds_target
+    t0 = time.perf_counter()
+    ref.ensemble(n, p, DT, 1, threads, threads, SEED)
+    one = time.perf_counter() - t0
+    steps = max(1, int(seconds_target / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    ref.ensemble(n, p, DT, steps, threads, threads, SEED)
+    el = time.perf_counter() - t0
+    value = threads * steps / el
+    sample = (f"hzl::ensemble (reference CPU build, -O2) at {n}^2: {threads} members x {steps} "
+              f"steps on {threads} threads, {el:.1f} s, includes the reference's per-step "
+              f"validate_step diagnostics")
+    return value, threads, sample
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    value, threads, sample = cpu_reference_sample(N, seconds_target=max(5.0, 3.0 * args.steps))
+    out = {
+        "metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * threads / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{N}^2 ensemble step, reference CPU solver", "n": N},
+        "cpu_baseline": {"value": value, "unit": "member-steps/s", "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "member-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--members", type=int, default=MEMBERS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import hzl_stochasticflowinference_b200 as hz
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    M = args.members
+    cfg = hz.Config(n=N, members=M, precision=4, nu=NU, alpha=0.0, forcing_kmax=0,
+                    noise_sigma=SIGMA, noise_kmax=4, seed=SEED, member_base=rank * M, device=local)
+    ens = hz.Ensemble(cfg)
+    # seeded initial fields (host FP64 generator, compact layout)
+    init = np.zeros((M, ens.compact_size), np.complex64)
+    for m in range(M):
+        init[m] = hz.full_to_compact(hz.grf_spectrum(N, SEED, rank * M + m), N)[0]
+    ens.set_state_compact(init)
+    ens.set_forcing(hz.kolmogorov_forcing(N)[None])
+    ens.set_time(0.0, 0)
+    stream = torch.cuda.ExternalStream(ens.stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if not pg:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- value: device-resident steps ---------------------------------------------
+    for _ in range(args.warmup):
+        ens.step(DT, 1)
+    ens.synchronize()
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            ens.step(DT, 1)
+        stop.record(stream)
+        ens.synchronize()
+        barrier()
+    ms = start.elapsed_time(stop)
+    ms = max_over_ranks(ms)
+    status = ens.status()
+    value = world * M * args.steps / (ms / 1e3)
+    ms_per_step = ms / args.steps
+
+    # ---- roofline: per-launch events on the library stream -----------------------
+    row_ms, col_ms = ens.step_profiled(DT, max(2, args.steps // 4))
+    K = (N - 1) // 3
+    C, LD = K + 1, 2 * K + 1
+    cb = 8  # complex64 bytes
+    row_bytes = M * (4 * C * N + C * N) * cb                 # read W (4 fields), write NL
+    col_bytes = M * (C * N + 4 * C * N + 5 * C * LD) * cb    # read NL, write W, state r/w
+    row_gbs = row_bytes / (row_ms * 1e-3) / 1e9
+    col_gbs = col_bytes / (col_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    dom = ("column_kernel", col_gbs, col_bytes, col_ms) if col_ms >= row_ms else \
+        ("row_kernel", row_gbs, row_bytes, row_ms)
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        tj = json.loads(tf.read_text())
+        if dom[0] in tj:
+            traffic = tj[dom[0]]["bytes_per_member"] * M
+
+    # ---- e2e: host state in/out around every step ---------------------------------
+    state_bytes = M * ens.compact_size * cb
+    host_in = torch.from_numpy(ens.get_state_compact().view(np.float32)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        ens.set_state_compact_ptr(host_in.data_ptr(), 0, M)
+        ens.step(DT, 1)
+        ens.get_state_compact_ptr(host_out.data_ptr(), 0, M)
+    barrier()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(e2e_steps):
+        ens.set_state_compact_ptr(host_in.data_ptr(), 0, M)
+        ens.step(DT, 1)
+        ens.get_state_compact_ptr(host_out.data_ptr(), 0, M)
+    t1.record(stream)
+    ens.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1))
+    e2e_value = world * M * e2e_steps / (e2e_ms / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            v, cores, sample = cpu_reference_sample(N)
+            cpu = {"value": v, "unit": "member-steps/s", "cores": cores, "kind": "reference",
+                   "sample": sample}
+        except Exception as exc:   # the reference library is test infrastructure; report why
+            cpu = {"value": None, "unit": "member-steps/s", "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"{N}^2 FP32 ensemble RK4 step, {M} members per GPU "
+                                   "(Kolmogorov forcing + Philox EM noise, GRF initial fields)",
+                       "n": N, "members_per_gpu": M, "nu": NU, "dt": DT,
+                       "l2": "inputs larger than L2 (state + stage buffers ~2.5 GB per GPU)",
+                       "parallelism": f"member shards x{world}"},
+            "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": dom[1], "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": dom[1] / peak,
+                         "traffic": traffic, "algorithmic_bytes": dom[2],
+                         "launch_ms": dom[3],
+                         "row_kernel": {"ms": row_ms, "gbs": row_gbs},
+                         "column_kernel": {"ms": col_ms, "gbs": col_gbs}},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "member-steps/s",
+                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
+            "gpu_launches": 8 * args.steps,
+            "clocks": clocks.summary(),
+            "status": status,
+        }
+        print(json.dumps(out), flush=True)
+    ens.close()
+    if pg:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,366 @@
+"""B200 ensemble forecast/analysis path for pvasbob/HZL-stochasticFlowInference.
+
+Python mirror of the reference's interface for this path, over the C ABI of
+``include/hzlb.h`` (``libhzlb.so``, built in-tree by ``build.py``).  There is no CPU
+fallback: importing this package without the built library, or creating an ensemble without
+a CUDA device, raises.
+
+Reference correspondences (paths relative to the reference repository):
+
+* :class:`Ensemble` -- M resident ``hzl::CudaSolver`` instances advanced together
+  (include/hzl/cuda_solver.hpp:7-22, src/cuda_solver.cu); state I/O in the reference's
+  full-complex layout (include/hzl/fft.hpp:7-9).
+* :meth:`Ensemble.diagnostics` -- ``Solver::diagnostics`` per member (src/solver.cpp:381-397).
+* :meth:`Ensemble.observe` -- ``Solver::physical_vorticity`` sampled at sensors
+  (src/solver.cpp:398-402).
+* :meth:`Ensemble.pf_loglik`, :func:`pf_weights`, :func:`systematic_resample`,
+  :meth:`Ensemble.gather` -- the weight and resample steps of ``bootstrap_filter``
+  (src/filter.cpp:66-120).
+* :meth:`Ensemble.inflate`, :meth:`Ensemble.enkf_analysis` -- the analysis of
+  ``ensemble_kalman_filter`` (src/filter.cpp:237-321) in batched form.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libhzlb.so"
+
+HZLB_OK, HZLB_EINVAL, HZLB_ERUNTIME, HZLB_ECUDA, HZLB_ETIMEOUT = 0, -1, -2, -3, -4
+STATUS_CFL, STATUS_NONFINITE, STATUS_TIMEOUT = 1, 2, 4
+
+_dp = C.POINTER(C.c_double)
+_u32p = C.POINTER(C.c_uint32)
+
+
+class hzlb_config(C.Structure):
+    _fields_ = [
+        ("n", C.c_int), ("members", C.c_int), ("precision", C.c_int),
+        ("nu", C.c_double), ("alpha", C.c_double),
+        ("forcing_kmax", C.c_int), ("forcing_per_member", C.c_int),
+        ("noise_sigma", C.c_double), ("noise_kmax", C.c_int),
+        ("seed", C.c_uint64), ("member_base", C.c_uint32), ("device", C.c_int),
+    ]
+
+
+class HzlbError(RuntimeError):
+    """A failure reported through the C ABI (std::runtime_error in the reference)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+class HzlbInvalidArgument(HzlbError, ValueError):
+    """HZLB_EINVAL (std::invalid_argument in the reference)."""
+
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    """Loads libhzlb.so; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: run `python {PKG / 'build.py'}` "
+                          "(nvcc, sm_100a) before using the B200 path")
+    lib = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    sig = {
+        "hzlb_last_error": (C.c_char_p, []),
+        "hzlb_version": (C.c_char_p, []),
+        "hzlb_ensemble_create": (C.c_int, [C.POINTER(hzlb_config), C.POINTER(vp)]),
+        "hzlb_ensemble_destroy": (None, [vp]),
+        "hzlb_set_state": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
+        "hzlb_get_state": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
+        "hzlb_set_state_compact": (C.c_int, [vp, vp, C.c_int, C.c_int]),
+        "hzlb_get_state_compact": (C.c_int, [vp, vp, C.c_int, C.c_int]),
+        "hzlb_compact_size": (C.c_size_t, [vp]),
+        "hzlb_set_forcing": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
+        "hzlb_step": (C.c_int, [vp, C.c_double, C.c_uint64]),
+        "hzlb_status": (C.c_int, [vp, _u32p]),
+        "hzlb_synchronize": (C.c_int, [vp]),
+        "hzlb_stream": (C.c_void_p, [vp]),
+        "hzlb_step_profiled": (C.c_int, [vp, C.c_double, C.c_uint64, _dp, _dp]),
+        "hzlb_time": (C.c_int, [vp, _dp, C.POINTER(C.c_uint64)]),
+        "hzlb_set_time": (C.c_int, [vp, C.c_double, C.c_uint64]),
+        "hzlb_diagnostics": (C.c_int, [vp, _dp]),
+        "hzlb_physical": (C.c_int, [vp, _dp]),
+        "hzlb_observe": (C.c_int, [vp, _u32p, _u32p, C.c_size_t, _dp]),
+        "hzlb_pf_loglik": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp]),
+        "hzlb_pf_weights": (C.c_int, [_dp, C.c_size_t, _dp, _dp, _dp, _dp]),
+        "hzlb_systematic_resample": (C.c_int, [vp, _dp, C.c_size_t, C.c_double, _u32p]),
+        "hzlb_gather_members": (C.c_int, [vp, _u32p]),
+        "hzlb_inflate": (C.c_int, [vp, C.c_double]),
+        "hzlb_enkf_analysis": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp]),
+        "hzlb_grf_spectrum": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, _dp]),
+        "hzlb_kolmogorov_forcing": (C.c_int, [C.c_int, C.c_double, C.c_int, _dp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != HZLB_OK:
+        msg = library().hzlb_last_error().decode()
+        if rc == HZLB_EINVAL:
+            raise HzlbInvalidArgument(rc, msg)
+        raise HzlbError(rc, msg)
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _c128(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _pu(a: np.ndarray):
+    return a.ctypes.data_as(_u32p)
+
+
+def retained_k(n: int) -> int:
+    """Largest retained |k| under the strict 2/3 rule 3|k| < n (src/solver.cpp:133-134)."""
+    return (n - 1) // 3
+
+
+@dataclass
+class Config:
+    n: int
+    members: int
+    precision: int = 4            # 4: FP32 spectra, 8: FP64 spectra
+    nu: float = 1e-3
+    alpha: float = 0.0
+    forcing_kmax: int = -1        # forcing columns kx <= forcing_kmax; -1: none
+    forcing_per_member: bool = False
+    noise_sigma: float = 0.0
+    noise_kmax: int = 4
+    seed: int = 42
+    member_base: int = 0
+    device: int = 0
+
+    def to_c(self) -> hzlb_config:
+        return hzlb_config(self.n, self.members, self.precision, self.nu, self.alpha,
+                           self.forcing_kmax, int(self.forcing_per_member), self.noise_sigma,
+                           self.noise_kmax, self.seed, self.member_base, self.device)
+
+
+class Ensemble:
+    """M members of the periodic 2-D vorticity model advanced together on one B200."""
+
+    def __init__(self, config: Config):
+        self.config = config
+        self.n, self.members = config.n, config.members
+        self._lib = library()
+        self._h = C.c_void_p()
+        cfg = config.to_c()
+        _check(self._lib.hzlb_ensemble_create(C.byref(cfg), C.byref(self._h)))
+        self.compact_size = int(self._lib.hzlb_compact_size(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hzlb_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state ------------------------------------------------------------------------
+    def set_state(self, spectra: np.ndarray, first: int = 0):
+        """spectra: (count, n, n) complex128 in the reference layout [y, x]."""
+        s = _c128(spectra).reshape(-1, self.n, self.n)
+        _check(self._lib.hzlb_set_state(self._h, s.view(np.float64).ctypes.data_as(_dp), first,
+                                        len(s)))
+
+    def get_state(self, first: int = 0, count: int | None = None) -> np.ndarray:
+        count = self.members - first if count is None else count
+        out = np.zeros((count, self.n, self.n), np.complex128)
+        _check(self._lib.hzlb_get_state(self._h, out.view(np.float64).ctypes.data_as(_dp), first,
+                                        count))
+        return out
+
+    @property
+    def compact_dtype(self):
+        return np.complex64 if self.config.precision == 4 else np.complex128
+
+    def set_state_compact(self, compact: np.ndarray, first: int = 0):
+        a = np.ascontiguousarray(compact, dtype=self.compact_dtype).reshape(-1, self.compact_size)
+        _check(self._lib.hzlb_set_state_compact(self._h, a.ctypes.data_as(C.c_void_p), first,
+                                                len(a)))
+        self._keep = a   # the copy is asynchronous; keep the source alive until the next call
+
+    def get_state_compact(self, first: int = 0, count: int | None = None) -> np.ndarray:
+        count = self.members - first if count is None else count
+        out = np.zeros((count, self.compact_size), self.compact_dtype)
+        _check(self._lib.hzlb_get_state_compact(self._h, out.ctypes.data_as(C.c_void_p), first,
+                                                count))
+        return out
+
+    def set_state_compact_ptr(self, ptr: int, first: int, count: int):
+        """Bulk upload from a raw (device or pinned host) pointer in the compact layout."""
+        _check(self._lib.hzlb_set_state_compact(self._h, C.c_void_p(ptr), first, count))
+
+    def get_state_compact_ptr(self, ptr: int, first: int, count: int):
+        _check(self._lib.hzlb_get_state_compact(self._h, C.c_void_p(ptr), first, count))
+
+    def set_forcing(self, spectra: np.ndarray, first: int = 0):
+        s = _c128(spectra).reshape(-1, self.n, self.n)
+        _check(self._lib.hzlb_set_forcing(self._h, s.view(np.float64).ctypes.data_as(_dp), first,
+                                          len(s)))
+
+    # -- stepping ---------------------------------------------------------------------
+    def step(self, dt: float, steps: int = 1):
+        _check(self._lib.hzlb_step(self._h, dt, steps))
+
+    def step_profiled(self, dt: float, steps: int):
+        """Steps with per-launch CUDA events; returns mean (row_ms, column_ms) per launch."""
+        r, c = C.c_double(), C.c_double()
+        _check(self._lib.hzlb_step_profiled(self._h, dt, steps, C.byref(r), C.byref(c)))
+        return r.value, c.value
+
+    @property
+    def stream(self) -> int:
+        """The handle's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self._lib.hzlb_stream(self._h) or 0)
+
+    def status(self) -> int:
+        s = C.c_uint32()
+        _check(self._lib.hzlb_status(self._h, C.byref(s)))
+        return s.value
+
+    def synchronize(self):
+        _check(self._lib.hzlb_synchronize(self._h))
+
+    def time(self):
+        t, s = C.c_double(), C.c_uint64()
+        _check(self._lib.hzlb_time(self._h, C.byref(t), C.byref(s)))
+        return t.value, s.value
+
+    def set_time(self, time: float, step_index: int):
+        _check(self._lib.hzlb_set_time(self._h, time, step_index))
+
+    # -- diagnostics / observation --------------------------------------------------
+    def diagnostics(self) -> np.ndarray:
+        """(members, 6): time, energy, enstrophy, dissipation, injection, cfl_rate."""
+        out = np.zeros((self.members, 6))
+        _check(self._lib.hzlb_diagnostics(self._h, _p(out)))
+        return out
+
+    def physical(self) -> np.ndarray:
+        out = np.zeros((self.members, self.n, self.n))
+        _check(self._lib.hzlb_physical(self._h, _p(out)))
+        return out
+
+    def observe(self, x, y) -> np.ndarray:
+        x, y = _u32(x), _u32(y)
+        out = np.zeros((self.members, len(x)))
+        _check(self._lib.hzlb_observe(self._h, _pu(x), _pu(y), len(x), _p(out)))
+        return out
+
+    # -- particle filter -------------------------------------------------------------
+    def pf_loglik(self, x, y, values, sd, log_weights) -> np.ndarray:
+        x, y, v, s = _u32(x), _u32(y), _f64(values), _f64(sd)
+        lw = _f64(log_weights).copy()
+        _check(self._lib.hzlb_pf_loglik(self._h, _pu(x), _pu(y), _p(v), _p(s), len(x), _p(lw)))
+        return lw
+
+    def resample(self, weights, u: float) -> np.ndarray:
+        w = _f64(weights)
+        out = np.zeros(len(w), np.uint32)
+        _check(self._lib.hzlb_systematic_resample(self._h, _p(w), len(w), u, _pu(out)))
+        return out
+
+    def gather(self, ancestors):
+        a = _u32(ancestors)
+        _check(self._lib.hzlb_gather_members(self._h, _pu(a)))
+
+    # -- EnKF -------------------------------------------------------------------------
+    def inflate(self, inflation: float):
+        _check(self._lib.hzlb_inflate(self._h, inflation))
+
+    def enkf_analysis(self, x, y, values, sd, perturbations):
+        x, y, v, s = _u32(x), _u32(y), _f64(values), _f64(sd)
+        e = _f64(perturbations).reshape(self.members, len(x))
+        _check(self._lib.hzlb_enkf_analysis(self._h, _pu(x), _pu(y), _p(v), _p(s), len(x),
+                                            _p(e)))
+
+
+def pf_weights(log_weights):
+    """(weights, increment, ess, max_weight) as in filter.cpp:76-92."""
+    lw = _f64(log_weights)
+    w = np.zeros_like(lw)
+    inc, ess, mw = C.c_double(), C.c_double(), C.c_double()
+    _check(library().hzlb_pf_weights(_p(lw), len(lw), _p(w), C.byref(inc), C.byref(ess),
+                                     C.byref(mw)))
+    return w, inc.value, ess.value, mw.value
+
+
+def systematic_resample(weights, u: float) -> np.ndarray:
+    """Host systematic resampling (filter.cpp:102-112); see Ensemble.resample for the device."""
+    w = _f64(weights)
+    out = np.zeros(len(w), np.uint32)
+    _check(library().hzlb_systematic_resample(None, _p(w), len(w), u, _pu(out)))
+    return out
+
+
+def grf_spectrum(n: int, seed: int, member: int) -> np.ndarray:
+    out = np.zeros((n, n), np.complex128)
+    _check(library().hzlb_grf_spectrum(n, seed, member, out.view(np.float64).ctypes.data_as(_dp)))
+    return out
+
+
+def kolmogorov_forcing(n: int, amplitude: float = 0.1, wavenumber: int = 4) -> np.ndarray:
+    out = np.zeros((n, n), np.complex128)
+    _check(library().hzlb_kolmogorov_forcing(n, amplitude, wavenumber,
+                                             out.view(np.float64).ctypes.data_as(_dp)))
+    return out
+
+
+def compact_to_full(compact: np.ndarray, n: int) -> np.ndarray:
+    """Compact half-spectrum layout -> reference full-complex layout (Hermitian fill)."""
+    k = retained_k(n)
+    ld = 2 * k + 1
+    c = np.asarray(compact).reshape(-1, k + 1, ld).astype(np.complex128)
+    j = np.arange(ld)
+    ypos = np.where(j <= k, j, n - ld + j)
+    full = np.zeros((len(c), n, n), np.complex128)
+    full[:, ypos[:, None], np.arange(k + 1)[None, :]] = c.transpose(0, 2, 1)
+    kx = np.arange(1, k + 1)
+    full[:, ((n - ypos) % n)[:, None], (n - kx)[None, :]] = np.conj(c[:, 1:, :]).transpose(0, 2, 1)
+    return full
+
+
+def full_to_compact(full: np.ndarray, n: int) -> np.ndarray:
+    k = retained_k(n)
+    ld = 2 * k + 1
+    j = np.arange(ld)
+    ypos = np.where(j <= k, j, n - ld + j)
+    f = np.asarray(full).reshape(-1, n, n)
+    out = f[:, ypos][:, :, : k + 1].transpose(0, 2, 1).copy()
+    out[:, 0, 0] = 0
+    return out.reshape(len(f), -1)

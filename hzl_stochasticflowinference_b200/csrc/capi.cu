@@ -1,0 +1,230 @@
+// extern "C" boundary (include/hzlb.h): exception -> status code mapping around the engine.
+#include "engine.h"
+
+#include <cmath>
+#include <exception>
+#include <string>
+#include <vector>
+
+struct hzlb_ensemble {
+    std::unique_ptr<hzlb::Engine> engine;
+};
+
+namespace {
+thread_local std::string last_error;
+
+template <class F> int guarded(F &&f) {
+    try {
+        f();
+        return HZLB_OK;
+    } catch (const hzlb::Error &e) {
+        last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        last_error = "host allocation failed";
+        return HZLB_ERUNTIME;
+    } catch (const std::exception &e) {
+        last_error = e.what();
+        return HZLB_ERUNTIME;
+    } catch (...) {
+        last_error = "unknown failure";
+        return HZLB_ERUNTIME;
+    }
+}
+hzlb::Engine &engine(hzlb_ensemble *h) {
+    if (!h || !h->engine)
+        hzlb::raise(HZLB_EINVAL, "null ensemble handle");
+    return *h->engine;
+}
+void need(const void *p, const char *what) {
+    if (!p)
+        hzlb::raise(HZLB_EINVAL, std::string("null pointer: ") + what);
+}
+} // namespace
+
+extern "C" {
+
+const char *hzlb_last_error(void) { return last_error.c_str(); }
+const char *hzlb_version(void) { return "hzlb 0.1 (sm_100a)"; }
+
+int hzlb_ensemble_create(const hzlb_config *config, hzlb_ensemble **out) {
+    return guarded([&] {
+        need(config, "config");
+        need(out, "out");
+        *out = nullptr;
+        auto h = std::make_unique<hzlb_ensemble>();
+        h->engine = hzlb::make_engine(*config);
+        *out = h.release();
+    });
+}
+void hzlb_ensemble_destroy(hzlb_ensemble *h) { delete h; }
+
+int hzlb_set_state(hzlb_ensemble *h, const double *spectra, int first, int count) {
+    return guarded([&] {
+        need(spectra, "spectra");
+        engine(h).set_state(spectra, first, count);
+    });
+}
+int hzlb_get_state(hzlb_ensemble *h, double *spectra, int first, int count) {
+    return guarded([&] {
+        need(spectra, "spectra");
+        engine(h).get_state(spectra, first, count);
+    });
+}
+int hzlb_set_state_compact(hzlb_ensemble *h, const void *compact, int first, int count) {
+    return guarded([&] {
+        need(compact, "compact");
+        engine(h).set_state_compact(compact, first, count);
+    });
+}
+int hzlb_get_state_compact(hzlb_ensemble *h, void *compact, int first, int count) {
+    return guarded([&] {
+        need(compact, "compact");
+        engine(h).get_state_compact(compact, first, count);
+    });
+}
+size_t hzlb_compact_size(const hzlb_ensemble *h) {
+    return h && h->engine ? h->engine->compact_size() : 0;
+}
+int hzlb_set_forcing(hzlb_ensemble *h, const double *spectra, int first, int count) {
+    return guarded([&] {
+        need(spectra, "spectra");
+        engine(h).set_forcing(spectra, first, count);
+    });
+}
+int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps) {
+    return guarded([&] { engine(h).step(dt, nsteps); });
+}
+void *hzlb_stream(hzlb_ensemble *h) { return h && h->engine ? h->engine->stream() : nullptr; }
+int hzlb_step_profiled(hzlb_ensemble *h, double dt, uint64_t nsteps, double *row_ms,
+                       double *column_ms) {
+    return guarded([&] {
+        need(row_ms, "row_ms");
+        need(column_ms, "column_ms");
+        engine(h).step_profiled(dt, nsteps, row_ms, column_ms);
+    });
+}
+int hzlb_status(hzlb_ensemble *h, uint32_t *status) {
+    return guarded([&] {
+        need(status, "status");
+        *status = engine(h).status();
+    });
+}
+int hzlb_synchronize(hzlb_ensemble *h) {
+    return guarded([&] { engine(h).synchronize(); });
+}
+int hzlb_time(hzlb_ensemble *h, double *time, uint64_t *step_index) {
+    return guarded([&] {
+        auto &e = engine(h);
+        if (time)
+            *time = e.time;
+        if (step_index)
+            *step_index = e.step_index;
+    });
+}
+int hzlb_set_time(hzlb_ensemble *h, double time, uint64_t step_index) {
+    return guarded([&] {
+        if (!std::isfinite(time) || time < 0)
+            hzlb::raise(HZLB_EINVAL, "invalid time");
+        engine(h).set_time(time, step_index);
+    });
+}
+int hzlb_diagnostics(hzlb_ensemble *h, double *out) {
+    return guarded([&] {
+        need(out, "out");
+        engine(h).diagnostics(out);
+    });
+}
+int hzlb_physical(hzlb_ensemble *h, double *out) {
+    return guarded([&] {
+        need(out, "out");
+        engine(h).physical(out);
+    });
+}
+int hzlb_observe(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, size_t p, double *out) {
+    return guarded([&] {
+        if (p) {
+            need(x, "x");
+            need(y, "y");
+            need(out, "out");
+        }
+        engine(h).observe(x, y, p, out);
+    });
+}
+
+int hzlb_pf_loglik(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, const double *values,
+                   const double *sd, size_t p, double *log_weights) {
+    return guarded([&] {
+        need(log_weights, "log_weights");
+        if (p == 0)
+            return;
+        need(values, "values");
+        need(sd, "sd");
+        auto &e = engine(h);
+        const size_t members = static_cast<size_t>(e.members());
+        std::vector<double> field(members * p);
+        e.observe(x, y, p, field.data());
+        // filter.cpp:66-74, member by member in the reference's order of operations
+        const double log_two_pi = std::log(2 * 3.141592653589793238462643383279502884);
+        for (size_t m = 0; m < members; ++m) {
+            double value = log_weights[m];
+            for (size_t o = 0; o < p; ++o) {
+                const double residual = (field[m * p + o] - values[o]) / sd[o];
+                value -= 0.5 * residual * residual + std::log(sd[o]) + 0.5 * log_two_pi;
+            }
+            log_weights[m] = value;
+        }
+    });
+}
+
+int hzlb_pf_weights(const double *log_weights, size_t count, double *weights, double *increment,
+                    double *ess, double *max_weight) {
+    return guarded([&] {
+        need(log_weights, "log_weights");
+        need(weights, "weights");
+        need(increment, "increment");
+        need(ess, "ess");
+        need(max_weight, "max_weight");
+        hzlb::pf_weights_host(log_weights, count, weights, increment, ess, max_weight);
+    });
+}
+int hzlb_systematic_resample(hzlb_ensemble *h, const double *weights, size_t count, double u,
+                             uint32_t *ancestors) {
+    return guarded([&] {
+        need(weights, "weights");
+        need(ancestors, "ancestors");
+        if (count == 0)
+            hzlb::raise(HZLB_EINVAL, "resampling needs at least one weight");
+        if (!std::isfinite(u) || u < 0 || u >= 1)
+            hzlb::raise(HZLB_EINVAL, "resampling uniform must lie in [0, 1)");
+        if (h)
+            engine(h).resample(weights, count, u, ancestors);
+        else
+            hzlb::systematic_resample_host(weights, count, u, ancestors);
+    });
+}
+int hzlb_gather_members(hzlb_ensemble *h, const uint32_t *ancestors) {
+    return guarded([&] {
+        need(ancestors, "ancestors");
+        engine(h).gather(ancestors);
+    });
+}
+int hzlb_inflate(hzlb_ensemble *h, double inflation) {
+    return guarded([&] { engine(h).inflate(inflation); });
+}
+int hzlb_enkf_analysis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
+                       const double *values, const double *sd, size_t p,
+                       const double *perturbations) {
+    return guarded([&] {
+        if (p) {
+            need(x, "x");
+            need(y, "y");
+            need(values, "values");
+            need(sd, "sd");
+            need(perturbations, "perturbations");
+        }
+        engine(h).enkf(x, y, values, sd, p, perturbations);
+    });
+}
+
+} // extern "C"

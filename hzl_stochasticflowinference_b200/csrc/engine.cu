@@ -1,0 +1,616 @@
+// Ensemble engine: owns the device state of one handle and schedules the kernels.
+#include "engine.h"
+#include "filters.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace hzlb {
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+bool valid_grid(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
+int wave(int i, int n) { return i < n / 2 ? i : i - n; }
+
+template <typename R> class EngineT final : public Engine {
+  public:
+    explicit EngineT(const hzlb_config &c) : cfg_(c) {
+        if (!valid_grid(c.n))
+            raise(HZLB_EINVAL, "grid must be a power of two between 8 and 512");
+        if (c.members < 1)
+            raise(HZLB_EINVAL, "ensemble needs at least one member");
+        if (!std::isfinite(c.nu) || c.nu < 0 || !std::isfinite(c.alpha) || c.alpha < 0)
+            raise(HZLB_EINVAL, "nu and alpha must be finite and nonnegative");
+        if (!std::isfinite(c.noise_sigma) || c.noise_sigma < 0)
+            raise(HZLB_EINVAL, "noise sigma must be finite and nonnegative");
+        n_ = c.n;
+        M_ = c.members;
+        K_ = (n_ - 1) / 3;
+        C_ = K_ + 1;
+        LD_ = 2 * K_ + 1;
+        compact_ = static_cast<size_t>(C_) * LD_;
+        fcols_ = c.forcing_kmax < 0 ? 0 : std::min(c.forcing_kmax + 1, C_);
+        fcount_ = fcols_ == 0 ? 0 : (c.forcing_per_member ? M_ : 1);
+        if (c.noise_sigma > 0 && (c.noise_kmax < 1 || 3 * c.noise_kmax >= n_))
+            raise(HZLB_EINVAL, "noise shell must lie strictly inside the dealiased grid");
+        int devices = 0;
+        cuda_check(cudaGetDeviceCount(&devices), "query CUDA devices");
+        if (c.device < 0 || c.device >= devices)
+            raise(HZLB_EINVAL, "invalid CUDA device ordinal");
+        cuda_check(cudaSetDevice(c.device), "select CUDA device");
+        cuda_check(prepare_kernels<R>(n_), "configure kernels");
+        cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create stream");
+        const size_t cb = sizeof(cx<R>);
+        omega_.ensure(cb * compact_ * M_, "allocate GPU state");
+        ystage_.ensure(cb * compact_ * M_, "allocate GPU stage input");
+        acc_.ensure(cb * compact_ * M_, "allocate GPU RK accumulator");
+        w_.ensure(cb * 4 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU derivative columns");
+        nl_.ensure(cb * C_ * static_cast<size_t>(n_) * M_, "allocate GPU Jacobian rows");
+        if (fcount_)
+            forcing_.ensure(cb * static_cast<size_t>(fcols_) * LD_ * fcount_, "allocate GPU forcing");
+        ctl_.ensure(sizeof(StepControl), "allocate step control");
+        tw_.ensure(cb * n_, "allocate twiddles");
+        cuda_check(cudaMemsetAsync(omega_.ptr, 0, omega_.bytes, stream_), "clear GPU state");
+        if (fcount_)
+            cuda_check(cudaMemsetAsync(forcing_.ptr, 0, forcing_.bytes, stream_), "clear forcing");
+        cuda_check(cudaMemsetAsync(ctl_.ptr, 0, sizeof(StepControl), stream_), "clear control");
+        // W_N^k = exp(-2 pi i k / N), the construction of the reference's roots (fft.cpp:25-27)
+        std::vector<cx<R>> tw(n_);
+        for (int k = 0; k < n_; ++k) {
+            const double theta = -2.0 * kPi * static_cast<double>(k) / static_cast<double>(n_);
+            tw[k] = mk<R>(static_cast<R>(std::cos(theta)), static_cast<R>(std::sin(theta)));
+        }
+        cuda_check(cudaMemcpyAsync(tw_.ptr, tw.data(), cb * n_, cudaMemcpyHostToDevice, stream_),
+                   "upload twiddles");
+        cuda_check(cudaStreamSynchronize(stream_), "initialise ensemble");
+    }
+    ~EngineT() override {
+        drop_graphs();
+        if (stream_)
+            cudaStreamDestroy(stream_);
+    }
+
+    size_t compact_size() const override { return compact_; }
+    int members() const override { return M_; }
+    void *stream() const override { return stream_; }
+
+    // ---- state I/O ----------------------------------------------------------------
+    void check_range(int first, int count) const {
+        if (first < 0 || count < 0 || first + count > M_)
+            raise(HZLB_EINVAL, "member range out of bounds");
+    }
+    void set_state(const double *s, int first, int count) override {
+        check_range(first, count);
+        const size_t nn = static_cast<size_t>(n_) * n_;
+        for (size_t i = 0; i < 2 * nn * count; ++i)
+            if (!std::isfinite(s[i]))
+                raise(HZLB_EINVAL, "nonfinite initial GPU state");
+        staging_.ensure(sizeof(cx<R>) * compact_ * count);
+        cx<R> *out = staging_.as<cx<R>>();
+        for (int m = 0; m < count; ++m)
+            for (int kx = 0; kx < C_; ++kx)
+                for (int j = 0; j < LD_; ++j) {
+                    const int ypos = j <= K_ ? j : n_ - LD_ + j;
+                    const double *z = s + 2 * (m * nn + static_cast<size_t>(ypos) * n_ + kx);
+                    const bool zero_mode = kx == 0 && j == 0;
+                    out[(static_cast<size_t>(m) * C_ + kx) * LD_ + j] =
+                        zero_mode ? mk<R>(0, 0) : mk<R>(static_cast<R>(z[0]), static_cast<R>(z[1]));
+                }
+        cuda_check(cudaMemcpyAsync(omega_.as<cx<R>>() + static_cast<size_t>(first) * compact_, out,
+                                   sizeof(cx<R>) * compact_ * count, cudaMemcpyHostToDevice, stream_),
+                   "initial state upload");
+        cuda_check(cudaStreamSynchronize(stream_), "initial state upload");
+        w_valid_ = false;
+    }
+    void get_state(double *s, int first, int count) override {
+        check_range(first, count);
+        staging_.ensure(sizeof(cx<R>) * compact_ * count);
+        cx<R> *in = staging_.as<cx<R>>();
+        cuda_check(cudaMemcpyAsync(in, omega_.as<cx<R>>() + static_cast<size_t>(first) * compact_,
+                                   sizeof(cx<R>) * compact_ * count, cudaMemcpyDeviceToHost, stream_),
+                   "final state download");
+        cuda_check(cudaStreamSynchronize(stream_), "final state download");
+        const size_t nn = static_cast<size_t>(n_) * n_;
+        std::memset(s, 0, sizeof(double) * 2 * nn * count);
+        for (int m = 0; m < count; ++m)
+            for (int kx = 0; kx < C_; ++kx)
+                for (int j = 0; j < LD_; ++j) {
+                    const cx<R> z = in[(static_cast<size_t>(m) * C_ + kx) * LD_ + j];
+                    const int ypos = j <= K_ ? j : n_ - LD_ + j;
+                    double *d = s + 2 * (m * nn + static_cast<size_t>(ypos) * n_ + kx);
+                    d[0] = z.x;
+                    d[1] = z.y;
+                    if (kx > 0) {   // conjugate partner (-kx, -ky)
+                        double *e = s + 2 * (m * nn + static_cast<size_t>((n_ - ypos) % n_) * n_ +
+                                             (n_ - kx));
+                        e[0] = z.x;
+                        e[1] = -static_cast<double>(z.y);
+                    }
+                }
+        for (size_t i = 0; i < 2 * nn * count; ++i)
+            if (!std::isfinite(s[i]))
+                raise(HZLB_ERUNTIME, "nonfinite GPU result");
+    }
+    void set_state_compact(const void *d, int first, int count) override {
+        check_range(first, count);
+        cuda_check(cudaMemcpyAsync(omega_.as<cx<R>>() + static_cast<size_t>(first) * compact_, d,
+                                   sizeof(cx<R>) * compact_ * count, cudaMemcpyDefault, stream_),
+                   "compact state upload");
+        w_valid_ = false;
+    }
+    void get_state_compact(void *d, int first, int count) override {
+        check_range(first, count);
+        cuda_check(cudaMemcpyAsync(d, omega_.as<cx<R>>() + static_cast<size_t>(first) * compact_,
+                                   sizeof(cx<R>) * compact_ * count, cudaMemcpyDefault, stream_),
+                   "compact state download");
+        cuda_check(cudaStreamSynchronize(stream_), "compact state download");
+    }
+    void set_forcing(const double *s, int first, int count) override {
+        if (fcount_ == 0)
+            raise(HZLB_EINVAL, "ensemble was created without forcing");
+        if (first < 0 || count < 0 || first + count > fcount_)
+            raise(HZLB_EINVAL, "forcing member range out of bounds");
+        const size_t nn = static_cast<size_t>(n_) * n_;
+        const size_t block = static_cast<size_t>(fcols_) * LD_;
+        staging_.ensure(sizeof(cx<R>) * block * count);
+        cx<R> *out = staging_.as<cx<R>>();
+        for (int m = 0; m < count; ++m) {
+            const double *f = s + 2 * m * nn;
+            for (int y = 0; y < n_; ++y)
+                for (int x = 0; x < n_; ++x) {
+                    const size_t i = static_cast<size_t>(y) * n_ + x,
+                                 partner = static_cast<size_t>((n_ - y) % n_) * n_ + (n_ - x) % n_;
+                    const double re = f[2 * i], im = f[2 * i + 1];
+                    if (!std::isfinite(re) || !std::isfinite(im))
+                        raise(HZLB_EINVAL, "nonfinite GPU forcing");
+                    // conjugate symmetry to 1e-12 (cuda_solver.cu:191-194)
+                    const double dr = re - f[2 * partner], di = im + f[2 * partner + 1];
+                    if (std::hypot(dr, di) > 1e-12 * (1 + std::hypot(re, im)))
+                        raise(HZLB_EINVAL, "GPU forcing must preserve conjugate symmetry");
+                    const int kx = wave(x, n_), ky = wave(y, n_);
+                    const bool retained = 3 * std::abs(kx) < n_ && 3 * std::abs(ky) < n_;
+                    if (retained && std::abs(kx) >= fcols_ && (re != 0 || im != 0))
+                        raise(HZLB_EINVAL, "forcing outside the configured columns");
+                }
+            for (int kx = 0; kx < fcols_; ++kx)
+                for (int j = 0; j < LD_; ++j) {
+                    const int ypos = j <= K_ ? j : n_ - LD_ + j;
+                    const double *z = f + 2 * (static_cast<size_t>(ypos) * n_ + kx);
+                    out[static_cast<size_t>(m) * block + static_cast<size_t>(kx) * LD_ + j] =
+                        mk<R>(static_cast<R>(z[0]), static_cast<R>(z[1]));
+                }
+        }
+        cuda_check(cudaMemcpyAsync(forcing_.as<cx<R>>() + static_cast<size_t>(first) * block, out,
+                                   sizeof(cx<R>) * block * count, cudaMemcpyHostToDevice, stream_),
+                   "midpoint forcing upload");
+        cuda_check(cudaStreamSynchronize(stream_), "midpoint forcing upload");
+    }
+
+    // ---- stepping -----------------------------------------------------------------
+    ColumnArgs<R> column_args(double dt) const {
+        ColumnArgs<R> a{};
+        a.nl = nl_.as<cx<R>>();
+        a.w = w_.as<cx<R>>();
+        a.omega = omega_.as<cx<R>>();
+        a.ystage = ystage_.as<cx<R>>();
+        a.acc = acc_.as<cx<R>>();
+        a.forcing = fcount_ ? forcing_.as<cx<R>>() : nullptr;
+        a.forcing_stride = cfg_.forcing_per_member ? static_cast<long long>(fcols_) * LD_ : 0;
+        a.forcing_cols = fcols_;
+        a.tw = tw_.as<cx<R>>();
+        a.nu = cfg_.nu;
+        a.alpha = cfg_.alpha;
+        a.dt = dt;
+        a.stage = 0;
+        a.emit = 1;
+        a.noise_scale = cfg_.noise_sigma > 0 ? cfg_.noise_sigma * std::sqrt(dt) / std::sqrt(2.0) : 0.0;
+        a.noise_kmax2 = cfg_.noise_kmax * cfg_.noise_kmax;
+        a.seed = cfg_.seed;
+        a.member_base = cfg_.member_base;
+        a.ctl = ctl_.as<StepControl>();
+        a.members = M_;
+        return a;
+    }
+    RowArgs<R> row_args() const {
+        RowArgs<R> r{};
+        r.w = w_.as<cx<R>>();
+        r.nl = nl_.as<cx<R>>();
+        r.tw = tw_.as<cx<R>>();
+        r.cfl_scale = 0;
+        r.ctl = ctl_.as<StepControl>();
+        r.members = M_;
+        return r;
+    }
+    void launch_start() {
+        ColumnArgs<R> a = column_args(1.0);
+        a.stage = 0;
+        cuda_check(launch_column<R>(n_, a, stream_), "launch start column pass");
+    }
+    // The eight launches of one RK4 step; the final column pass also emits the derivative
+    // columns of the new state, so consecutive steps chain without a separate start pass.
+    void enqueue_step(double dt) {
+        ColumnArgs<R> a = column_args(dt);
+        RowArgs<R> r = row_args();
+        for (int s = 1; s <= 4; ++s) {
+            r.cfl_scale = s == 1 ? dt * n_ / (2 * kPi) : 0.0;
+            cuda_check(launch_row<R>(n_, r, stream_), "launch row pass");
+            a.stage = s;
+            cuda_check(launch_column<R>(n_, a, stream_), "launch column pass");
+        }
+    }
+    void drop_graphs() {
+        for (auto &g : graphs_)
+            if (g.exec)
+                cudaGraphExecDestroy(g.exec);
+        graphs_.clear();
+    }
+    cudaGraphExec_t graph_for(double dt, int steps) {
+        for (auto &g : graphs_)
+            if (g.dt == dt && g.steps == steps)
+                return g.exec;
+        cudaGraph_t graph = nullptr;
+        cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal),
+                   "begin step capture");
+        try {
+            for (int i = 0; i < steps; ++i)
+                enqueue_step(dt);
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            throw;
+        }
+        cuda_check(cudaStreamEndCapture(stream_, &graph), "end step capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "instantiate step graph");
+        graphs_.push_back({dt, steps, exec});
+        return exec;
+    }
+    void step(double dt, uint64_t nsteps) override {
+        const int largest = (n_ - 1) / 3;
+        if (!std::isfinite(dt) || dt <= 0 ||
+            dt * (2 * cfg_.nu * largest * largest + cfg_.alpha) > 2.5)
+            raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");
+        if (nsteps == 0)
+            return;
+        if (!w_valid_)
+            launch_start();
+        constexpr int kBatch = 8;
+        uint64_t left = nsteps;
+        while (left >= kBatch) {
+            cuda_check(cudaGraphLaunch(graph_for(dt, kBatch), stream_), "launch step graph");
+            left -= kBatch;
+        }
+        for (; left > 0; --left)
+            cuda_check(cudaGraphLaunch(graph_for(dt, 1), stream_), "launch step graph");
+        w_valid_ = true;
+        time += dt * static_cast<double>(nsteps);
+        step_index += nsteps;
+    }
+    void step_profiled(double dt, uint64_t nsteps, double *row_ms, double *col_ms) override {
+        const int largest = (n_ - 1) / 3;
+        if (!std::isfinite(dt) || dt <= 0 ||
+            dt * (2 * cfg_.nu * largest * largest + cfg_.alpha) > 2.5)
+            raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");
+        *row_ms = *col_ms = 0;
+        if (nsteps == 0)
+            return;
+        if (!w_valid_)
+            launch_start();
+        std::vector<cudaEvent_t> ev(8 * nsteps + 1);
+        for (auto &e : ev)
+            cuda_check(cudaEventCreate(&e), "create profiling event");
+        ColumnArgs<R> a = column_args(dt);
+        RowArgs<R> r = row_args();
+        size_t k = 0;
+        cuda_check(cudaEventRecord(ev[k++], stream_), "record event");
+        (void)k;
+        for (uint64_t i = 0; i < nsteps; ++i)
+            for (int s = 1; s <= 4; ++s) {
+                r.cfl_scale = s == 1 ? dt * n_ / (2 * kPi) : 0.0;
+                cuda_check(launch_row<R>(n_, r, stream_), "launch row pass");
+                cuda_check(cudaEventRecord(ev[k++], stream_), "record event");
+                a.stage = s;
+                cuda_check(launch_column<R>(n_, a, stream_), "launch column pass");
+                cuda_check(cudaEventRecord(ev[k++], stream_), "record event");
+            }
+        cuda_check(cudaStreamSynchronize(stream_), "profiled steps");
+        double rsum = 0, csum = 0;
+        // events: ev[0] before the first launch, then one after every launch
+        for (size_t i = 0; i < 4 * nsteps; ++i) {
+            float t1 = 0, t2 = 0;
+            cuda_check(cudaEventElapsedTime(&t1, ev[2 * i], ev[2 * i + 1]), "event time");
+            cuda_check(cudaEventElapsedTime(&t2, ev[2 * i + 1], ev[2 * i + 2]), "event time");
+            rsum += t1;
+            csum += t2;
+        }
+        for (auto &e : ev)
+            cudaEventDestroy(e);
+        *row_ms = rsum / (4.0 * nsteps);
+        *col_ms = csum / (4.0 * nsteps);
+        w_valid_ = true;
+        time += dt * static_cast<double>(nsteps);
+        step_index += nsteps;
+    }
+    void set_time(double t, uint64_t s) override {
+        time = t;
+        step_index = s;
+        StepControl c{};
+        c.step = s;
+        cuda_check(cudaMemcpyAsync(ctl_.ptr, &c, sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                                   stream_),
+                   "set step counter");
+        cuda_check(cudaStreamSynchronize(stream_), "set step counter");
+    }
+    uint32_t status() override {
+        StepControl c{};
+        cuda_check(cudaMemcpyAsync(&c, ctl_.ptr, sizeof c, cudaMemcpyDeviceToHost, stream_),
+                   "read status");
+        cuda_check(cudaStreamSynchronize(stream_), "read status");
+        if (c.status) {
+            const unsigned zero = 0;
+            cuda_check(cudaMemcpyAsync(&ctl_.as<StepControl>()->status, &zero, sizeof zero,
+                                       cudaMemcpyHostToDevice, stream_),
+                       "clear status");
+            cuda_check(cudaStreamSynchronize(stream_), "clear status");
+        }
+        return c.status;
+    }
+    void synchronize() override { cuda_check(cudaStreamSynchronize(stream_), "synchronize GPU"); }
+
+    // ---- diagnostics and observations ---------------------------------------------
+    void diagnostics(double *out) override {
+        scratch_d_.ensure(sizeof(double) * 3 * M_, "allocate diagnostics");
+        vbits_.ensure(sizeof(unsigned long long) * M_, "allocate CFL reduction");
+        cuda_check(launch_diagnostics<R>(n_, omega_.as<cx<R>>(), fcount_ ? forcing_.as<cx<R>>() : nullptr,
+                                         cfg_.forcing_per_member ? static_cast<long long>(fcols_) * LD_ : 0,
+                                         fcols_, M_, scratch_d_.as<double>(), stream_),
+                   "launch diagnostics");
+        launch_start();
+        w_valid_ = true;
+        cuda_check(cudaMemsetAsync(vbits_.ptr, 0, sizeof(unsigned long long) * M_, stream_),
+                   "reset CFL reduction");
+        cuda_check(launch_velocity_max<R>(n_, w_.as<cx<R>>(), vbits_.as<unsigned long long>(),
+                                          tw_.as<cx<R>>(), M_, stream_),
+                   "launch CFL reduction");
+        std::vector<double> sums(3 * M_);
+        std::vector<unsigned long long> bits(M_);
+        cuda_check(cudaMemcpyAsync(sums.data(), scratch_d_.ptr, sizeof(double) * 3 * M_,
+                                   cudaMemcpyDeviceToHost, stream_),
+                   "diagnostics download");
+        cuda_check(cudaMemcpyAsync(bits.data(), vbits_.ptr, sizeof(unsigned long long) * M_,
+                                   cudaMemcpyDeviceToHost, stream_),
+                   "CFL scalar transfer");
+        cuda_check(cudaStreamSynchronize(stream_), "diagnostics");
+        for (int m = 0; m < M_; ++m) {
+            double vmax;
+            std::memcpy(&vmax, &bits[m], sizeof vmax);
+            out[6 * m + 0] = time;
+            out[6 * m + 1] = sums[3 * m];
+            out[6 * m + 2] = sums[3 * m + 1];
+            out[6 * m + 3] = 2 * cfg_.nu * sums[3 * m + 1];
+            out[6 * m + 4] = sums[3 * m + 2];
+            out[6 * m + 5] = vmax * static_cast<double>(n_) / (2 * kPi);
+        }
+    }
+    // physical fields into phys_ (device), via the Jacobian-row buffer as column scratch
+    void physical_device() {
+        phys_.ensure(sizeof(R) * static_cast<size_t>(n_) * n_ * M_, "allocate physical fields");
+        cuda_check(launch_physical<R>(n_, omega_.as<cx<R>>(), static_cast<long long>(compact_),
+                                      nl_.as<cx<R>>(), phys_.as<R>(), tw_.as<cx<R>>(), M_, stream_),
+                   "launch physical transform");
+    }
+    void physical(double *out) override {
+        physical_device();
+        const size_t count = static_cast<size_t>(n_) * n_ * M_;
+        staging_.ensure(sizeof(R) * count);
+        cuda_check(cudaMemcpyAsync(staging_.ptr, phys_.ptr, sizeof(R) * count,
+                                   cudaMemcpyDeviceToHost, stream_),
+                   "physical field download");
+        cuda_check(cudaStreamSynchronize(stream_), "physical field download");
+        const R *p = staging_.as<R>();
+        for (size_t i = 0; i < count; ++i)
+            out[i] = p[i];
+    }
+    void observe_device(const uint32_t *x, const uint32_t *y, size_t p) {
+        for (size_t o = 0; o < p; ++o)
+            if (x[o] >= static_cast<uint32_t>(n_) || y[o] >= static_cast<uint32_t>(n_))
+                raise(HZLB_EINVAL, "observation location out of bounds");
+        physical_device();
+        obs_xy_.ensure(sizeof(uint32_t) * 2 * std::max<size_t>(p, 1), "allocate observation points");
+        obs_.ensure(sizeof(double) * std::max<size_t>(p, 1) * M_, "allocate observations");
+        cuda_check(cudaMemcpyAsync(obs_xy_.ptr, x, sizeof(uint32_t) * p, cudaMemcpyHostToDevice, stream_),
+                   "upload observation points");
+        cuda_check(cudaMemcpyAsync(obs_xy_.as<uint32_t>() + p, y, sizeof(uint32_t) * p,
+                                   cudaMemcpyHostToDevice, stream_),
+                   "upload observation points");
+        cuda_check(launch_gather<R>(phys_.as<R>(), n_, obs_xy_.as<unsigned>(),
+                                    obs_xy_.as<unsigned>() + p, static_cast<int>(p), M_,
+                                    obs_.as<double>(), stream_),
+                   "launch observation gather");
+    }
+    void observe(const uint32_t *x, const uint32_t *y, size_t p, double *out) override {
+        observe_device(x, y, p);
+        cuda_check(cudaMemcpyAsync(out, obs_.ptr, sizeof(double) * p * M_, cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "observation download");
+        cuda_check(cudaStreamSynchronize(stream_), "observation download");
+    }
+
+    // ---- filters --------------------------------------------------------------------
+    void resample(const double *w, size_t count, double u, uint32_t *anc) override {
+        scratch_d_.ensure(sizeof(double) * 2 * count, "allocate resampling weights");
+        anc_.ensure(sizeof(unsigned) * count, "allocate ancestors");
+        cuda_check(cudaMemcpyAsync(scratch_d_.ptr, w, sizeof(double) * count, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "upload weights");
+        systematic_resample_kernel<<<1, 1024, 0, stream_>>>(
+            scratch_d_.as<double>(), scratch_d_.as<double>() + count, static_cast<int>(count), u,
+            anc_.as<unsigned>());
+        cuda_check(cudaGetLastError(), "launch resampling");
+        cuda_check(cudaMemcpyAsync(anc, anc_.ptr, sizeof(unsigned) * count, cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "download ancestors");
+        cuda_check(cudaStreamSynchronize(stream_), "resampling");
+    }
+    void gather(const uint32_t *ancestors) override {
+        for (int i = 0; i < M_; ++i)
+            if (ancestors[i] >= static_cast<uint32_t>(M_))
+                raise(HZLB_EINVAL, "ancestor index out of range");
+        anc_.ensure(sizeof(unsigned) * M_, "allocate ancestors");
+        cuda_check(cudaMemcpyAsync(anc_.ptr, ancestors, sizeof(unsigned) * M_, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "upload ancestors");
+        const dim3 grid(std::max<int>(1, static_cast<int>((compact_ + 255) / 256)), M_);
+        gather_blocks<R><<<grid, 256, 0, stream_>>>(omega_.as<cx<R>>(), ystage_.as<cx<R>>(),
+                                                    anc_.as<unsigned>(), static_cast<long long>(compact_));
+        cuda_check(cudaGetLastError(), "launch member gather");
+        cuda_check(cudaMemcpyAsync(omega_.ptr, ystage_.ptr, sizeof(cx<R>) * compact_ * M_,
+                                   cudaMemcpyDeviceToDevice, stream_),
+                   "commit member gather");
+        if (fcount_ > 1) {
+            const long long fb = static_cast<long long>(fcols_) * LD_;
+            const dim3 fg(std::max<int>(1, static_cast<int>((fb + 255) / 256)), M_);
+            gather_blocks<R><<<fg, 256, 0, stream_>>>(forcing_.as<cx<R>>(), ystage_.as<cx<R>>(),
+                                                      anc_.as<unsigned>(), fb);
+            cuda_check(cudaGetLastError(), "launch forcing gather");
+            cuda_check(cudaMemcpyAsync(forcing_.ptr, ystage_.ptr, sizeof(cx<R>) * fb * M_,
+                                       cudaMemcpyDeviceToDevice, stream_),
+                       "commit forcing gather");
+        }
+        cuda_check(cudaStreamSynchronize(stream_), "member gather");
+        w_valid_ = false;
+    }
+    void inflate(double inflation) override {
+        if (!std::isfinite(inflation) || inflation < 1)
+            raise(HZLB_EINVAL, "EnKF inflation must be >= 1");
+        if (inflation == 1)
+            return;
+        const int blocks = static_cast<int>(std::min<size_t>((compact_ + 255) / 256, 4096));
+        inflate_kernel<R><<<blocks, 256, 0, stream_>>>(omega_.as<cx<R>>(),
+                                                       static_cast<long long>(compact_), M_, inflation);
+        cuda_check(cudaGetLastError(), "launch inflation");
+        w_valid_ = false;
+    }
+    void enkf(const uint32_t *x, const uint32_t *y, const double *values, const double *sd,
+              size_t p, const double *eps) override {
+        if (M_ < 2)
+            raise(HZLB_EINVAL, "EnKF requires at least two ensemble members");
+        if (p == 0)
+            return;
+        for (size_t o = 0; o < p; ++o)
+            if (!std::isfinite(values[o]) || !std::isfinite(sd[o]) || sd[o] <= 0)
+                raise(HZLB_EINVAL, "observations must be finite and have positive uncertainty");
+        observe_device(x, y, p);
+        const size_t mp = static_cast<size_t>(M_) * p;
+        enkf_.ensure(sizeof(double) * (2 * p + 3 * mp + p * p + static_cast<size_t>(M_) * M_) + 64,
+                     "allocate EnKF workspace");
+        double *ybuf = enkf_.as<double>(), *sdbuf = ybuf + p, *eps_d = sdbuf + p, *ha = eps_d + mp,
+               *d = ha + mp, *P = d + mp, *W = P + p * p;
+        int *info = reinterpret_cast<int *>(W + static_cast<size_t>(M_) * M_);
+        cuda_check(cudaMemcpyAsync(ybuf, values, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
+                   "upload observations");
+        cuda_check(cudaMemcpyAsync(sdbuf, sd, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
+                   "upload observation errors");
+        cuda_check(cudaMemcpyAsync(eps_d, eps, sizeof(double) * mp, cudaMemcpyHostToDevice, stream_),
+                   "upload perturbations");
+        const int pi = static_cast<int>(p);
+        enkf_innovations<<<(pi + 127) / 128, 128, 0, stream_>>>(obs_.as<double>(), ybuf, sdbuf, eps_d,
+                                                                M_, pi, ha, d);
+        enkf_gram<<<dim3((pi + 15) / 16, (pi + 15) / 16), dim3(16, 16), 0, stream_>>>(ha, sdbuf, M_,
+                                                                                      pi, P);
+        cholesky_kernel<<<1, 1024, 0, stream_>>>(P, pi, info);
+        cholesky_solve<<<(M_ + 127) / 128, 128, 0, stream_>>>(P, pi, d, M_);
+        enkf_weights<<<dim3((M_ + 15) / 16, (M_ + 15) / 16), dim3(16, 16), 0, stream_>>>(ha, d, M_, pi, W);
+        cuda_check(cudaGetLastError(), "launch EnKF analysis");
+        // X_a = X + (X - mean) W, written to the stage buffer then committed
+        cx<R> *mean = acc_.as<cx<R>>();   // free between steps
+        const int mb = static_cast<int>(std::min<size_t>((compact_ + 255) / 256, 4096));
+        ensemble_mean<R><<<mb, 256, 0, stream_>>>(omega_.as<cx<R>>(), static_cast<long long>(compact_),
+                                                  M_, mean);
+        const dim3 ug(static_cast<unsigned>((compact_ + 63) / 64), (M_ + 15) / 16);
+        anomaly_update<R><<<ug, 64, 0, stream_>>>(omega_.as<cx<R>>(), mean, W,
+                                                  static_cast<long long>(compact_), M_,
+                                                  ystage_.as<cx<R>>());
+        cuda_check(cudaGetLastError(), "launch EnKF update");
+        cuda_check(cudaMemcpyAsync(omega_.ptr, ystage_.ptr, sizeof(cx<R>) * compact_ * M_,
+                                   cudaMemcpyDeviceToDevice, stream_),
+                   "commit EnKF update");
+        int host_info = 0;
+        cuda_check(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                   "read Cholesky status");
+        cuda_check(cudaStreamSynchronize(stream_), "EnKF analysis");
+        w_valid_ = false;
+        if (host_info != 0)
+            raise(HZLB_ERUNTIME, "EnKF innovation covariance is not positive definite");
+    }
+
+  private:
+    struct Graph {
+        double dt;
+        int steps;
+        cudaGraphExec_t exec;
+    };
+    hzlb_config cfg_;
+    int n_ = 0, M_ = 0, K_ = 0, C_ = 0, LD_ = 0, fcols_ = 0, fcount_ = 0;
+    size_t compact_ = 0;
+    cudaStream_t stream_ = nullptr;
+    DeviceBuffer omega_, ystage_, acc_, w_, nl_, forcing_, ctl_, tw_, phys_, scratch_d_, vbits_,
+        obs_xy_, obs_, anc_, enkf_;
+    PinnedBuffer staging_;
+    std::vector<Graph> graphs_;
+    bool w_valid_ = false;
+};
+
+} // namespace
+
+std::unique_ptr<Engine> make_engine(const hzlb_config &c) {
+    if (c.precision == 4)
+        return std::make_unique<EngineT<float>>(c);
+    if (c.precision == 8)
+        return std::make_unique<EngineT<double>>(c);
+    raise(HZLB_EINVAL, "precision must be 4 (FP32) or 8 (FP64)");
+}
+
+void pf_weights_host(const double *logs, size_t count, double *w, double *inc, double *ess,
+                     double *mw) {
+    if (count < 2)
+        raise(HZLB_EINVAL, "particle filter needs at least two particles");
+    double maximum = logs[0];
+    for (size_t i = 1; i < count; ++i)
+        if (maximum < logs[i])
+            maximum = logs[i];
+    if (!std::isfinite(maximum))
+        raise(HZLB_ERUNTIME, "particle likelihood collapsed numerically");
+    double total = 0;
+    for (size_t i = 0; i < count; ++i)
+        total += std::exp(logs[i] - maximum);
+    const double increment = maximum + std::log(total);
+    double squared = 0, max_weight = 0;
+    for (size_t i = 0; i < count; ++i) {
+        w[i] = std::exp(logs[i] - increment);
+        squared += w[i] * w[i];
+        max_weight = std::max(max_weight, w[i]);
+    }
+    *inc = increment;
+    *ess = 1 / squared;
+    *mw = max_weight;
+}
+
+void systematic_resample_host(const double *w, size_t count, double u, uint32_t *anc) {
+    size_t ancestor = 0;
+    double cumulative = w[0];
+    const double start = u / static_cast<double>(count);
+    for (size_t i = 0; i < count; ++i) {
+        const double position = start + static_cast<double>(i) / static_cast<double>(count);
+        while (position > cumulative && ancestor + 1 < count)
+            cumulative += w[++ancestor];
+        anc[i] = static_cast<uint32_t>(ancestor);
+    }
+}
+
+} // namespace hzlb

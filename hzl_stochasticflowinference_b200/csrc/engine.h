@@ -1,0 +1,105 @@
+// C++ host runtime of one ensemble handle: device buffers, the RK4 stage schedule (replayed
+// from captured CUDA graphs), state/forcing I/O in the reference layout, diagnostics, the
+// observation operator and the filter analysis steps.
+#pragma once
+#include "../../include/hzlb.h"
+#include "launch.h"
+
+#include <cuda_runtime.h>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace hzlb {
+
+// Exceptions carry the C-ABI code they map to.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+[[noreturn]] inline void raise(int code, const std::string &message) { throw Error(code, message); }
+inline void cuda_check(cudaError_t e, const char *operation) {
+    if (e != cudaSuccess)
+        raise(HZLB_ECUDA, std::string(operation) + ": " + cudaGetErrorString(e));
+}
+
+// Device allocation owned by RAII.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr)
+            cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    void ensure(size_t b, const char *what) {
+        if (b <= bytes)
+            return;
+        release();
+        cuda_check(cudaMalloc(&ptr, b), what);
+        bytes = b;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+struct PinnedBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    ~PinnedBuffer() {
+        if (ptr)
+            cudaFreeHost(ptr);
+    }
+    void ensure(size_t b) {
+        if (b <= bytes)
+            return;
+        if (ptr)
+            cudaFreeHost(ptr);
+        ptr = nullptr;
+        cuda_check(cudaMallocHost(&ptr, b), "allocate pinned staging buffer");
+        bytes = b;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+class Engine {
+  public:
+    virtual ~Engine() = default;
+    virtual void set_state(const double *spectra, int first, int count) = 0;
+    virtual void get_state(double *spectra, int first, int count) = 0;
+    virtual void set_state_compact(const void *data, int first, int count) = 0;
+    virtual void get_state_compact(void *data, int first, int count) = 0;
+    virtual void set_forcing(const double *spectra, int first, int count) = 0;
+    virtual void step(double dt, uint64_t nsteps) = 0;
+    virtual uint32_t status() = 0;
+    virtual void synchronize() = 0;
+    virtual void diagnostics(double *out) = 0;
+    virtual void physical(double *out) = 0;
+    virtual void observe(const uint32_t *x, const uint32_t *y, size_t p, double *out) = 0;
+    virtual void resample(const double *w, size_t count, double u, uint32_t *anc) = 0;
+    virtual void gather(const uint32_t *ancestors) = 0;
+    virtual void inflate(double inflation) = 0;
+    virtual void enkf(const uint32_t *x, const uint32_t *y, const double *values, const double *sd,
+                      size_t p, const double *perturbations) = 0;
+    virtual size_t compact_size() const = 0;
+    virtual int members() const = 0;
+    virtual void *stream() const = 0;
+    virtual void step_profiled(double dt, uint64_t nsteps, double *row_ms, double *col_ms) = 0;
+
+    double time = 0;
+    uint64_t step_index = 0;
+    virtual void set_time(double t, uint64_t s) = 0;
+};
+
+std::unique_ptr<Engine> make_engine(const hzlb_config &c);
+
+// Host-side reference-order particle weights and systematic resampling (filter.cpp:76-112).
+void pf_weights_host(const double *logs, size_t count, double *w, double *inc, double *ess,
+                     double *mw);
+void systematic_resample_host(const double *w, size_t count, double u, uint32_t *anc);
+
+} // namespace hzlb

@@ -1,0 +1,157 @@
+// Template instantiation and launch dispatch for the spectral kernels, N = 8..512, float and
+// double.  Grids put members on x (no 65535 limit) and column blocks / row tiles on y.
+#include "launch.h"
+#include "physical.cuh"
+
+namespace hzlb {
+namespace {
+
+template <typename R, int N> struct L {
+    using G = Cfg<R, N>;
+    static constexpr size_t col_smem = sizeof(cx<R>) * (N + G::LPB * G::BUF);
+    static constexpr size_t row_smem =
+        sizeof(cx<R>) * (N + 4 * G::TY * G::SC + G::C * (G::TY + 1) + G::GROUPS * G::BUF);
+    static constexpr size_t prow_smem = sizeof(cx<R>) * (N + G::GROUPS * G::BUF);
+    static_assert(row_smem <= 227 * 1024, "row kernel shared memory");
+
+    static cudaError_t prepare() {
+        cudaError_t e = cudaFuncSetAttribute(column_kernel<R, N>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(col_smem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(row_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(row_smem));
+        return e;
+    }
+    static dim3 col_grid(int members) { return dim3(members, (G::C + G::LPB - 1) / G::LPB); }
+    static dim3 row_grid(int members) { return dim3(members, N / G::TY); }
+    static cudaError_t column(const ColumnArgs<R> &a, cudaStream_t s) {
+        column_kernel<R, N><<<col_grid(a.members), G::COL_THREADS, col_smem, s>>>(a);
+        return cudaGetLastError();
+    }
+    static cudaError_t row(const RowArgs<R> &a, cudaStream_t s) {
+        row_kernel<R, N><<<row_grid(a.members), G::ROW_THREADS, row_smem, s>>>(a);
+        return cudaGetLastError();
+    }
+    static cudaError_t physical(const cx<R> *field, long long stride, cx<R> *cols, R *phys,
+                                const cx<R> *tw, int members, cudaStream_t s) {
+        field_column_inverse<R, N><<<col_grid(members), G::COL_THREADS, col_smem, s>>>(
+            field, stride, cols, tw);
+        field_row_inverse<R, N><<<row_grid(members), G::ROW_THREADS, prow_smem, s>>>(cols, phys, tw);
+        return cudaGetLastError();
+    }
+    static cudaError_t vmax(const cx<R> *w, unsigned long long *bits, const cx<R> *tw, int members,
+                            cudaStream_t s) {
+        velocity_max<R, N><<<row_grid(members), G::ROW_THREADS, prow_smem, s>>>(w, bits, tw);
+        return cudaGetLastError();
+    }
+    static void shape(KernelShape &k) {
+        k.col_threads = G::COL_THREADS;
+        k.row_threads = G::ROW_THREADS;
+        k.col_blocks_per_member = (G::C + G::LPB - 1) / G::LPB;
+        k.row_blocks_per_member = N / G::TY;
+        k.col_smem = col_smem;
+        k.row_smem = row_smem;
+        k.elements_per_thread = G::E;
+        k.rows_per_block = G::TY;
+    }
+};
+
+template <typename R, template <typename, int> class F, typename... A>
+cudaError_t dispatch(int n, A &&...args) {
+    switch (n) {
+    case 8: return F<R, 8>::run(args...);
+    case 16: return F<R, 16>::run(args...);
+    case 32: return F<R, 32>::run(args...);
+    case 64: return F<R, 64>::run(args...);
+    case 128: return F<R, 128>::run(args...);
+    case 256: return F<R, 256>::run(args...);
+    case 512: return F<R, 512>::run(args...);
+    default: return cudaErrorInvalidValue;
+    }
+}
+template <typename R, int N> struct DoPrepare {
+    static cudaError_t run() { return L<R, N>::prepare(); }
+};
+template <typename R, int N> struct DoColumn {
+    static cudaError_t run(const ColumnArgs<R> &a, cudaStream_t s) { return L<R, N>::column(a, s); }
+};
+template <typename R, int N> struct DoRow {
+    static cudaError_t run(const RowArgs<R> &a, cudaStream_t s) { return L<R, N>::row(a, s); }
+};
+template <typename R, int N> struct DoPhysical {
+    static cudaError_t run(const cx<R> *f, long long st, cx<R> *c, R *p, const cx<R> *tw, int m,
+                           cudaStream_t s) {
+        return L<R, N>::physical(f, st, c, p, tw, m, s);
+    }
+};
+template <typename R, int N> struct DoVmax {
+    static cudaError_t run(const cx<R> *w, unsigned long long *b, const cx<R> *tw, int m,
+                           cudaStream_t s) {
+        return L<R, N>::vmax(w, b, tw, m, s);
+    }
+};
+template <typename R, int N> struct DoShape {
+    static cudaError_t run(KernelShape &k) {
+        L<R, N>::shape(k);
+        return cudaSuccess;
+    }
+};
+} // namespace
+
+template <typename R> cudaError_t prepare_kernels(int n) { return dispatch<R, DoPrepare>(n); }
+template <typename R> cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s) {
+    return dispatch<R, DoColumn>(n, a, s);
+}
+template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s) {
+    return dispatch<R, DoRow>(n, a, s);
+}
+template <typename R>
+cudaError_t launch_physical(int n, const cx<R> *field, long long stride, cx<R> *cols, R *phys,
+                            const cx<R> *tw, int members, cudaStream_t s) {
+    return dispatch<R, DoPhysical>(n, field, stride, cols, phys, tw, members, s);
+}
+template <typename R>
+cudaError_t launch_velocity_max(int n, const cx<R> *w, unsigned long long *bits, const cx<R> *tw,
+                                int members, cudaStream_t s) {
+    return dispatch<R, DoVmax>(n, w, bits, tw, members, s);
+}
+template <typename R>
+cudaError_t launch_diagnostics(int n, const cx<R> *omega, const cx<R> *forcing, long long fstride,
+                               int fcols, int members, double *out, cudaStream_t s) {
+    integral_diagnostics<R><<<members, 256, 0, s>>>(omega, forcing, fstride, fcols, n, out);
+    return cudaGetLastError();
+}
+template <typename R>
+cudaError_t launch_gather(const R *phys, int n, const unsigned *xs, const unsigned *ys, int p,
+                          int members, double *out, cudaStream_t s) {
+    const long long total = static_cast<long long>(members) * p;
+    if (total == 0)
+        return cudaSuccess;
+    gather_points<R><<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(phys, n, xs, ys, p,
+                                                                              members, out);
+    return cudaGetLastError();
+}
+template <typename R> KernelShape kernel_shape(int n) {
+    KernelShape k{};
+    dispatch<R, DoShape>(n, k);
+    return k;
+}
+
+#define HZLB_INSTANTIATE(R)                                                                        \
+    template cudaError_t prepare_kernels<R>(int);                                                  \
+    template cudaError_t launch_column<R>(int, const ColumnArgs<R> &, cudaStream_t);               \
+    template cudaError_t launch_row<R>(int, const RowArgs<R> &, cudaStream_t);                     \
+    template cudaError_t launch_physical<R>(int, const cx<R> *, long long, cx<R> *, R *,          \
+                                            const cx<R> *, int, cudaStream_t);                     \
+    template cudaError_t launch_velocity_max<R>(int, const cx<R> *, unsigned long long *,         \
+                                                const cx<R> *, int, cudaStream_t);                 \
+    template cudaError_t launch_diagnostics<R>(int, const cx<R> *, const cx<R> *, long long, int, \
+                                               int, double *, cudaStream_t);                       \
+    template cudaError_t launch_gather<R>(const R *, int, const unsigned *, const unsigned *, int, \
+                                          int, double *, cudaStream_t);                            \
+    template KernelShape kernel_shape<R>(int);
+HZLB_INSTANTIATE(float)
+HZLB_INSTANTIATE(double)
+
+} // namespace hzlb

@@ -1,0 +1,31 @@
+// Host-side declarations of the kernel launchers (implemented in launch.cu).
+#pragma once
+#include "spectral_step.cuh"
+
+namespace hzlb {
+
+struct KernelShape {
+    int col_threads, row_threads;
+    int col_blocks_per_member, row_blocks_per_member;
+    size_t col_smem, row_smem;
+    int elements_per_thread, rows_per_block;
+};
+
+template <typename R> cudaError_t prepare_kernels(int n);
+template <typename R> cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s);
+template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s);
+template <typename R>
+cudaError_t launch_physical(int n, const cx<R> *field, long long stride, cx<R> *cols, R *phys,
+                            const cx<R> *tw, int members, cudaStream_t s);
+template <typename R>
+cudaError_t launch_velocity_max(int n, const cx<R> *w, unsigned long long *bits, const cx<R> *tw,
+                                int members, cudaStream_t s);
+template <typename R>
+cudaError_t launch_diagnostics(int n, const cx<R> *omega, const cx<R> *forcing, long long fstride,
+                               int fcols, int members, double *out, cudaStream_t s);
+template <typename R>
+cudaError_t launch_gather(const R *phys, int n, const unsigned *xs, const unsigned *ys, int p,
+                          int members, double *out, cudaStream_t s);
+template <typename R> KernelShape kernel_shape(int n);
+
+} // namespace hzlb

@@ -1,0 +1,171 @@
+/* hzlb.h -- C ABI of the B200 ensemble forecast/analysis path.
+ *
+ * This library replaces, for the reference pvasbob/HZL-stochasticFlowInference, the
+ * GPU solver and the per-member loops of its ensemble, particle-filter and EnKF drivers:
+ *
+ *   reference interface (include/hzl/...)              replaced by
+ *   CudaSolver(n, Parameters, initial)                 hzlb_ensemble_create + hzlb_set_state
+ *     (cuda_solver.hpp:9, cuda_solver.cu:126-171)
+ *   CudaSolver::step(dt) / step(dt, forcing)           hzlb_set_forcing + hzlb_step
+ *     (cuda_solver.hpp:13-14, cuda_solver.cu:173-218)
+ *   CudaSolver::coefficients()                         hzlb_get_state
+ *     (cuda_solver.hpp:16, cuda_solver.cu:222-235)
+ *   Solver::diagnostics() per member                   hzlb_diagnostics
+ *     (solver.hpp:85, solver.cpp:381-397)
+ *   Solver::physical_vorticity() per member            hzlb_physical / hzlb_observe
+ *     (solver.hpp:86, solver.cpp:398-402)
+ *   hzl::ensemble(n, p, dt, steps, count, ...)         hzlb_ensemble_create + hzlb_step +
+ *     (inference.hpp:85-86, inference.cpp:555-590)     hzlb_diagnostics
+ *   bootstrap_filter weights / resampling             hzlb_pf_weights, hzlb_systematic_resample,
+ *     (filter.hpp:17-18, filter.cpp:66-120)            hzlb_gather_members
+ *   ensemble_kalman_filter analysis                    hzlb_enkf_analysis
+ *     (filter.hpp:52-54, filter.cpp:237-321)
+ *
+ * Conventions.  Every function returns HZLB_OK (0) or a negative HZLB_E* code; the message
+ * of the last failure on the calling thread is hzlb_last_error().  HZLB_EINVAL corresponds
+ * to the reference's std::invalid_argument, HZLB_ERUNTIME to std::runtime_error (CFL limit,
+ * nonfinite state), HZLB_ECUDA to CUDA failures (std::runtime_error("<op>: <cuda msg>") in
+ * the reference).  The caller owns host buffers; the library owns device memory.  Each
+ * ensemble handle owns one CUDA stream; calls on one handle are not thread-safe, separate
+ * handles are independent.
+ *
+ * Field layout at this boundary: complex spectra as interleaved (re, im) doubles, n*n
+ * entries per member in the reference layout (index y*n + x, Fourier coefficients
+ * normalised by 1/n^2 on the forward transform: include/hzl/fft.hpp:7-9).  Members are
+ * consecutive.
+ */
+#ifndef HZLB_H
+#define HZLB_H
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HZLB_API __attribute__((visibility("default")))
+#else
+#define HZLB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HZLB_OK 0
+#define HZLB_EINVAL (-1)
+#define HZLB_ERUNTIME (-2)
+#define HZLB_ECUDA (-3)
+#define HZLB_ETIMEOUT (-4)
+
+/* Device status bits returned by hzlb_status. */
+#define HZLB_STATUS_CFL 1u       /* dt * max(|u|+|v|) n / 2pi > 0.5 (solver.cpp:213) */
+#define HZLB_STATUS_NONFINITE 2u /* nonfinite coefficient after a step (solver.cpp:247-250) */
+#define HZLB_STATUS_TIMEOUT 4u
+
+typedef struct hzlb_ensemble hzlb_ensemble;
+
+typedef struct {
+    int n;                     /* grid size, power of two in [8, 512] */
+    int members;               /* ensemble members held by this handle */
+    int precision;             /* 4: complex64 spectra (FP32 path), 8: complex128 (FP64 path) */
+    double nu, alpha;          /* viscosity, linear friction (hzl::Parameters, solver.hpp:16-17) */
+    int forcing_kmax;          /* forcing stored for columns kx <= forcing_kmax; -1: no forcing */
+    int forcing_per_member;    /* 0: one forcing field shared by all members; 1: one per member */
+    double noise_sigma;        /* Euler-Maruyama noise amplitude after each step; 0: off */
+    int noise_kmax;            /* noise on modes with 1 <= |k|^2 <= noise_kmax^2 */
+    uint64_t seed;             /* Philox key for the noise */
+    uint32_t member_base;      /* global index of member 0 (Philox key; sharding offset) */
+    int device;                /* CUDA device ordinal */
+} hzlb_config;
+
+HZLB_API const char *hzlb_last_error(void);
+/* Library version string. */
+HZLB_API const char *hzlb_version(void);
+
+HZLB_API int hzlb_ensemble_create(const hzlb_config *config, hzlb_ensemble **out);
+HZLB_API void hzlb_ensemble_destroy(hzlb_ensemble *h);
+
+/* Spectral state of members [first, first+count), reference layout (see above).  set_state
+ * keeps only the retained 2/3-rule modes, as CudaSolver's constructor and Solver::project do
+ * (cuda_solver.cu:158-167, solver.cpp:140-144); nonfinite input is HZLB_EINVAL. */
+HZLB_API int hzlb_set_state(hzlb_ensemble *h, const double *spectra, int first, int count);
+HZLB_API int hzlb_get_state(hzlb_ensemble *h, double *spectra, int first, int count);
+/* The same in the handle's compact device layout ([member][kx 0..K][j 0..2K], K=(n-1)/3,
+ * ky = j for j <= K else j - 2K - 1), in the handle's precision (float or double pairs).
+ * No layout conversion; used for bulk transfers. */
+HZLB_API int hzlb_set_state_compact(hzlb_ensemble *h, const void *compact, int first, int count);
+HZLB_API int hzlb_get_state_compact(hzlb_ensemble *h, void *compact, int first, int count);
+HZLB_API size_t hzlb_compact_size(const hzlb_ensemble *h); /* complex entries per member */
+
+/* Forcing spectra held constant over each step (the midpoint forcing of the reference's
+ * RK4 step, solver.cpp:217-234; CudaSolver::step(dt, forcing), cuda_solver.cu:184-202).
+ * Shared forcing: count must be 1.  Must be conjugate-symmetric to 1e-12 and vanish outside
+ * columns |kx| <= forcing_kmax (HZLB_EINVAL otherwise). */
+HZLB_API int hzlb_set_forcing(hzlb_ensemble *h, const double *spectra, int first, int count);
+
+/* Advance every member by nsteps RK4 steps of size dt (asynchronous on the handle's stream).
+ * HZLB_EINVAL for a nonpositive/nonfinite dt or dt * (2 nu K^2 + alpha) > 2.5
+ * (cuda_solver.cu:205-208). */
+HZLB_API int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps);
+/* Waits for the handle's stream; returns the accumulated status bits and clears them. */
+HZLB_API int hzlb_status(hzlb_ensemble *h, uint32_t *status);
+HZLB_API int hzlb_synchronize(hzlb_ensemble *h);
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own work or
+ * record events against the library's kernels. */
+HZLB_API void *hzlb_stream(hzlb_ensemble *h);
+/* Profiling variant of hzlb_step: runs nsteps steps with individual launches (no graph) and
+ * CUDA events around every launch; returns the mean duration in milliseconds of the row-pass
+ * and column-pass launches.  Same results as hzlb_step. */
+HZLB_API int hzlb_step_profiled(hzlb_ensemble *h, double dt, uint64_t nsteps, double *row_ms,
+                                double *column_ms);
+/* Simulated time and the noise step counter. */
+HZLB_API int hzlb_time(hzlb_ensemble *h, double *time, uint64_t *step_index);
+HZLB_API int hzlb_set_time(hzlb_ensemble *h, double time, uint64_t step_index);
+
+/* Per member {time, energy, enstrophy, dissipation, injection, cfl_rate} (hzl::Diagnostics,
+ * solver.hpp:24-26); out has 6*members doubles. */
+HZLB_API int hzlb_diagnostics(hzlb_ensemble *h, double *out);
+/* Physical vorticity of every member, members*n*n doubles indexed [m][y][x]. */
+HZLB_API int hzlb_physical(hzlb_ensemble *h, double *out);
+/* Physical vorticity at p grid points (x[o], y[o]) of every member: out[m*p + o]. */
+HZLB_API int hzlb_observe(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, size_t p, double *out);
+
+/* ---- particle filter (filter.cpp:66-120) ------------------------------------------- */
+/* Adds the Gaussian observation log-likelihood of every member to log_weights[m] (the
+ * residual (field - value)/sd with the log sd + log(2 pi)/2 constants, filter.cpp:66-75). */
+HZLB_API int hzlb_pf_loglik(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, const double *values,
+                   const double *sd, size_t p, double *log_weights);
+/* Log-sum-exp increment, normalised weights, ESS = 1/sum w^2, max weight (filter.cpp:76-92). */
+HZLB_API int hzlb_pf_weights(const double *log_weights, size_t count, double *weights, double *increment,
+                    double *ess, double *max_weight);
+/* Systematic resampling: start = u/M, positions start + i/M walked against the sequential
+ * cumulative sum of the weights (filter.cpp:102-112).  Bit-exact with the reference given
+ * identical weights and u.  Runs on the device when h is non-NULL, else on the host. */
+HZLB_API int hzlb_systematic_resample(hzlb_ensemble *h, const double *weights, size_t count, double u,
+                             uint32_t *ancestors);
+/* Replace member i's state with member ancestors[i]'s (and its forcing if per member). */
+HZLB_API int hzlb_gather_members(hzlb_ensemble *h, const uint32_t *ancestors);
+
+/* ---- EnKF (filter.cpp:237-321) ------------------------------------------------------ */
+/* Multiplicative anomaly inflation of the spectral state about the ensemble mean
+ * (filter.cpp:237-253 for the vorticity part). */
+HZLB_API int hzlb_inflate(hzlb_ensemble *h, double inflation);
+/* Perturbed-observation EnKF analysis of all p observations at once:
+ *   X_a = X + A (HA)^T (HA HA^T/(M-1) + R)^{-1} (y + sd*eps - HX) / (M-1)
+ * with the p x p innovation system factorised by an FP64 Cholesky on the device.
+ * perturbations: M x p standard normals (row m = member).  With p = 1 this equals the
+ * reference's serial scalar update (filter.cpp:265-321, no localisation). */
+HZLB_API int hzlb_enkf_analysis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
+                       const double *values, const double *sd, size_t p,
+                       const double *perturbations);
+
+/* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
+ * analytic initial fields, solver.cpp:145-161) -------------------------------------- */
+/* Gaussian random vorticity spectrum, E(k) ~ k^4 exp(-(k/6)^2), unit enstrophy, retained modes
+ * only; Philox4x32-10 normals keyed by (seed, member).  out: n*n complex, reference layout. */
+HZLB_API int hzlb_grf_spectrum(int n, uint64_t seed, uint32_t member, double *out);
+/* amplitude * sin(wavenumber * y) as spectral coefficients, reference layout. */
+HZLB_API int hzlb_kolmogorov_forcing(int n, double amplitude, int wavenumber, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,295 @@
+// TEST INFRASTRUCTURE ONLY: a C wrapper over the reference's own C++ API.
+//
+// This file is compiled together with the reference sources (src/fft.cpp, src/solver.cpp,
+// src/inference.cpp, src/adjoint.cpp, src/filter.cpp, src/reduced.cpp of the reference tree,
+// which stay where they lie) into oracle/_ref/libhzlref.so by oracle/Makefile.  The library
+// is the checker for the CUDA path and the "reference" CPU baseline; nothing in the product
+// links it.  Every function returns 0 on success and a negative code after catching a C++
+// exception, whose message is kept for ref_last_error().
+//
+// Complex fields cross this boundary as interleaved (re, im) doubles, n*n entries in the
+// reference layout (index y*n + x, include/hzl/fft.hpp:7-8).
+#include "hzl/filter.hpp"
+#include "hzl/inference.hpp"
+#include "hzl/reduced.hpp"
+#include "hzl/solver.hpp"
+
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace {
+thread_local std::string last_error;
+
+template <class F> int guarded(F &&f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::invalid_argument &e) {
+        last_error = e.what();
+        return -1;
+    } catch (const std::exception &e) {
+        last_error = e.what();
+        return -2;
+    } catch (...) {
+        last_error = "unknown exception";
+        return -3;
+    }
+}
+
+hzl::Field to_field(const double *v, std::size_t count) {
+    hzl::Field f(count);
+    for (std::size_t i = 0; i < count; ++i)
+        f[i] = {v[2 * i], v[2 * i + 1]};
+    return f;
+}
+
+void from_field(const hzl::Field &f, double *out) {
+    for (std::size_t i = 0; i < f.size(); ++i) {
+        out[2 * i] = f[i].real();
+        out[2 * i + 1] = f[i].imag();
+    }
+}
+
+hzl::Parameters params(const double *p6) {
+    hzl::Parameters p;
+    p.viscosity = p6[0];
+    p.friction = p6[1];
+    p.forcing_sigma = p6[2];
+    p.forcing_tau = p6[3];
+    p.forcing_min = static_cast<int>(p6[4]);
+    p.forcing_max = static_cast<int>(p6[5]);
+    return p;
+}
+
+hzl::Dataset dataset(std::size_t n, double dt, int stochastic, int fmin, int fmax,
+                     std::size_t count, const unsigned long long *steps, const unsigned *xs,
+                     const unsigned *ys, const double *values, const double *sds) {
+    hzl::Dataset d;
+    d.n = n;
+    d.dt = dt;
+    d.stochastic = stochastic != 0;
+    d.forcing_min = fmin;
+    d.forcing_max = fmax;
+    d.observations.resize(count);
+    for (std::size_t i = 0; i < count; ++i)
+        d.observations[i] = {static_cast<std::size_t>(steps[i]), xs[i], ys[i], values[i], sds[i]};
+    return d;
+}
+} // namespace
+
+extern "C" {
+const char *ref_last_error(void) { return last_error.c_str(); }
+
+unsigned long long ref_stream_seed(unsigned long long base, unsigned long long index) {
+    return hzl::stream_seed(base, index);
+}
+
+int ref_fft(int n, double *data, int inverse) {
+    return guarded([&] {
+        hzl::Fourier2D f(static_cast<std::size_t>(n));
+        auto field = to_field(data, static_cast<std::size_t>(n) * n);
+        if (inverse)
+            f.inverse(field);
+        else
+            f.forward(field);
+        from_field(field, data);
+    });
+}
+
+// ---- hzl::Solver ------------------------------------------------------------------------
+int ref_solver_create(int n, const double *p6, unsigned long long seed, void **out) {
+    return guarded([&] { *out = new hzl::Solver(static_cast<std::size_t>(n), params(p6), seed); });
+}
+void ref_solver_destroy(void *h) { delete static_cast<hzl::Solver *>(h); }
+int ref_solver_initialize(void *h, const char *name) {
+    return guarded([&] { static_cast<hzl::Solver *>(h)->initialize(name); });
+}
+int ref_solver_initialize_physical(void *h, const double *field) {
+    return guarded([&] {
+        auto *s = static_cast<hzl::Solver *>(h);
+        s->initialize_physical(to_field(field, s->size() * s->size()));
+    });
+}
+int ref_solver_step(void *h, double dt, int steps) {
+    return guarded([&] {
+        for (int i = 0; i < steps; ++i)
+            static_cast<hzl::Solver *>(h)->step(dt);
+    });
+}
+int ref_solver_coefficients(void *h, double *out) {
+    return guarded([&] { from_field(static_cast<hzl::Solver *>(h)->coefficients(), out); });
+}
+int ref_solver_forcing(void *h, double *out) {
+    return guarded([&] { from_field(static_cast<hzl::Solver *>(h)->forcing(), out); });
+}
+int ref_solver_midpoint_forcing(void *h, double *out) {
+    return guarded([&] { from_field(static_cast<hzl::Solver *>(h)->midpoint_forcing(), out); });
+}
+int ref_solver_update_latent_state(void *h, const double *w, const double *f) {
+    return guarded([&] {
+        auto *s = static_cast<hzl::Solver *>(h);
+        const auto c = s->size() * s->size();
+        s->update_latent_state(to_field(w, c), to_field(f, c));
+    });
+}
+int ref_solver_diagnostics(void *h, double *out6) {
+    return guarded([&] {
+        const auto d = static_cast<hzl::Solver *>(h)->diagnostics();
+        out6[0] = d.time;
+        out6[1] = d.energy;
+        out6[2] = d.enstrophy;
+        out6[3] = d.dissipation;
+        out6[4] = d.injection;
+        out6[5] = d.cfl_rate;
+    });
+}
+int ref_solver_physical_vorticity(void *h, double *out) {
+    return guarded([&] { from_field(static_cast<hzl::Solver *>(h)->physical_vorticity(), out); });
+}
+int ref_solver_drift(void *h, const double *state, double *out) {
+    return guarded([&] {
+        auto *s = static_cast<hzl::Solver *>(h);
+        from_field(s->drift(to_field(state, s->size() * s->size())), out);
+    });
+}
+int ref_solver_reseed_future(void *h, unsigned long long seed) {
+    return guarded([&] { static_cast<hzl::Solver *>(h)->reseed_future(seed); });
+}
+
+// ---- hzl::ShellForcing ------------------------------------------------------------------
+int ref_shell_forcing_create(int n, const double *p6, unsigned long long seed, void **out) {
+    return guarded(
+        [&] { *out = new hzl::ShellForcing(static_cast<std::size_t>(n), params(p6), seed); });
+}
+void ref_shell_forcing_destroy(void *h) { delete static_cast<hzl::ShellForcing *>(h); }
+int ref_shell_forcing_midpoint_step(void *h, double dt, double *midpoint_out) {
+    return guarded(
+        [&] { from_field(static_cast<hzl::ShellForcing *>(h)->midpoint_step(dt), midpoint_out); });
+}
+int ref_shell_forcing_coefficients(void *h, double *out) {
+    return guarded([&] { from_field(static_cast<hzl::ShellForcing *>(h)->coefficients(), out); });
+}
+
+// ---- hzl::ensemble ----------------------------------------------------------------------
+int ref_ensemble(int n, const double *p6, double dt, unsigned long long steps,
+                 unsigned long long count, unsigned long long workers, unsigned long long seed,
+                 double *out6xcount) {
+    return guarded([&] {
+        const auto r = hzl::ensemble(static_cast<std::size_t>(n), params(p6), dt, steps, count,
+                                     workers, seed);
+        for (std::size_t i = 0; i < r.size(); ++i) {
+            out6xcount[6 * i + 0] = r[i].time;
+            out6xcount[6 * i + 1] = r[i].energy;
+            out6xcount[6 * i + 2] = r[i].enstrophy;
+            out6xcount[6 * i + 3] = r[i].dissipation;
+            out6xcount[6 * i + 4] = r[i].injection;
+            out6xcount[6 * i + 5] = r[i].cfl_rate;
+        }
+    });
+}
+
+// ---- observations -----------------------------------------------------------------------
+// Writes at most `capacity` observations; *count receives the number produced.
+int ref_synthetic_observations(int n, double dt, unsigned long long steps, unsigned long long every,
+                               const double *p6, double noise, unsigned long long seed,
+                               unsigned long long capacity, unsigned long long *count,
+                               unsigned long long *out_steps, unsigned *out_x, unsigned *out_y,
+                               double *out_values, double *out_sd) {
+    return guarded([&] {
+        const auto d = hzl::synthetic_observations(static_cast<std::size_t>(n), dt, steps, every,
+                                                   params(p6), noise, seed);
+        if (d.observations.size() > capacity)
+            throw std::invalid_argument("observation buffer too small");
+        *count = d.observations.size();
+        for (std::size_t i = 0; i < d.observations.size(); ++i) {
+            const auto &o = d.observations[i];
+            out_steps[i] = o.step;
+            out_x[i] = static_cast<unsigned>(o.x);
+            out_y[i] = static_cast<unsigned>(o.y);
+            out_values[i] = o.value;
+            out_sd[i] = o.standard_deviation;
+        }
+    });
+}
+
+// ---- filters ----------------------------------------------------------------------------
+// History arrays: per observation group, (step, increment, ess, max weight) and optionally
+// the mean physical vorticity (n*n complex interleaved).
+int ref_bootstrap_filter(int n, double dt, int stochastic, int fmin, int fmax,
+                         unsigned long long nobs, const unsigned long long *steps,
+                         const unsigned *xs, const unsigned *ys, const double *values,
+                         const double *sds, const double *p6, unsigned long long particles,
+                         unsigned long long seed, int retain, double *loglik,
+                         unsigned long long *resampling_events, unsigned long long capacity,
+                         unsigned long long *groups, double *record4, double *means) {
+    return guarded([&] {
+        const auto d = dataset(static_cast<std::size_t>(n), dt, stochastic, fmin, fmax, nobs, steps,
+                               xs, ys, values, sds);
+        const auto r = hzl::bootstrap_filter(d, params(p6), particles, seed, retain != 0);
+        if (r.history.size() > capacity)
+            throw std::invalid_argument("history buffer too small");
+        *loglik = r.log_likelihood;
+        *resampling_events = r.resampling_events;
+        *groups = r.history.size();
+        for (std::size_t g = 0; g < r.history.size(); ++g) {
+            const auto &h = r.history[g];
+            record4[4 * g + 0] = static_cast<double>(h.step);
+            record4[4 * g + 1] = h.log_likelihood_increment;
+            record4[4 * g + 2] = h.effective_particles;
+            record4[4 * g + 3] = h.maximum_weight;
+            if (retain && means)
+                from_field(h.mean_vorticity, means + 2 * g * static_cast<std::size_t>(n) * n);
+        }
+    });
+}
+
+int ref_enkf(int n, double dt, int stochastic, int fmin, int fmax, unsigned long long nobs,
+             const unsigned long long *steps, const unsigned *xs, const unsigned *ys,
+             const double *values, const double *sds, const double *p6, unsigned long long members,
+             unsigned long long seed, double inflation, double localization,
+             unsigned long long forecast_steps, unsigned long long forecast_every,
+             unsigned long long capacity, unsigned long long *records, double *record4,
+             double *means) {
+    return guarded([&] {
+        const auto d = dataset(static_cast<std::size_t>(n), dt, stochastic, fmin, fmax, nobs, steps,
+                               xs, ys, values, sds);
+        const auto r = hzl::ensemble_kalman_filter(
+            d, params(p6), members, seed, {inflation, localization, forecast_steps, forecast_every});
+        if (r.size() > capacity)
+            throw std::invalid_argument("history buffer too small");
+        *records = r.size();
+        for (std::size_t g = 0; g < r.size(); ++g) {
+            record4[4 * g + 0] = static_cast<double>(r[g].step);
+            record4[4 * g + 1] = r[g].forecast_sensor_rmse;
+            record4[4 * g + 2] = r[g].posterior_spread;
+            record4[4 * g + 3] = r[g].is_forecast ? 1.0 : 0.0;
+            if (means)
+                from_field(r[g].mean_vorticity, means + 2 * g * static_cast<std::size_t>(n) * n);
+        }
+    });
+}
+
+// ---- POD --------------------------------------------------------------------------------
+// snapshots: m fields of `dimension` complex entries; outputs up to max_rank modes.
+int ref_fit_pod(unsigned long long m, unsigned long long dimension, const double *snapshots,
+                unsigned long long max_rank, double fraction, unsigned long long *rank,
+                double *mean, double *modes, double *singular_values, double *captured) {
+    return guarded([&] {
+        std::vector<hzl::Field> s(m);
+        for (std::size_t i = 0; i < m; ++i)
+            s[i] = to_field(snapshots + 2 * i * dimension, dimension);
+        const auto b = hzl::fit_pod(s, max_rank, fraction);
+        *rank = b.modes.size();
+        from_field(b.mean, mean);
+        for (std::size_t j = 0; j < b.modes.size(); ++j) {
+            from_field(b.modes[j], modes + 2 * j * dimension);
+            singular_values[j] = b.singular_values[j];
+        }
+        *captured = b.captured_variance;
+    });
+}
+} // extern "C"

@@ -1,0 +1,243 @@
+"""Parity of the batched B200 RK4 step with the CPU oracle (through the C ABI).
+
+Bars: FP64 relative L2 <= 1e-12 on the vorticity spectrum against the FP64 oracle; the FP32
+path's error against the same oracle is bounded explicitly below.  The reference-physics
+cases (OU forcing uploaded per step, friction) follow the reference's own GPU parity method
+(src/cuda_benchmark.cpp:37-80: host ShellForcing midpoint forcing, rel-L2 gate 1e-9)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import device_synthetic, oracle_synthetic_run, rel_l2
+from oracle.oracle import params6
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+
+
+@pytest.mark.parametrize("n", [8, 16, 32, 64, 128, 256])
+def test_fp64_synthetic_parity(hzlb, oracle, n):
+    members, steps, dt, nu, sigma, seed = 3, 6, 1e-3, 1e-3, 0.05, 7
+    kmax = min(4, (n - 1) // 3)
+    ref, _ = oracle_synthetic_run(oracle, n, members, steps, dt, nu, sigma, seed,
+                                  wavenumber=kmax, noise_kmax=kmax)
+    e = device_synthetic(hzlb, n, members, 8, nu, sigma, seed, wavenumber=kmax, noise_kmax=kmax)
+    e.step(dt, steps)
+    assert e.status() == 0
+    got = e.get_state()
+    for m in range(members):
+        assert rel_l2(got[m], ref[m]) <= FP64_TOL, (n, m, rel_l2(got[m], ref[m]))
+
+
+def test_fp64_512_parity(hzlb, oracle):
+    n, steps, dt, nu, sigma, seed = 512, 2, 5e-4, 2e-4, 0.05, 3
+    ref, _ = oracle_synthetic_run(oracle, n, 1, steps, dt, nu, sigma, seed)
+    e = device_synthetic(hzlb, n, 1, 8, nu, sigma, seed)
+    e.step(dt, steps)
+    assert rel_l2(e.get_state()[0], ref[0]) <= FP64_TOL
+
+
+def test_config0_fp64_1000_steps(hzlb, oracle):
+    """N=64, nu=1e-3, Kolmogorov 0.1 sin(4y), sigma=0.05 EM noise on 1<=|k|<=4, dt=1e-3,
+    1000 steps, GRF initial field: final vorticity and the energy/enstrophy series."""
+    n, steps, dt, nu, sigma, seed = 64, 1000, 1e-3, 1e-3, 0.05, 42
+    ref, series = oracle_synthetic_run(oracle, n, 1, steps, dt, nu, sigma, seed)
+    e = device_synthetic(hzlb, n, 1, 8, nu, sigma, seed)
+    got_series = []
+    for i in range(steps):
+        e.step(dt, 1)
+        if i % 100 == 99:
+            d = e.diagnostics()[0]
+            got_series.append((d[1], d[2]))
+    assert e.status() == 0
+    assert rel_l2(e.get_state()[0], ref[0]) <= FP64_TOL
+    np.testing.assert_allclose(np.array(got_series), series[99::100], rtol=1e-12)
+
+
+def test_fp32_error_against_fp64_oracle(hzlb, oracle):
+    """FP32 path (complex64 spectra): stated error bound against the FP64 oracle."""
+    n, members, steps, dt, nu, sigma, seed = 128, 2, 100, 5e-4, 5e-4, 0.05, 11
+    ref, _ = oracle_synthetic_run(oracle, n, members, steps, dt, nu, sigma, seed)
+    e = device_synthetic(hzlb, n, members, 4, nu, sigma, seed)
+    e.step(dt, steps)
+    got = e.get_state()
+    for m in range(members):
+        err = rel_l2(got[m], ref[m])
+        assert err < 2e-5, err
+        z_ref = np.sum(np.abs(ref[m]) ** 2)
+        z_got = np.sum(np.abs(got[m]) ** 2)
+        assert abs(z_got / z_ref - 1) < 2e-5
+
+
+@pytest.mark.parametrize("precision", [4, 8])
+def test_reference_physics_ou_forcing(hzlb, oracle, reference, precision):
+    """Reference physics (nu, alpha, OU shell forcing frozen at the midpoint) with the forcing
+    generated by the reference's own ShellForcing and uploaded per step, against the
+    reference Solver (cuda_benchmark.cpp:41-80 method)."""
+    n, steps, dt = 32, 10, 0.005
+    p = params6(0.01, 0.1, 0.2, 0.5, 2, 3)
+    solver = reference.solver(n, p, 0)
+    solver.initialize("multimode")
+    initial = solver.coefficients()
+    sf = reference.shell_forcing(n, p, 0)
+    cfg = hzlb.Config(n=n, members=1, precision=precision, nu=0.01, alpha=0.1, forcing_kmax=3,
+                      forcing_per_member=True)
+    e = hzlb.Ensemble(cfg)
+    e.set_state(initial[None])
+    for _ in range(steps):
+        e.set_forcing(sf.midpoint_step(dt)[None])
+        e.step(dt, 1)
+    cpu = reference.solver(n, p, 0)
+    cpu.initialize("multimode")
+    # The reference's CPU Solver draws its own OU path from the same seed (Solver(n, p, 0) and
+    # ShellForcing(n, p, 0) share NormalStream(0), tests/verification.cpp:334-350).
+    cpu.step(dt, steps)
+    tol = 1e-12 if precision == 8 else 1e-5
+    assert rel_l2(e.get_state()[0], cpu.coefficients()) <= tol
+
+
+def test_deterministic_gpu_step_matches_cuda_solver_semantics(hzlb, reference):
+    """CudaSolver::step(dt) with sigma = 0 (cuda_solver.cu:173-183): no forcing."""
+    n, steps, dt = 64, 20, 0.005
+    p = params6(0.001, 0.1, 0.0, 0.5, 2, 3)
+    cpu = reference.solver(n, p, 0)
+    cpu.initialize("multimode")
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=8, nu=0.001, alpha=0.1))
+    e.set_state(cpu.coefficients()[None])
+    e.step(dt, steps)
+    cpu.step(dt, steps)
+    assert rel_l2(e.get_state()[0], cpu.coefficients()) <= FP64_TOL
+
+
+def test_fourier_normalisation_and_physical(hzlb, oracle):
+    """tests/verification.cpp:28-43 on the device observation operator: the physical field of
+    the spectrum of sin(3x) + 0.7 cos(2y) is that field."""
+    n = 32
+    x = np.arange(n)
+    field = (np.sin(3 * 2 * np.pi * x / n)[None, :] + 0.7 * np.cos(2 * 2 * np.pi * x / n)[:, None])
+    spec = oracle.fft(field.astype(np.complex128), inverse=False)
+    assert abs(spec[0, 3] - (0 - 0.5j)) < 1e-14
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=2, precision=8))
+    e.set_state(np.array([spec, 2 * spec]))
+    phys = e.physical()
+    np.testing.assert_allclose(phys[0], field, atol=1e-14)
+    np.testing.assert_allclose(phys[1], 2 * field, atol=1e-14)
+    xs, ys = np.array([0, 5, 31]), np.array([0, 7, 30])
+    np.testing.assert_allclose(e.observe(xs, ys), phys[:, ys, xs], rtol=0, atol=0)
+
+
+def test_taylor_green_decay_order(hzlb, oracle):
+    """tests/verification.cpp:44-65: Taylor-Green decays as exp(-2 (nu k^2 ... )) exactly;
+    RK4 error ratios > 14 when dt halves."""
+    n = 16
+    nu, alpha = 0.7, 0.6
+    s = oracle.solver(n, params6(nu, alpha, 0.0, 0.5, 2, 3), 1)
+    s.initialize("taylor-green")
+    w0 = s.state()[0]
+    exact = w0 * np.exp(-2.0 * 0.4)
+    errors = []
+    for dt in (0.04, 0.02, 0.01):
+        e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=8, nu=nu, alpha=alpha))
+        e.set_state(w0[None])
+        e.step(dt, int(round(0.4 / dt)))
+        errors.append(rel_l2(e.get_state()[0], exact))
+        d = e.diagnostics()[0]
+        assert abs(d[1] / (np.pi ** 2 * np.exp(-4.0 * 0.4)) - 1) < 1e-6
+        assert abs(d[3] - 2 * nu * d[2]) < 1e-13
+    assert errors[0] / errors[1] > 14 and errors[1] / errors[2] > 14
+
+
+@pytest.mark.parametrize("precision,tol", [(8, 1e-9), (4, 2e-5)])
+def test_inviscid_conservation(hzlb, oracle, precision, tol):
+    """tests/verification.cpp:86-108: inviscid multimode flow at N=32 conserves energy and
+    enstrophy (1e-9 in FP64)."""
+    n = 32
+    s = oracle.solver(n, params6(0.0, 0.0, 0.0, 0.5, 2, 3), 1)
+    s.initialize("multimode")
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=precision, nu=0.0, alpha=0.0))
+    e.set_state(s.state()[0][None])
+    before = e.diagnostics()[0]
+    e.step(0.005, 100)
+    after = e.diagnostics()[0]
+    assert abs(after[1] / before[1] - 1) < tol
+    assert abs(after[2] / before[2] - 1) < tol
+
+
+def test_diagnostics_match_oracle(hzlb, oracle):
+    n = 64
+    w = oracle.grf(n, 5, 0)
+    f = oracle.kolmogorov(n)
+    s = oracle.solver(n, params6(1e-3, 0.0, 0.0, 0.5, 1, 4), 0)
+    s.set_state(w, f)
+    ref = s.diagnostics()
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=8, nu=1e-3, forcing_kmax=0))
+    e.set_state(w[None])
+    e.set_forcing(f[None])
+    got = e.diagnostics()[0]
+    np.testing.assert_allclose(got[1:], ref[1:], rtol=1e-12)
+
+
+def test_batch_composition_independence(hzlb):
+    """A member's trajectory does not depend on which other members share the batch
+    (the analogue of the reference's worker-count independence, verification.cpp:160-163)."""
+    n, dt, seed = 64, 1e-3, 9
+    big = device_synthetic(hzlb, n, 6, 4, 1e-3, 0.05, seed)
+    big.step(dt, 5)
+    cfg = hzlb.Config(n=n, members=2, precision=4, nu=1e-3, forcing_kmax=0, noise_sigma=0.05,
+                      seed=seed, member_base=4)
+    small = hzlb.Ensemble(cfg)
+    small.set_state(np.array([hzlb.grf_spectrum(n, seed, m) for m in (4, 5)]))
+    small.set_forcing(hzlb.kolmogorov_forcing(n)[None])
+    small.set_time(0.0, 0)
+    small.step(dt, 5)
+    np.testing.assert_array_equal(small.get_state_compact(), big.get_state_compact(4, 2))
+
+
+def test_cfl_violation_is_flagged(hzlb):
+    n = 32
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=8, nu=0.0))
+    w = hzlb.grf_spectrum(n, 1, 0) * 200.0
+    e.set_state(w[None])
+    e.step(0.05, 1)
+    assert e.status() & hzlb.STATUS_CFL
+
+
+def test_invalid_arguments(hzlb):
+    e = hzlb.Ensemble(hzlb.Config(n=32, members=2, precision=8, nu=1e-3, forcing_kmax=2))
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.step(-1.0, 1)
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.step(float("nan"), 1)
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.step(20.0, 1)   # diffusion limit: dt (2 nu K^2 + alpha) = 20 * 0.2 > 2.5 (K = 10)
+    bad = np.zeros((1, 32, 32), np.complex128)
+    bad[0, 1, 1] = np.nan
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.set_state(bad)
+    asym = np.zeros((1, 32, 32), np.complex128)
+    asym[0, 1, 0] = 1.0   # partner (0, -1) left at zero: not conjugate-symmetric
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.set_forcing(asym)
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.get_state(1, 5)
+
+
+def test_empty_step_and_single_member(hzlb, oracle):
+    n = 16
+    e = device_synthetic(hzlb, n, 1, 8, 1e-3, 0.0, 1)
+    before = e.get_state()
+    e.step(1e-3, 0)
+    np.testing.assert_array_equal(e.get_state(), before)
+
+
+def test_nonfinite_state_flagged(hzlb):
+    n = 16
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=4, nu=0.0))
+    w = hzlb.grf_spectrum(n, 1, 0).astype(np.complex64)
+    compact = hzlb.full_to_compact(w, n).astype(np.complex64)
+    compact[0, 5] = np.inf
+    e.set_state_compact(compact)
+    e.step(1e-4, 1)
+    assert e.status() & hzlb.STATUS_NONFINITE

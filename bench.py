@@ -65,7 +65,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -156,7 +156,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--members", type=int, default=MEMBERS)
@@ -228,8 +228,12 @@ def main():
     K = (N - 1) // 3
     C, LD = K + 1, 2 * K + 1
     cb = 8  # complex64 bytes
-    row_bytes = M * (4 * C * N + C * N) * cb                 # read W (4 fields), write NL
-    col_bytes = M * (C * N + 4 * C * N + 5 * C * LD) * cb    # read NL, write W, state r/w
+    # per launch: row kernel reads the 2 velocity column fields and writes the 2 product fields;
+    # column kernel reads the 2 product fields, writes the 2 velocity fields and reads/writes
+    # the compact state, stage input and accumulator (3, 5, 5, 4 entries per mode on stages
+    # 1-4: 4.25 on average)
+    row_bytes = M * (2 * C * N + 2 * C * N) * cb
+    col_bytes = int(M * (2 * C * N + 2 * C * N + 4.25 * C * LD) * cb)
     row_gbs = row_bytes / (row_ms * 1e-3) / 1e9
     col_gbs = col_bytes / (col_ms * 1e-3) / 1e9
     peak, peak_kind = peaks()

@@ -47,6 +47,38 @@ class hzlb_config(C.Structure):
     ]
 
 
+class hzlb_parameters(C.Structure):
+    _fields_ = [("viscosity", C.c_double), ("friction", C.c_double),
+                ("forcing_sigma", C.c_double), ("forcing_tau", C.c_double),
+                ("forcing_min", C.c_int), ("forcing_max", C.c_int)]
+
+
+class hzlb_observation(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("x", C.c_uint32), ("y", C.c_uint32),
+                ("value", C.c_double), ("standard_deviation", C.c_double)]
+
+
+class hzlb_dataset(C.Structure):
+    _fields_ = [("n", C.c_int), ("dt", C.c_double), ("stochastic", C.c_int),
+                ("forcing_min", C.c_int), ("forcing_max", C.c_int), ("count", C.c_size_t),
+                ("observations", C.POINTER(hzlb_observation))]
+
+
+class hzlb_filter_record(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("log_likelihood_increment", C.c_double),
+                ("effective_particles", C.c_double), ("maximum_weight", C.c_double)]
+
+
+class hzlb_enkf_options(C.Structure):
+    _fields_ = [("inflation", C.c_double), ("localization_radius", C.c_double),
+                ("forecast_steps", C.c_uint64), ("forecast_every", C.c_uint64)]
+
+
+class hzlb_enkf_record(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("forecast_sensor_rmse", C.c_double),
+                ("posterior_spread", C.c_double), ("is_forecast", C.c_int)]
+
+
 class HzlbError(RuntimeError):
     """A failure reported through the C ABI (std::runtime_error in the reference)."""
 
@@ -100,6 +132,19 @@ def library() -> C.CDLL:
         "hzlb_inflate": (C.c_int, [vp, C.c_double]),
         "hzlb_enkf_analysis": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp]),
         "hzlb_grf_spectrum": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, _dp]),
+        "hzlb_run_ensemble": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), C.c_double,
+                                        C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_int,
+                                        _dp]),
+        "hzlb_bootstrap_filter": (C.c_int, [C.POINTER(hzlb_dataset), C.POINTER(hzlb_parameters),
+                                            C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.c_int,
+                                            _dp, C.POINTER(C.c_uint64),
+                                            C.POINTER(hzlb_filter_record), C.c_size_t,
+                                            C.POINTER(C.c_size_t), _dp]),
+        "hzlb_ensemble_kalman_filter": (C.c_int, [C.POINTER(hzlb_dataset),
+                                                  C.POINTER(hzlb_parameters), C.c_uint64,
+                                                  C.c_uint64, C.POINTER(hzlb_enkf_options),
+                                                  C.c_int, C.c_int, C.POINTER(hzlb_enkf_record),
+                                                  C.c_size_t, C.POINTER(C.c_size_t), _dp]),
         "hzlb_kolmogorov_forcing": (C.c_int, [C.c_int, C.c_double, C.c_int, _dp]),
     }
     for name, (res, args) in sig.items():
@@ -364,3 +409,81 @@ def full_to_compact(full: np.ndarray, n: int) -> np.ndarray:
     out = f[:, ypos][:, :, : k + 1].transpose(0, 2, 1).copy()
     out[:, 0, 0] = 0
     return out.reshape(len(f), -1)
+
+
+# ---- drop-ins for the reference's ensemble entry points ------------------------------------
+@dataclass
+class Parameters:
+    """hzl::Parameters (include/hzl/solver.hpp:15-23) with the reference defaults."""
+    viscosity: float = 0.01
+    friction: float = 0.1
+    forcing_sigma: float = 0.2
+    forcing_tau: float = 0.5
+    forcing_min: int = 2
+    forcing_max: int = 3
+
+    def to_c(self) -> hzlb_parameters:
+        return hzlb_parameters(self.viscosity, self.friction, self.forcing_sigma,
+                               self.forcing_tau, self.forcing_min, self.forcing_max)
+
+
+def _dataset_c(ds: dict):
+    count = len(ds["steps"])
+    obs = (hzlb_observation * count)()
+    for i in range(count):
+        obs[i] = hzlb_observation(int(ds["steps"][i]), int(ds["x"][i]), int(ds["y"][i]),
+                                  float(ds["value"][i]), float(ds["sd"][i]))
+    c = hzlb_dataset(ds["n"], ds["dt"], int(ds.get("stochastic", 1)), ds["forcing_min"],
+                     ds["forcing_max"], count, obs)
+    return c, obs
+
+
+def ensemble(n: int, p: Parameters, dt: float, steps: int, count: int, seed: int,
+             precision: int = 8, device: int = 0) -> np.ndarray:
+    """hzl::ensemble (src/inference.cpp:555-590): (count, 6) diagnostics in member order."""
+    out = np.zeros((count, 6))
+    pc = p.to_c()
+    _check(library().hzlb_run_ensemble(n, C.byref(pc), dt, steps, count, seed, precision,
+                                       device, _p(out)))
+    return out
+
+
+def bootstrap_filter(ds: dict, p: Parameters, particles: int, seed: int,
+                     retain_states: bool = True, precision: int = 8, device: int = 0) -> dict:
+    """hzl::bootstrap_filter (src/filter.cpp:38-126)."""
+    dc, keep = _dataset_c(ds)
+    cap = len(np.unique(ds["steps"])) + 1
+    recs = (hzlb_filter_record * cap)()
+    means = np.zeros((cap, ds["n"], ds["n"]), np.complex128)
+    ll, ev, nrec = C.c_double(), C.c_uint64(), C.c_size_t()
+    pc = p.to_c()
+    _check(library().hzlb_bootstrap_filter(
+        C.byref(dc), C.byref(pc), particles, seed, int(retain_states), precision, device,
+        C.byref(ll), C.byref(ev), recs, cap, C.byref(nrec),
+        means.view(np.float64).ctypes.data_as(_dp) if retain_states else None))
+    k = nrec.value
+    rec = np.array([[recs[i].step, recs[i].log_likelihood_increment,
+                     recs[i].effective_particles, recs[i].maximum_weight] for i in range(k)])
+    return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec.reshape(-1, 4),
+                means=means[:k].copy())
+
+
+def ensemble_kalman_filter(ds: dict, p: Parameters, members: int, seed: int,
+                           inflation: float = 1.0, localization_radius: float = 0.0,
+                           forecast_steps: int = 0, forecast_every: int = 1,
+                           precision: int = 8, device: int = 0) -> dict:
+    """hzl::ensemble_kalman_filter (src/filter.cpp:204-356)."""
+    dc, keep = _dataset_c(ds)
+    cap = len(np.unique(ds["steps"])) + forecast_steps + 1
+    recs = (hzlb_enkf_record * cap)()
+    means = np.zeros((cap, ds["n"], ds["n"]), np.complex128)
+    nrec = C.c_size_t()
+    pc = p.to_c()
+    opt = hzlb_enkf_options(inflation, localization_radius, forecast_steps, forecast_every)
+    _check(library().hzlb_ensemble_kalman_filter(
+        C.byref(dc), C.byref(pc), members, seed, C.byref(opt), precision, device, recs, cap,
+        C.byref(nrec), means.view(np.float64).ctypes.data_as(_dp)))
+    k = nrec.value
+    rec = np.array([[recs[i].step, recs[i].forecast_sensor_rmse, recs[i].posterior_spread,
+                     recs[i].is_forecast] for i in range(k)])
+    return dict(records=rec.reshape(-1, 4), means=means[:k].copy())

@@ -42,6 +42,8 @@ void need(const void *p, const char *what) {
 }
 } // namespace
 
+void hzlb::set_last_error(const std::string &message) { last_error = message; }
+
 extern "C" {
 
 const char *hzlb_last_error(void) { return last_error.c_str(); }

@@ -1,0 +1,691 @@
+// Drop-in drivers for the reference's ensemble entry points, on the batched B200 engine:
+//   hzl::ensemble               (src/inference.cpp:555-590)
+//   hzl::bootstrap_filter       (src/filter.cpp:38-126)
+//   hzl::ensemble_kalman_filter (src/filter.cpp:204-356)
+// They keep the reference's semantics exactly: member i's OU forcing draws from
+// NormalStream(stream_seed(seed, i)) (mt19937_64 + Box-Muller), forcing is frozen at the
+// midpoint over the RK4 step (solver.cpp:217-254), the particle filter resamples with
+// mt19937_64(stream_seed(seed, 2^64-1)) and reseeds clones with stream_seed(seed, (g+1)M+i),
+// and the EnKF assimilates scalar observations serially with perturbations from
+// NormalStream(stream_seed(seed, M)).  The OU forcing is a few shell modes per member, so it
+// lives on the host (one batched upload per step); the flow state lives on the device.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <limits>
+#include <random>
+
+namespace hzlb {
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643383279502884;
+using cd = std::complex<double>;
+
+int wave(int i, int n) { return i < n / 2 ? i : i - n; }
+
+// SplitMix64 mix of (base, index): the reference's logical stream identities.
+uint64_t stream_seed(uint64_t base, uint64_t index) {
+    uint64_t x = base + 0x9e3779b97f4a7c15ULL * (index + 1);
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebULL;
+    return x ^ (x >> 31);
+}
+
+// mt19937_64 uniforms ((x >> 11) + 1/2) 2^-53 and Box-Muller with a cached spare.
+class NormalStream {
+  public:
+    explicit NormalStream(uint64_t seed = 0) : engine_(seed) {}
+    double operator()() {
+        if (has_spare_) {
+            has_spare_ = false;
+            return spare_;
+        }
+        const double u1 = (static_cast<double>(engine_() >> 11) + 0.5) * 0x1.0p-53;
+        const double r = std::sqrt(-2 * std::log(u1));
+        const double u2 = (static_cast<double>(engine_() >> 11) + 0.5) * 0x1.0p-53;
+        const double angle = 2 * kPi * u2;
+        spare_ = r * std::sin(angle);
+        has_spare_ = true;
+        return r * std::cos(angle);
+    }
+
+  private:
+    std::mt19937_64 engine_;
+    bool has_spare_ = false;
+    double spare_ = 0;
+};
+
+struct Params {
+    double nu, alpha, sigma, tau;
+    int kmin, kmax;
+};
+void validate_params(int n, const Params &p) {
+    if (!std::isfinite(p.nu) || p.nu < 0 || !std::isfinite(p.alpha) || p.alpha < 0 ||
+        !std::isfinite(p.sigma) || p.sigma < 0 || !std::isfinite(p.tau) || p.tau <= 0)
+        raise(HZLB_EINVAL, "nu, alpha, sigma must be finite and nonnegative; tau must be positive");
+    if (p.kmin < 1 || p.kmax < p.kmin || 3LL * p.kmax >= static_cast<long long>(n))
+        raise(HZLB_EINVAL, "forcing shell must lie strictly inside the dealiased grid");
+}
+
+// Per-member OU shell forcing: the pairs (i < partner) of retained modes with
+// kmin^2 <= |k|^2 <= kmax^2 in the reference's enumeration order (y outer, x inner).
+class OuBank {
+  public:
+    OuBank(int n, const Params &p, int members, uint64_t seed) : n_(n), p_(p), M_(members) {
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                const int a = wave(x, n), b = wave(y, n);
+                const int i = y * n + x, partner = ((n - y) % n) * n + (n - x) % n;
+                const int k2 = a * a + b * b;
+                if (3 * std::abs(a) < n && 3 * std::abs(b) < n && i < partner &&
+                    k2 >= p.kmin * p.kmin && k2 <= p.kmax * p.kmax)
+                    modes_.push_back({a, b});
+            }
+        if (modes_.empty())
+            raise(HZLB_EINVAL, "empty forcing shell");
+        const size_t P = modes_.size();
+        value_.assign(static_cast<size_t>(M_) * P, cd(0, 0));
+        midpoint_.assign(value_.size(), cd(0, 0));
+        streams_.reserve(M_);
+        const double scale = p.sigma * std::sqrt(p.tau / 4);   // stationary draw
+        for (int m = 0; m < M_; ++m) {
+            streams_.emplace_back(stream_seed(seed, m));
+            for (size_t k = 0; k < P; ++k) {
+                const double re = streams_[m](), im = streams_[m]();
+                value_[m * P + k] = scale * cd(re, im);
+            }
+        }
+    }
+    size_t pairs() const { return modes_.size(); }
+    void transition(double h) {
+        const double decay = std::exp(-h / p_.tau),
+                     scale = p_.sigma * std::sqrt(-p_.tau * std::expm1(-2 * h / p_.tau) / 4);
+        const size_t P = modes_.size();
+        for (int m = 0; m < M_; ++m)
+            for (size_t k = 0; k < P; ++k) {
+                const double re = streams_[m](), im = streams_[m]();
+                value_[m * P + k] = decay * value_[m * P + k] + scale * cd(re, im);
+            }
+    }
+    // OU(dt/2), keep the midpoint, OU(dt/2): Solver::step's forcing schedule.
+    void midpoint_step(double dt) {
+        if (!std::isfinite(dt) || dt <= 0)
+            raise(HZLB_EINVAL, "invalid OU transition interval");
+        transition(dt / 2);
+        midpoint_ = value_;
+        transition(dt / 2);
+    }
+    // Compact forcing (columns kx <= kmax) of `which` (midpoint or current), interleaved.
+    void compact(bool midpoint, int cols, std::vector<double> &out) const {
+        const int K = (n_ - 1) / 3, LD = 2 * K + 1;
+        const size_t block = static_cast<size_t>(cols) * LD, P = modes_.size();
+        out.assign(2 * block * M_, 0.0);
+        const auto &src = midpoint ? midpoint_ : value_;
+        for (int m = 0; m < M_; ++m)
+            for (size_t k = 0; k < P; ++k) {
+                int kx = modes_[k].first, ky = modes_[k].second;
+                cd v = src[m * P + k];
+                if (kx < 0 || (kx == 0 && ky < 0)) {   // store the kx >= 0 member of the pair
+                    kx = -kx;
+                    ky = -ky;
+                    v = std::conj(v);
+                }
+                auto put = [&](int kxx, int kyy, cd z) {
+                    const int j = kyy >= 0 ? kyy : kyy + LD;
+                    const size_t at = m * block + static_cast<size_t>(kxx) * LD + j;
+                    out[2 * at] = z.real();
+                    out[2 * at + 1] = z.imag();
+                };
+                put(kx, ky, v);
+                if (kx == 0)
+                    put(0, -ky, std::conj(v));
+            }
+    }
+    void gather(const std::vector<uint32_t> &anc) {
+        const size_t P = modes_.size();
+        std::vector<cd> v(value_.size()), mid(midpoint_.size());
+        for (int i = 0; i < M_; ++i)
+            for (size_t k = 0; k < P; ++k) {
+                v[i * P + k] = value_[anc[i] * P + k];
+                mid[i * P + k] = midpoint_[anc[i] * P + k];
+            }
+        value_.swap(v);
+        midpoint_.swap(mid);
+    }
+    void reseed(int m, uint64_t seed) { streams_[m] = NormalStream(seed); }
+    std::vector<cd> &values() { return value_; }
+    const std::vector<std::pair<int, int>> &modes() const { return modes_; }
+
+  private:
+    int n_;
+    Params p_;
+    int M_;
+    std::vector<std::pair<int, int>> modes_;   // (kx, ky) of the pair's first index
+    std::vector<cd> value_, midpoint_;         // [member][pair]
+    std::vector<NormalStream> streams_;
+};
+
+// 2-D transform in the reference convention (forward scaled by 1/n^2), radix-2 with
+// precomputed roots; used on single fields (ensemble means, covariances).
+void host_fft2(int n, std::vector<cd> &a, bool inverse) {
+    std::vector<cd> roots(n / 2), line(n);
+    for (int i = 0; i < n / 2; ++i)
+        roots[i] = std::polar(1.0, (inverse ? 2.0 : -2.0) * kPi * i / n);
+    int bits = 0;
+    while ((1 << bits) < n)
+        ++bits;
+    auto transform = [&](cd *base, int stride) {
+        for (int i = 0; i < n; ++i) {
+            int r = 0;
+            for (int b = 0; b < bits; ++b)
+                r |= ((i >> b) & 1) << (bits - 1 - b);
+            line[r] = base[static_cast<size_t>(i) * stride];
+        }
+        for (int len = 2; len <= n; len <<= 1)
+            for (int s = 0; s < n; s += len)
+                for (int j = 0; j < len / 2; ++j) {
+                    const cd u = line[s + j], t = roots[j * (n / len)] * line[s + j + len / 2];
+                    line[s + j] = u + t;
+                    line[s + j + len / 2] = u - t;
+                }
+        for (int i = 0; i < n; ++i)
+            base[static_cast<size_t>(i) * stride] = line[i];
+    };
+    for (int y = 0; y < n; ++y)
+        transform(&a[static_cast<size_t>(y) * n], 1);
+    for (int x = 0; x < n; ++x)
+        transform(&a[x], n);
+    if (!inverse)
+        for (auto &z : a)
+            z /= static_cast<double>(n) * n;
+}
+
+// compact interleaved (kx 0..K, j) -> full n*n reference layout with conjugate partners
+std::vector<cd> compact_to_full(int n, const std::vector<double> &c) {
+    const int K = (n - 1) / 3, LD = 2 * K + 1;
+    std::vector<cd> f(static_cast<size_t>(n) * n, cd(0, 0));
+    for (int kx = 0; kx <= K; ++kx)
+        for (int j = 0; j < LD; ++j) {
+            const int ypos = j <= K ? j : n - LD + j;
+            const size_t at = static_cast<size_t>(kx) * LD + j;
+            const cd z(c[2 * at], c[2 * at + 1]);
+            f[static_cast<size_t>(ypos) * n + kx] = z;
+            if (kx > 0)
+                f[static_cast<size_t>((n - ypos) % n) * n + (n - kx)] = std::conj(z);
+        }
+    return f;
+}
+std::vector<double> full_to_compact(int n, const std::vector<cd> &f) {
+    const int K = (n - 1) / 3, LD = 2 * K + 1;
+    std::vector<double> c(2 * static_cast<size_t>(K + 1) * LD);
+    for (int kx = 0; kx <= K; ++kx)
+        for (int j = 0; j < LD; ++j) {
+            const int ypos = j <= K ? j : n - LD + j;
+            const cd z = f[static_cast<size_t>(ypos) * n + kx];
+            const size_t at = static_cast<size_t>(kx) * LD + j;
+            c[2 * at] = z.real();
+            c[2 * at + 1] = z.imag();
+        }
+    c[0] = c[1] = 0;
+    return c;
+}
+
+// The reference's "multimode" initial vorticity (solver.cpp:145-161) as coefficients.
+std::vector<cd> initial_field(int n, const char *name) {
+    std::vector<cd> w(static_cast<size_t>(n) * n);
+    const bool zero = std::strcmp(name, "zero") == 0, mm = std::strcmp(name, "multimode") == 0;
+    for (int y = 0; y < n; ++y)
+        for (int x = 0; x < n; ++x) {
+            const double a = 2 * kPi * x / n, b = 2 * kPi * y / n;
+            double v = zero ? 0.0 : 2 * std::cos(a) * std::cos(b);
+            if (mm)
+                v += 0.6 * std::sin(2 * a + b) + 0.4 * std::cos(a - 3 * b) + 0.3 * std::sin(3 * a + 2 * b);
+            w[static_cast<size_t>(y) * n + x] = v;
+        }
+    host_fft2(n, w, false);
+    return w;
+}
+
+struct Dataset {
+    int n;
+    double dt;
+    int fmin, fmax;
+    std::vector<hzlb_observation> obs;
+};
+Dataset load_dataset(const hzlb_dataset *d) {
+    if (!d || (d->count && !d->observations))
+        raise(HZLB_EINVAL, "invalid observation dataset");
+    Dataset ds{d->n, d->dt, d->forcing_min, d->forcing_max, {}};
+    if (d->n < 16 || d->n > 512 || (d->n & (d->n - 1)) || !std::isfinite(d->dt) || d->dt <= 0 ||
+        d->count == 0)
+        raise(HZLB_EINVAL, "invalid observation dataset");
+    Params p{0.01, 0.1, 0.2, 0.5, d->forcing_min, d->forcing_max};
+    validate_params(d->n, p);
+    ds.obs.assign(d->observations, d->observations + d->count);
+    uint64_t previous = 0;
+    for (const auto &o : ds.obs) {
+        if (o.step < previous || o.x >= static_cast<uint32_t>(d->n) ||
+            o.y >= static_cast<uint32_t>(d->n) || !std::isfinite(o.value) ||
+            !std::isfinite(o.standard_deviation) || o.standard_deviation <= 0)
+            raise(HZLB_EINVAL, "observations must be time ordered, finite, in bounds, and have "
+                               "positive uncertainty");
+        previous = o.step;
+    }
+    return ds;
+}
+
+// An ensemble of reference-physics members on the engine plus their host OU forcing.
+struct RefEnsemble {
+    int n, M;
+    Params p;
+    std::unique_ptr<Engine> engine;
+    OuBank bank;
+    int precision_;
+    std::vector<double> fbuf;
+    RefEnsemble(int n_, const Params &p_, int members, uint64_t seed, int precision, int device)
+        : n(n_), M(members), p(p_), bank(n_, p_, members, seed), precision_(precision) {
+        hzlb_config c{};
+        c.n = n;
+        c.members = M;
+        c.precision = precision;
+        c.nu = p.nu;
+        c.alpha = p.alpha;
+        c.forcing_kmax = p.kmax;
+        c.forcing_per_member = 1;
+        c.device = device;
+        engine = make_engine(c);
+    }
+    void set_initial(const char *name) {
+        const auto w = initial_field(n, name);
+        const auto c = full_to_compact(n, w);
+        std::vector<double> all(c.size() * M);
+        for (int m = 0; m < M; ++m)
+            std::copy(c.begin(), c.end(), all.begin() + m * c.size());
+        if (engine->compact_size() * 2 != c.size())
+            raise(HZLB_ERUNTIME, "compact layout mismatch");
+        upload_compact(all);
+    }
+    void upload_compact(const std::vector<double> &all) {
+        // the engine's compact upload takes its own precision
+        const size_t elems = all.size() / 2;
+        if (precision() == 8) {
+            engine->set_state_compact(all.data(), 0, M);
+            engine->synchronize();
+        } else {
+            std::vector<float> f(2 * elems);
+            for (size_t i = 0; i < 2 * elems; ++i)
+                f[i] = static_cast<float>(all[i]);
+            engine->set_state_compact(f.data(), 0, M);
+            engine->synchronize();
+        }
+    }
+    int precision() const { return precision_; }
+    void step(double dt) {
+        bank.midpoint_step(dt);
+        bank.compact(true, engine->forcing_columns(), fbuf);
+        engine->set_forcing_compact(fbuf.data(), 0, M);
+        engine->step(dt, 1);
+    }
+    void check_status() {
+        const uint32_t s = engine->status();
+        if (s & HZLB_STATUS_NONFINITE)
+            raise(HZLB_ERUNTIME, "nonfinite flow state");
+        if (s & HZLB_STATUS_CFL)
+            raise(HZLB_ERUNTIME, "time step exceeds conservative explicit stability limits; reduce dt");
+    }
+    void upload_current_forcing() {
+        bank.compact(false, engine->forcing_columns(), fbuf);
+        engine->set_forcing_compact(fbuf.data(), 0, M);
+    }
+    std::vector<double> mean() {   // sum of coefficient / M in member order
+        std::vector<double> out(2 * engine->compact_size());
+        engine->member_sum(nullptr, static_cast<double>(M), out.data());
+        return out;
+    }
+};
+
+void validate_dt(int n, const Params &p, double dt) {
+    const int largest = (n - 1) / 3;
+    if (!std::isfinite(dt) || dt <= 0 || dt * (2 * p.nu * largest * largest + p.alpha) > 2.5)
+        raise(HZLB_EINVAL, "invalid time step or diffusion stability limit exceeded");
+}
+
+} // namespace
+} // namespace hzlb
+
+using namespace hzlb;
+
+namespace {
+thread_local std::string driver_error;
+template <class F> int guarded_driver(F &&f) {
+    try {
+        f();
+        return HZLB_OK;
+    } catch (const Error &e) {
+        driver_error = e.what();
+        set_last_error(driver_error);
+        return e.code;
+    } catch (const std::exception &e) {
+        driver_error = e.what();
+        set_last_error(driver_error);
+        return HZLB_ERUNTIME;
+    }
+}
+Params to_params(const hzlb_parameters *p) {
+    if (!p)
+        raise(HZLB_EINVAL, "null parameters");
+    return Params{p->viscosity, p->friction, p->forcing_sigma, p->forcing_tau, p->forcing_min,
+                  p->forcing_max};
+}
+} // namespace
+
+extern "C" {
+
+HZLB_API int hzlb_run_ensemble(int n, const hzlb_parameters *params, double dt, uint64_t steps,
+                               uint64_t count, uint64_t seed, int precision, int device,
+                               double *out) {
+    return guarded_driver([&] {
+        if (count == 0)
+            raise(HZLB_EINVAL, "ensemble count and workers must be positive");
+        if (!out)
+            raise(HZLB_EINVAL, "null output");
+        const Params p = to_params(params);
+        if (n < 8 || n > 512 || (n & (n - 1)))
+            raise(HZLB_EINVAL, "grid must be a power of two between 8 and 512");
+        validate_params(n, p);
+        if (steps)
+            validate_dt(n, p, dt);
+        RefEnsemble e(n, p, static_cast<int>(count), seed, precision, device);
+        e.set_initial("zero");
+        for (uint64_t s = 0; s < steps; ++s)
+            e.step(dt);
+        e.check_status();
+        e.upload_current_forcing();
+        e.engine->diagnostics(out);
+    });
+}
+
+HZLB_API int hzlb_bootstrap_filter(const hzlb_dataset *data, const hzlb_parameters *params,
+                                   uint64_t count, uint64_t seed, int retain_states, int precision,
+                                   int device, double *log_likelihood, uint64_t *resampling_events,
+                                   hzlb_filter_record *records, size_t capacity, size_t *nrecords,
+                                   double *mean_vorticity) {
+    return guarded_driver([&] {
+        if (!log_likelihood || !resampling_events || !nrecords || (capacity && !records))
+            raise(HZLB_EINVAL, "null output");
+        const Dataset ds = load_dataset(data);
+        Params p = to_params(params);
+        p.kmin = ds.fmin;
+        p.kmax = ds.fmax;
+        validate_params(ds.n, p);
+        if (count < 2)
+            raise(HZLB_EINVAL, "particle filter needs at least two particles");
+        validate_dt(ds.n, p, ds.dt);
+        const int M = static_cast<int>(count), n = ds.n;
+        RefEnsemble e(n, p, M, seed, precision, device);
+        e.set_initial("multimode");
+        std::vector<double> weights(M, 1 / static_cast<double>(M)), logs(M), w(M);
+        std::mt19937_64 resampling(stream_seed(seed, std::numeric_limits<uint64_t>::max()));
+        double ll = 0;
+        uint64_t events = 0;
+        size_t nrec = 0, current = 0, begin = 0, group = 0;
+        const size_t nn = static_cast<size_t>(n) * n;
+        while (begin < ds.obs.size()) {
+            const uint64_t target = ds.obs[begin].step;
+            size_t end = begin;
+            while (end < ds.obs.size() && ds.obs[end].step == target)
+                ++end;
+            for (uint64_t s = current; s < target; ++s)
+                e.step(ds.dt);
+            e.check_status();
+            // log-weights (filter.cpp:65-75)
+            const size_t p_count = end - begin;
+            std::vector<uint32_t> xs(p_count), ys(p_count);
+            for (size_t o = 0; o < p_count; ++o) {
+                xs[o] = ds.obs[begin + o].x;
+                ys[o] = ds.obs[begin + o].y;
+            }
+            std::vector<double> field(static_cast<size_t>(M) * p_count);
+            e.engine->observe(xs.data(), ys.data(), p_count, field.data());
+            const double half_log_two_pi = 0.5 * std::log(2 * kPi);
+            for (int i = 0; i < M; ++i) {
+                double value = weights[i] > 0 ? std::log(weights[i])
+                                              : -std::numeric_limits<double>::infinity();
+                for (size_t o = 0; o < p_count; ++o) {
+                    const auto &ob = ds.obs[begin + o];
+                    const double residual = (field[i * p_count + o] - ob.value) / ob.standard_deviation;
+                    value -= 0.5 * residual * residual + std::log(ob.standard_deviation) +
+                             half_log_two_pi;
+                }
+                logs[i] = value;
+            }
+            double maximum = logs[0];
+            for (int i = 1; i < M; ++i)
+                if (maximum < logs[i])
+                    maximum = logs[i];
+            if (!std::isfinite(maximum)) {
+                ll = -std::numeric_limits<double>::infinity();
+                break;
+            }
+            double inc = 0, ess = 0, mw = 0;
+            pf_weights_host(logs.data(), M, w.data(), &inc, &ess, &mw);
+            weights = w;
+            ll += inc;
+            if (nrec < capacity) {
+                records[nrec] = {target, inc, ess, mw};
+                if (retain_states && mean_vorticity) {
+                    std::vector<double> mean(2 * e.engine->compact_size());
+                    e.engine->member_sum(weights.data(), 0.0, mean.data());
+                    auto full = compact_to_full(n, mean);
+                    host_fft2(n, full, true);
+                    std::memcpy(mean_vorticity + 2 * nrec * nn, full.data(), sizeof(cd) * nn);
+                }
+            }
+            ++nrec;
+            if (ess < static_cast<double>(M) / 2 && end < ds.obs.size()) {
+                const double u = static_cast<double>(resampling() >> 11) * 0x1.0p-53;
+                std::vector<uint32_t> anc(M);
+                e.engine->resample(weights.data(), M, u, anc.data());
+                e.engine->gather(anc.data());
+                e.bank.gather(anc);
+                for (int i = 0; i < M; ++i)
+                    e.bank.reseed(i, stream_seed(seed, (group + 1) * count + i));
+                std::fill(weights.begin(), weights.end(), 1 / static_cast<double>(M));
+                ++events;
+            }
+            current = target;
+            begin = end;
+            ++group;
+        }
+        *log_likelihood = ll;
+        *resampling_events = events;
+        *nrecords = std::min(nrec, capacity);
+    });
+}
+
+HZLB_API int hzlb_ensemble_kalman_filter(const hzlb_dataset *data, const hzlb_parameters *params,
+                                         uint64_t count, uint64_t seed,
+                                         const hzlb_enkf_options *options, int precision,
+                                         int device, hzlb_enkf_record *records, size_t capacity,
+                                         size_t *nrecords, double *mean_vorticity) {
+    return guarded_driver([&] {
+        if (!nrecords || (capacity && !records))
+            raise(HZLB_EINVAL, "null output");
+        const Dataset ds = load_dataset(data);
+        const hzlb_enkf_options opt = options ? *options : hzlb_enkf_options{1.0, 0.0, 0, 1};
+        if (count < 2)
+            raise(HZLB_EINVAL, "EnKF requires at least two ensemble members");
+        if (!std::isfinite(opt.inflation) || opt.inflation < 1 ||
+            !std::isfinite(opt.localization_radius) || opt.localization_radius < 0)
+            raise(HZLB_EINVAL, "EnKF inflation must be >= 1 and localization radius nonnegative");
+        if (opt.forecast_every == 0)
+            raise(HZLB_EINVAL, "EnKF forecast output interval must be positive");
+        Params p = to_params(params);
+        p.kmin = ds.fmin;
+        p.kmax = ds.fmax;
+        validate_params(ds.n, p);
+        validate_dt(ds.n, p, ds.dt);
+        const int M = static_cast<int>(count), n = ds.n;
+        const size_t nn = static_cast<size_t>(n) * n;
+        RefEnsemble e(n, p, M, seed, precision, device);
+        e.set_initial("multimode");
+        NormalStream perturbations(stream_seed(seed, count));
+        size_t nrec = 0;
+        auto emit = [&](uint64_t step, double rmse, double spread, bool forecast) {
+            if (nrec < capacity) {
+                records[nrec] = {step, rmse, spread, forecast ? 1 : 0};
+                if (mean_vorticity) {
+                    auto full = compact_to_full(n, e.mean());
+                    host_fft2(n, full, true);
+                    std::memcpy(mean_vorticity + 2 * nrec * nn, full.data(), sizeof(cd) * nn);
+                }
+            }
+            ++nrec;
+        };
+        auto spread = [&]() {
+            const auto mean = e.mean();
+            return std::sqrt(e.engine->spread(mean.data()) / static_cast<double>(M - 1));
+        };
+        auto& vals = e.bank.values();
+        const size_t P = e.bank.pairs();
+        uint64_t step = 0;
+        size_t begin = 0;
+        while (begin < ds.obs.size()) {
+            const uint64_t target = ds.obs[begin].step;
+            size_t end = begin;
+            while (end < ds.obs.size() && ds.obs[end].step == target)
+                ++end;
+            for (uint64_t s = step; s < target; ++s)
+                e.step(ds.dt);
+            e.check_status();
+            if (opt.inflation > 1) {   // filter.cpp:237-253
+                e.engine->inflate(opt.inflation);
+                e.engine->symmetrize();
+                for (size_t k = 0; k < P; ++k) {
+                    cd mean(0, 0);
+                    for (int m = 0; m < M; ++m)
+                        mean += vals[m * P + k] / static_cast<double>(M);
+                    for (int m = 0; m < M; ++m)
+                        vals[m * P + k] = mean + opt.inflation * (vals[m * P + k] - mean);
+                }
+            }
+            // forecast sensor RMSE from the mean state, before any update (filter.cpp:254-264)
+            double forecast_error = 0;
+            {
+                auto full = compact_to_full(n, e.mean());
+                host_fft2(n, full, true);
+                for (size_t o = begin; o < end; ++o) {
+                    const double d = full[static_cast<size_t>(ds.obs[o].y) * n + ds.obs[o].x].real() -
+                                     ds.obs[o].value;
+                    forecast_error += d * d;
+                }
+            }
+            for (size_t o = begin; o < end; ++o) {   // serial scalar updates (filter.cpp:265-321)
+                const auto &ob = ds.obs[o];
+                std::vector<double> pred(M);
+                e.engine->observe(&ob.x, &ob.y, 1, pred.data());
+                double mean_prediction = 0;
+                for (int i = 0; i < M; ++i)
+                    mean_prediction += pred[i] / static_cast<double>(M);
+                double variance = 0;
+                std::vector<double> d(M);
+                for (int i = 0; i < M; ++i) {
+                    const double delta = pred[i] - mean_prediction;
+                    variance += delta * delta / static_cast<double>(M - 1);
+                    d[i] = delta / static_cast<double>(M - 1);
+                }
+                // forcing cross-covariance on the host (shell pairs only)
+                std::vector<cd> fcov(P, cd(0, 0));
+                for (size_t k = 0; k < P; ++k) {
+                    cd mean(0, 0);
+                    for (int m = 0; m < M; ++m)
+                        mean += vals[m * P + k] / static_cast<double>(M);
+                    for (int m = 0; m < M; ++m)
+                        fcov[k] += (vals[m * P + k] - mean) * d[m];
+                }
+                std::vector<double> cov;
+                if (opt.localization_radius > 0) {
+                    cov.resize(2 * e.engine->compact_size());
+                    e.engine->covariance(d.data(), cov.data());
+                    // Gaspari-Cohn taper in physical space (filter.cpp:25-36, 290-308)
+                    auto full = compact_to_full(n, cov);
+                    host_fft2(n, full, true);
+                    std::vector<cd> ffull(nn, cd(0, 0));
+                    for (size_t k = 0; k < P; ++k) {
+                        const auto [kx, ky] = e.bank.modes()[k];
+                        const int x = (kx + n) % n, y = (ky + n) % n;
+                        ffull[static_cast<size_t>(y) * n + x] = fcov[k];
+                        ffull[static_cast<size_t>((n - y) % n) * n + (n - x) % n] = std::conj(fcov[k]);
+                    }
+                    host_fft2(n, ffull, true);
+                    const double radius = opt.localization_radius;
+                    auto gc = [&](double dist) {
+                        const double x = dist / radius;
+                        if (x >= 2)
+                            return 0.0;
+                        if (x <= 1)
+                            return 1 - 5.0 / 3 * x * x + 5.0 / 8 * x * x * x + 0.5 * std::pow(x, 4) -
+                                   0.25 * std::pow(x, 5);
+                        return 4 - 5 * x + 5.0 / 3 * x * x + 5.0 / 8 * x * x * x - 0.5 * std::pow(x, 4) +
+                               std::pow(x, 5) / 12 - 2.0 / (3 * x);
+                    };
+                    for (int y = 0; y < n; ++y)
+                        for (int x = 0; x < n; ++x) {
+                            const int ax = std::abs(x - static_cast<int>(ob.x)),
+                                      ay = std::abs(y - static_cast<int>(ob.y));
+                            const double dx = std::min(ax, n - ax), dy = std::min(ay, n - ay);
+                            const double taper = gc(std::hypot(dx, dy));
+                            full[static_cast<size_t>(y) * n + x] *= taper;
+                            ffull[static_cast<size_t>(y) * n + x] *= taper;
+                        }
+                    host_fft2(n, full, false);
+                    host_fft2(n, ffull, false);
+                    // update_latent_state averages each pair with its conjugate partner
+                    for (int y = 0; y < n; ++y)
+                        for (int x = 1; x < n / 2; ++x) {
+                            const size_t i = static_cast<size_t>(y) * n + x,
+                                         j = static_cast<size_t>((n - y) % n) * n + (n - x);
+                            full[i] = 0.5 * (full[i] + std::conj(full[j]));
+                        }
+                    cov = full_to_compact(n, full);
+                    // forcing: restricted to the shell pairs and symmetrised by update_latent_state
+                    for (size_t k = 0; k < P; ++k) {
+                        const auto [kx, ky] = e.bank.modes()[k];
+                        const int x = (kx + n) % n, y = (ky + n) % n;
+                        const cd a = ffull[static_cast<size_t>(y) * n + x],
+                                 b = ffull[static_cast<size_t>((n - y) % n) * n + (n - x) % n];
+                        fcov[k] = 0.5 * (a + std::conj(b));
+                    }
+                } else {
+                    e.engine->covariance(d.data(), nullptr);
+                }
+                const double denominator = variance + ob.standard_deviation * ob.standard_deviation;
+                std::vector<double> innov(M);
+                for (int i = 0; i < M; ++i)
+                    innov[i] = (ob.value + ob.standard_deviation * perturbations() - pred[i]) / denominator;
+                e.engine->rank1(cov.empty() ? nullptr : cov.data(), innov.data());
+                e.engine->symmetrize();
+                // forcing update, then update_latent_state's pair symmetrisation
+                for (int m = 0; m < M; ++m)
+                    for (size_t k = 0; k < P; ++k)
+                        vals[m * P + k] += fcov[k] * innov[m];
+            }
+            emit(target, std::sqrt(forecast_error / static_cast<double>(end - begin)), spread(), false);
+            step = target;
+            begin = end;
+        }
+        for (uint64_t h = 1; h <= opt.forecast_steps; ++h) {   // filter.cpp:337-354
+            e.step(ds.dt);
+            if (h % opt.forecast_every != 0 && h != opt.forecast_steps)
+                continue;
+            e.check_status();
+            emit(step + h, std::numeric_limits<double>::quiet_NaN(), spread(), true);
+        }
+        *nrecords = std::min(nrec, capacity);
+    });
+}
+
+} // extern "C"

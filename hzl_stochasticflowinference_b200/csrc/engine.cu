@@ -46,8 +46,8 @@ template <typename R> class EngineT final : public Engine {
         omega_.ensure(cb * compact_ * M_, "allocate GPU state");
         ystage_.ensure(cb * compact_ * M_, "allocate GPU stage input");
         acc_.ensure(cb * compact_ * M_, "allocate GPU RK accumulator");
-        w_.ensure(cb * 4 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU derivative columns");
-        nl_.ensure(cb * C_ * static_cast<size_t>(n_) * M_, "allocate GPU Jacobian rows");
+        w_.ensure(cb * 2 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU velocity columns");
+        nl_.ensure(cb * 2 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU product rows");
         if (fcount_)
             forcing_.ensure(cb * static_cast<size_t>(fcols_) * LD_ * fcount_, "allocate GPU forcing");
         ctl_.ensure(sizeof(StepControl), "allocate step control");
@@ -68,6 +68,9 @@ template <typename R> class EngineT final : public Engine {
     }
     ~EngineT() override {
         drop_graphs();
+        for (auto &e : fevent_)
+            if (e)
+                cudaEventDestroy(e);
         if (stream_)
             cudaStreamDestroy(stream_);
     }
@@ -75,6 +78,101 @@ template <typename R> class EngineT final : public Engine {
     size_t compact_size() const override { return compact_; }
     int members() const override { return M_; }
     void *stream() const override { return stream_; }
+    int forcing_columns() const override { return fcols_; }
+
+    // ---- reference-order filter building blocks -----------------------------------
+    int grid_for(size_t elems) const {
+        return static_cast<int>(std::min<size_t>((elems + 255) / 256, 2048));
+    }
+    void member_sum(const double *w, double divisor, double *out) override {
+        aux_.ensure(sizeof(double) * (2 * compact_ + M_), "allocate member sum");
+        double *dout = aux_.as<double>(), *dw = dout + 2 * compact_;
+        if (divisor <= 0)
+            cuda_check(cudaMemcpyAsync(dw, w, sizeof(double) * M_, cudaMemcpyHostToDevice, stream_),
+                       "upload weights");
+        member_sum_kernel<R><<<grid_for(compact_), 256, 0, stream_>>>(
+            omega_.as<cx<R>>(), dw, divisor, static_cast<long long>(compact_), M_, dout);
+        cuda_check(cudaGetLastError(), "launch member sum");
+        cuda_check(cudaMemcpyAsync(out, dout, sizeof(double) * 2 * compact_, cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "download member sum");
+        cuda_check(cudaStreamSynchronize(stream_), "member sum");
+    }
+    void covariance(const double *d, double *cov_out) override {
+        aux_.ensure(sizeof(double) * (2 * compact_ + M_), "allocate covariance");
+        double *dcov = aux_.as<double>(), *dd = dcov + 2 * compact_;
+        cuda_check(cudaMemcpyAsync(dd, d, sizeof(double) * M_, cudaMemcpyHostToDevice, stream_),
+                   "upload covariance weights");
+        member_covariance_kernel<R><<<grid_for(compact_), 256, 0, stream_>>>(
+            omega_.as<cx<R>>(), dd, static_cast<long long>(compact_), M_, dcov);
+        cuda_check(cudaGetLastError(), "launch covariance");
+        if (cov_out) {
+            cuda_check(cudaMemcpyAsync(cov_out, dcov, sizeof(double) * 2 * compact_,
+                                       cudaMemcpyDeviceToHost, stream_),
+                       "download covariance");
+            cuda_check(cudaStreamSynchronize(stream_), "covariance");
+        }
+    }
+    void rank1(const double *cov, const double *innov) override {
+        aux_.ensure(sizeof(double) * (2 * compact_ + M_), "allocate covariance");
+        double *dcov = aux_.as<double>(), *dinn = dcov + 2 * compact_;
+        if (cov)
+            cuda_check(cudaMemcpyAsync(dcov, cov, sizeof(double) * 2 * compact_,
+                                       cudaMemcpyHostToDevice, stream_),
+                       "upload covariance");
+        cuda_check(cudaMemcpyAsync(dinn, innov, sizeof(double) * M_, cudaMemcpyHostToDevice, stream_),
+                   "upload innovations");
+        const dim3 grid(std::max(1, std::min(grid_for(compact_), 64)), M_);
+        rank1_update<R><<<grid, 256, 0, stream_>>>(omega_.as<cx<R>>(), dcov, dinn,
+                                                  static_cast<long long>(compact_), M_);
+        cuda_check(cudaGetLastError(), "launch rank-1 update");
+        cuda_check(cudaStreamSynchronize(stream_), "rank-1 update");
+        w_valid_ = false;
+    }
+    void symmetrize() override {
+        symmetrize_column0<R><<<M_, 64, 0, stream_>>>(omega_.as<cx<R>>(), n_, M_);
+        cuda_check(cudaGetLastError(), "launch symmetrisation");
+        w_valid_ = false;
+    }
+    double spread(const double *mean) override {
+        aux_.ensure(sizeof(double) * (2 * compact_ + 1), "allocate spread");
+        double *dmean = aux_.as<double>(), *dout = dmean + 2 * compact_;
+        cuda_check(cudaMemcpyAsync(dmean, mean, sizeof(double) * 2 * compact_, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "upload mean");
+        cuda_check(cudaMemsetAsync(dout, 0, sizeof(double), stream_), "clear spread");
+        spread_sum<R><<<grid_for(compact_), 256, 0, stream_>>>(
+            omega_.as<cx<R>>(), dmean, static_cast<long long>(compact_), LD_, M_, dout);
+        cuda_check(cudaGetLastError(), "launch spread");
+        double v = 0;
+        cuda_check(cudaMemcpyAsync(&v, dout, sizeof(double), cudaMemcpyDeviceToHost, stream_),
+                   "download spread");
+        cuda_check(cudaStreamSynchronize(stream_), "spread");
+        return v;
+    }
+    // Double-buffered pinned upload of per-member forcing in the compact layout (columns
+    // kx < forcing_columns); the host may prepare the next step's forcing while this one runs.
+    void set_forcing_compact(const double *compact, int first, int count) override {
+        if (fcount_ == 0)
+            raise(HZLB_EINVAL, "ensemble was created without forcing");
+        if (first < 0 || count < 0 || first + count > fcount_)
+            raise(HZLB_EINVAL, "forcing member range out of bounds");
+        const size_t block = static_cast<size_t>(fcols_) * LD_, elems = block * count;
+        const int b = fbuf_next_;
+        fbuf_next_ ^= 1;
+        if (!fevent_[b])
+            cuda_check(cudaEventCreateWithFlags(&fevent_[b], cudaEventDisableTiming), "create event");
+        else
+            cuda_check(cudaEventSynchronize(fevent_[b]), "wait for forcing staging");
+        fstage_[b].ensure(sizeof(cx<R>) * elems);
+        cx<R> *st = fstage_[b].as<cx<R>>();
+        for (size_t i = 0; i < elems; ++i)
+            st[i] = mk<R>(static_cast<R>(compact[2 * i]), static_cast<R>(compact[2 * i + 1]));
+        cuda_check(cudaMemcpyAsync(forcing_.as<cx<R>>() + static_cast<size_t>(first) * block, st,
+                                   sizeof(cx<R>) * elems, cudaMemcpyHostToDevice, stream_),
+                   "midpoint forcing upload");
+        cuda_check(cudaEventRecord(fevent_[b], stream_), "record forcing upload");
+    }
 
     // ---- state I/O ----------------------------------------------------------------
     void check_range(int first, int count) const {
@@ -560,8 +658,10 @@ template <typename R> class EngineT final : public Engine {
     size_t compact_ = 0;
     cudaStream_t stream_ = nullptr;
     DeviceBuffer omega_, ystage_, acc_, w_, nl_, forcing_, ctl_, tw_, phys_, scratch_d_, vbits_,
-        obs_xy_, obs_, anc_, enkf_;
-    PinnedBuffer staging_;
+        obs_xy_, obs_, anc_, enkf_, aux_;
+    PinnedBuffer staging_, fstage_[2];
+    cudaEvent_t fevent_[2] = {nullptr, nullptr};
+    int fbuf_next_ = 0;
     std::vector<Graph> graphs_;
     bool w_valid_ = false;
 };

@@ -88,6 +88,15 @@ class Engine {
     virtual size_t compact_size() const = 0;
     virtual int members() const = 0;
     virtual void *stream() const = 0;
+    // building blocks of the reference-order filter drivers (drivers.cu); compact fields cross
+    // as interleaved doubles
+    virtual void member_sum(const double *w, double divisor, double *out) = 0;
+    virtual void covariance(const double *d, double *cov_out) = 0;
+    virtual void rank1(const double *cov, const double *innov) = 0;
+    virtual void symmetrize() = 0;
+    virtual double spread(const double *mean) = 0;
+    virtual void set_forcing_compact(const double *compact, int first, int count) = 0;
+    virtual int forcing_columns() const = 0;
     virtual void step_profiled(double dt, uint64_t nsteps, double *row_ms, double *col_ms) = 0;
 
     double time = 0;
@@ -96,6 +105,9 @@ class Engine {
 };
 
 std::unique_ptr<Engine> make_engine(const hzlb_config &c);
+
+// Message returned by hzlb_last_error() on this thread.
+void set_last_error(const std::string &message);
 
 // Host-side reference-order particle weights and systematic resampling (filter.cpp:76-112).
 void pf_weights_host(const double *logs, size_t count, double *w, double *inc, double *ess,

@@ -228,3 +228,100 @@ __global__ void anomaly_update(const cx<R> *x, const cx<R> *mean, const double *
 }
 
 } // namespace hzlb
+
+namespace hzlb {
+// out[e] = sum over members (in member order) of w[m] x[m][e], or of x[m][e] / divisor when
+// divisor > 0 (the reference's mean accumulates coefficient / count, filter.cpp:238-243).
+template <typename R>
+__global__ void member_sum_kernel(const cx<R> *x, const double *w, double divisor, long long block,
+                           int members, double *out) {
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x) {
+        double sr = 0, si = 0;
+        for (int m = 0; m < members; ++m) {
+            const cx<R> v = x[static_cast<size_t>(m) * block + e];
+            if (divisor > 0) {
+                sr += static_cast<double>(v.x) / divisor;
+                si += static_cast<double>(v.y) / divisor;
+            } else {
+                sr += w[m] * static_cast<double>(v.x);
+                si += w[m] * static_cast<double>(v.y);
+            }
+        }
+        out[2 * e] = sr;
+        out[2 * e + 1] = si;
+    }
+}
+// cov[e] = sum_m (x[m][e] - mean[e]) d[m], mean[e] = sum_m x[m][e] / M (filter.cpp:272-288).
+template <typename R>
+__global__ void member_covariance_kernel(const cx<R> *x, const double *d, long long block, int members,
+                                  double *cov) {
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x) {
+        double mr = 0, mi = 0;
+        for (int m = 0; m < members; ++m) {
+            const cx<R> v = x[static_cast<size_t>(m) * block + e];
+            mr += static_cast<double>(v.x) / members;
+            mi += static_cast<double>(v.y) / members;
+        }
+        double cr = 0, ci = 0;
+        for (int m = 0; m < members; ++m) {
+            const cx<R> v = x[static_cast<size_t>(m) * block + e];
+            cr += (static_cast<double>(v.x) - mr) * d[m];
+            ci += (static_cast<double>(v.y) - mi) * d[m];
+        }
+        cov[2 * e] = cr;
+        cov[2 * e + 1] = ci;
+    }
+}
+// x[m][e] += cov[e] innov[m]   (filter.cpp:314-318)
+template <typename R>
+__global__ void rank1_update(cx<R> *x, const double *cov, const double *innov, long long block,
+                             int members) {
+    const int m = blockIdx.y;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x) {
+        cx<R> &v = x[static_cast<size_t>(m) * block + e];
+        v.x = static_cast<R>(static_cast<double>(v.x) + cov[2 * e] * innov[m]);
+        v.y = static_cast<R>(static_cast<double>(v.y) + cov[2 * e + 1] * innov[m]);
+    }
+}
+// Conjugate symmetry of the kx = 0 column (Solver::update_latent_state, solver.cpp:417-424):
+// w(0, ky) <- (w(0, ky) + conj w(0, -ky)) / 2 for ky > 0, w(0, -ky) <- conj w(0, ky).
+template <typename R> __global__ void symmetrize_column0(cx<R> *x, int n, int members) {
+    const int K = (n - 1) / 3, LD = 2 * K + 1;
+    const size_t block = static_cast<size_t>(K + 1) * LD;
+    const int m = blockIdx.x;
+    for (int ky = 1 + threadIdx.x; ky <= K; ky += blockDim.x) {
+        cx<R> &a = x[m * block + ky], &b = x[m * block + (LD - ky)];
+        const double re = 0.5 * (static_cast<double>(a.x) + static_cast<double>(b.x));
+        const double im = 0.5 * (static_cast<double>(a.y) - static_cast<double>(b.y));
+        a.x = static_cast<R>(re);
+        a.y = static_cast<R>(im);
+        b.x = static_cast<R>(re);
+        b.y = static_cast<R>(-im);
+    }
+}
+// sum over members and retained modes of |x - mean|^2 with Hermitian multiplicity (kx = 0
+// column once, kx > 0 twice): the reference's spread numerator (filter.cpp:326-330).
+template <typename R>
+__global__ void spread_sum(const cx<R> *x, const double *mean, long long block, int ld, int members,
+                           double *out) {
+    double s = 0;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const double mult = e < ld ? 1.0 : 2.0;
+        for (int m = 0; m < members; ++m) {
+            const cx<R> v = x[static_cast<size_t>(m) * block + e];
+            const double dr = static_cast<double>(v.x) - mean[2 * e],
+                         di = static_cast<double>(v.y) - mean[2 * e + 1];
+            s += mult * (dr * dr + di * di);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0)
+        atomicAdd(out, s);
+}
+} // namespace hzlb

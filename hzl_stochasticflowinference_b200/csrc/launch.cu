@@ -8,9 +8,8 @@ namespace {
 
 template <typename R, int N> struct L {
     using G = Cfg<R, N>;
-    static constexpr size_t col_smem = sizeof(cx<R>) * (N + G::LPB * G::BUF);
-    static constexpr size_t row_smem =
-        sizeof(cx<R>) * (N + 4 * G::TY * G::SC + G::C * (G::TY + 1) + G::GROUPS * G::BUF);
+    static constexpr size_t col_smem = hzlb::column_smem<R, N>();
+    static constexpr size_t row_smem = hzlb::row_smem<R, N>();
     static constexpr size_t prow_smem = sizeof(cx<R>) * (N + G::GROUPS * G::BUF);
     static_assert(row_smem <= 227 * 1024, "row kernel shared memory");
 

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     }
 }
 
-// max over the grid of |u| + |v| per member from the derivative columns W (fields 0, 1),
+// max over the grid of |u| + |v| per member from the velocity columns W (fields 0, 1),
 // written as the bit pattern of a nonnegative double (monotone as an unsigned integer).
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     __syncthreads();
     const int g = threadIdx.x / T, t = threadIdx.x % T, m = blockIdx.x;
     const bool active = g < TY / 2;
-    const cx<R> *u = w + static_cast<size_t>(m) * 4 * C * N, *v = u + static_cast<size_t>(C) * N;
+    const cx<R> *u = w + static_cast<size_t>(m) * 2 * C * N, *v = u + static_cast<size_t>(C) * N;
     double best = 0;
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {

@@ -3,18 +3,26 @@
 // restating the math of the reference's Solver::rhs/step (src/solver.cpp:177-254) and
 // CudaSolver (src/cuda_solver.cu:26-84, 203-218) for thousands of members at once.
 //
+// The advection term is evaluated in Basdevant's form for 2-D incompressible flow,
+//   u.grad(w) = d2/dxdy (v^2 - u^2) + (d2/dx2 - d2/dy2)(u v),
+// i.e. A^(k) = -kx ky F[v^2 - u^2] - (kx^2 - ky^2) F[u v].  With the strict 2/3 truncation the
+// products are alias-free on the retained modes, so this equals the reference's
+// F[u wx + v wy] there (to roundoff) while needing four real transforms per stage instead of
+// five: inverse u, v (one packed complex transform per row) and forward v^2 - u^2, u v (one
+// packed complex transform per row).
+//
 // One RK stage is two kernels:
-//   column kernel  (per member x kx column): forward column FFT of the row kernel's Jacobian
-//                  spectrum, RK stage epilogue (dealias mask, viscosity/friction, forcing,
-//                  accumulator, noise on the last stage), then the spectral derivatives
-//                  u^, v^, wx^, wy^ of the next stage input and their inverse column FFTs;
-//   row kernel     (per member x tile of y rows): packed inverse row FFTs (u + i v and
-//                  wx + i wy), the product u wx + v wy, CFL check on stage 1, and a paired
-//                  forward row FFT (rows y and y+1 packed) keeping kx = 0..K.
+//   column kernel  (per member x kx column): forward column FFTs of the two product spectra,
+//                  RK stage epilogue (dealias mask, viscosity/friction, forcing, accumulator,
+//                  noise on the last stage), then u^ = i ky psi^, v^ = -i kx psi^ of the next
+//                  stage input and their inverse column FFTs;
+//   row kernel     (per member x tile of y rows): inverse row FFT of u + i v, the products
+//                  v^2 - u^2 and u v, the CFL check on stage 1, and the forward row FFT of
+//                  (v^2 - u^2) + i (u v), keeping kx = 0..K of each.
 // HBM layouts (complex R):
 //   state / stage input / accumulator  [m][kx][j]          (K+1) x (2K+1) per member
-//   derivative columns W               [m][field][kx][y]   4 x (K+1) x N
-//   Jacobian rows NL                   [m][kx][y]          (K+1) x N
+//   velocity columns W                 [m][field][kx][y]   2 x (K+1) x N   (u^, v^)
+//   product rows NL                    [m][field][kx][y]   2 x (K+1) x N   (v^2-u^2, u v)
 #pragma once
 #include "fft.cuh"
 
@@ -29,9 +37,9 @@ template <typename R, int N> struct Cfg {
     static constexpr int LD = 2 * K + 1;     // compact column length
     static constexpr int LPB = T >= 64 ? 1 : 64 / T;  // column lines per block
     static constexpr int COL_THREADS = LPB * T;
-    static constexpr int TY_RAW = 256 / T;   // rows per row-kernel block
-    static constexpr int TY = TY_RAW > N ? N : TY_RAW;
-    static constexpr int GROUPS = (TY / 2) * T >= 32 ? TY / 2 : 32 / T;  // row-pair groups
+    static constexpr int TY_RAW = 128 / T;   // rows per row-kernel block, one row per group
+    static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
+    static constexpr int GROUPS = TY * T >= 32 ? TY : 32 / T;
     static constexpr int ROW_THREADS = GROUPS * T;
     static constexpr int SC = C | 1;         // odd row stride of the W tile (bank spread)
     static constexpr int BUF = N + N / E;
@@ -44,8 +52,8 @@ struct StepControl {
 };
 
 template <typename R> struct ColumnArgs {
-    const cx<R> *nl;        // [M][C][N]
-    cx<R> *w;               // [M][4][C][N]
+    const cx<R> *nl;        // [M][2][C][N]
+    cx<R> *w;               // [M][2][C][N]
     cx<R> *omega;           // [M][C][LD]
     cx<R> *ystage;          // [M][C][LD]
     cx<R> *acc;             // [M][C][LD]
@@ -65,8 +73,8 @@ template <typename R> struct ColumnArgs {
 };
 
 template <typename R> struct RowArgs {
-    const cx<R> *w;       // [M][4][C][N]
-    cx<R> *nl;            // [M][C][N]
+    const cx<R> *w;       // [M][2][C][N]
+    cx<R> *nl;            // [M][2][C][N]
     const cx<R> *tw;
     double cfl_scale;     // dt * N / (2 pi); > 0 enables the stage-1 CFL check
     StepControl *ctl;
@@ -112,11 +120,23 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             y[r] = (valid && j >= 0) ? a.omega[cbase + j] : mk<R>(0, 0);
         }
     } else {
-        // forward column FFT of the Jacobian spectrum (unnormalised; 1/N^2 below)
-        const cx<R> *src = a.nl + (static_cast<size_t>(m) * C + kxc) * N;
+        // forward column FFTs of the product spectra (unnormalised; 1/N^2 below):
+        // A^ = -kx ky P^ - (kx^2 - ky^2) Q^ with P = v^2 - u^2, Q = u v
+        const cx<R> *src = a.nl + (static_cast<size_t>(m) * 2 * C + kxc) * N;
+        cx<R> adv[E];
 #pragma unroll
         for (int r = 0; r < E; ++r)
             v[r] = valid ? src[t + r * T] : mk<R>(0, 0);
+        fft_line<N, E, -1, R>(v, sm, tw, t);
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            const int j = compact_j<N>(t + r * T);
+            const int ky = j <= K ? j : j - LD;
+            adv[r] = scale(static_cast<R>(-kxc * ky), v[r]);
+        }
+#pragma unroll
+        for (int r = 0; r < E; ++r)
+            v[r] = valid ? src[static_cast<size_t>(C) * N + t + r * T] : mk<R>(0, 0);
         fft_line<N, E, -1, R>(v, sm, tw, t);
         const R inv_n2 = static_cast<R>(1.0 / (static_cast<double>(N) * N));
         const R nu = static_cast<R>(a.nu), alpha = static_cast<R>(a.alpha),
@@ -133,10 +153,10 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             const size_t idx = cbase + j;
             const cx<R> wn = a.omega[idx];
             const cx<R> ys = a.stage == 1 ? wn : a.ystage[idx];
-            // rhs: active ? -N^ - (nu k^2 + alpha) w + f : 0   (solver.cpp:197-202)
+            // rhs: active ? -A^ - (nu k^2 + alpha) w + f : 0   (solver.cpp:197-202)
             cx<R> k = mk<R>(0, 0);
             if (!(kxc == 0 && j == 0)) {
-                const cx<R> nl = scale(inv_n2, v[r]);
+                const cx<R> nl = scale(inv_n2, adv[r] - scale(static_cast<R>(kxc * kxc - ky * ky), v[r]));
                 const R rate = nu * k2 + alpha;
                 k = mk<R>(-nl.x, -nl.y) - scale(rate, ys);
                 if (kxc < a.forcing_cols)
@@ -178,11 +198,11 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     }
 
     if (a.emit) {
-        // spectral derivatives of the next stage input (solver.cpp:177-191), then inverse
-        // column FFTs.  Fields: 0 u^ = i ky psi, 1 v^ = -i kx psi, 2 wx^ = i kx w, 3 wy^ = i ky w.
-        cx<R> *dst = a.w + (static_cast<size_t>(m) * 4 * C + kxc) * N;
+        // velocity of the next stage input (solver.cpp:177-185): u^ = i ky psi^,
+        // v^ = -i kx psi^ with psi^ = w^/k^2, then inverse column FFTs
+        cx<R> *dst = a.w + (static_cast<size_t>(m) * 2 * C + kxc) * N;
 #pragma unroll 1
-        for (int f = 0; f < 4; ++f) {
+        for (int f = 0; f < 2; ++f) {
 #pragma unroll
             for (int r = 0; r < E; ++r) {
                 const int j = compact_j<N>(t + r * T);
@@ -190,15 +210,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 if (j >= 0) {
                     const int ky = j <= K ? j : j - LD;
                     const R kyr = static_cast<R>(ky);
-                    if (f < 2) {
-                        const R k2 = static_cast<R>(kxc * kxc + ky * ky);
-                        const cx<R> psi = k2 > 0 ? mk<R>(y[r].x / k2, y[r].y / k2) : mk<R>(0, 0);
-                        z = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x)
-                                   : mk<R>(kxr * psi.y, -kxr * psi.x);
-                    } else {
-                        const R c = f == 2 ? kxr : kyr;
-                        z = mk<R>(-c * y[r].y, c * y[r].x);
-                    }
+                    const R k2 = static_cast<R>(kxc * kxc + ky * ky);
+                    const cx<R> psi = k2 > 0 ? mk<R>(y[r].x / k2, y[r].y / k2) : mk<R>(0, 0);
+                    z = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
                 }
                 v[r] = z;
             }
@@ -263,36 +277,32 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY, SC = G::SC;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *wt = tw + N;                      // [4][TY][SC]
-    cx<R> *nlt = wt + 4 * TY * SC;           // [C][TY+1]
-    cx<R> *lines = nlt + C * (TY + 1);       // [GROUPS][BUF]
+    cx<R> *wt = tw + N;                      // [2][TY][SC]
+    cx<R> *nlt = wt + 2 * TY * SC;           // [2][C][TY+1]
+    cx<R> *lines = nlt + 2 * C * (TY + 1);   // [GROUPS][BUF]
     const int m = blockIdx.x, y0 = blockIdx.y * TY;
     for (int i = threadIdx.x; i < N; i += blockDim.x)
         tw[i] = a.tw[i];
-    // load the W tile: for each (field, kx) a run of TY consecutive rows
-    const cx<R> *src = a.w + static_cast<size_t>(m) * 4 * C * N;
-    for (int i = threadIdx.x; i < 4 * C * TY; i += blockDim.x) {
+    // load the velocity tile: for each (field, kx) a run of TY consecutive rows
+    const cx<R> *src = a.w + static_cast<size_t>(m) * 2 * C * N;
+    for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
         const int ty = i % TY, fk = i / TY, f = fk / C, kx = fk % C;
         wt[(f * TY + ty) * SC + kx] = src[static_cast<size_t>(fk) * N + y0 + ty];
     }
     __syncthreads();
 
     const int g = threadIdx.x / T, t = threadIdx.x % T;
-    const bool active = g < TY / 2;
+    const bool active = g < TY;
+    const int ty = active ? g : 0;
     cx<R> *sm = lines + g * G::BUF;
-    R prod[2][E];
+    cx<R> z[E];
+    packed_row_inverse<N, E, R>(z, wt + (0 * TY + ty) * SC, wt + (1 * TY + ty) * SC, sm, tw, t);
     R vmax = 0;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int ty = active ? 2 * g + h : 0;
-        cx<R> z1[E], z2[E];
-        packed_row_inverse<N, E, R>(z1, wt + (0 * TY + ty) * SC, wt + (1 * TY + ty) * SC, sm, tw, t);
-        packed_row_inverse<N, E, R>(z2, wt + (2 * TY + ty) * SC, wt + (3 * TY + ty) * SC, sm, tw, t);
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            prod[h][r] = z1[r].x * z2[r].x + z1[r].y * z2[r].y;   // u wx + v wy
-            vmax = fmax(vmax, fabs(z1[r].x) + fabs(z1[r].y));
-        }
+    for (int r = 0; r < E; ++r) {
+        const R u = z[r].x, v = z[r].y;
+        vmax = fmax(vmax, fabs(u) + fabs(v));
+        z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
     }
     if (a.cfl_scale > 0) {
 #pragma unroll
@@ -301,33 +311,28 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
             atomicOr(&a.ctl->status, STATUS_CFL);
     }
-    // forward transform of rows (2g, 2g+1) packed as p_a + i p_b
-    cx<R> zp[E];
+    fft_line<N, E, -1, R>(z, sm, tw, t);
 #pragma unroll
     for (int r = 0; r < E; ++r)
-        zp[r] = mk<R>(prod[0][r], prod[1][r]);
-    fft_line<N, E, -1, R>(zp, sm, tw, t);
-#pragma unroll
-    for (int r = 0; r < E; ++r)
-        sm[pad<E>(t + r * T)] = zp[r];
+        sm[pad<E>(t + r * T)] = z[r];
     __syncwarp();
     if (active) {
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const int p = t + r * T;
             if (p <= K) {
-                const cx<R> zk = zp[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
+                const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
                 const cx<R> sa = zk + zc, sb = zk - zc;
-                nlt[p * (TY + 1) + 2 * g] = mk<R>(sa.x / 2, sa.y / 2);          // (Z + Z*)/2
-                nlt[p * (TY + 1) + 2 * g + 1] = mk<R>(sb.y / 2, -sb.x / 2);     // (Z - Z*)/(2i)
+                nlt[p * (TY + 1) + ty] = mk<R>(sa.x / 2, sa.y / 2);                  // P^
+                nlt[(C + p) * (TY + 1) + ty] = mk<R>(sb.y / 2, -sb.x / 2);           // Q^
             }
         }
     }
     __syncthreads();
-    cx<R> *dst = a.nl + static_cast<size_t>(m) * C * N;
-    for (int i = threadIdx.x; i < C * TY; i += blockDim.x) {
-        const int ty = i % TY, kx = i / TY;
-        dst[static_cast<size_t>(kx) * N + y0 + ty] = nlt[kx * (TY + 1) + ty];
+    cx<R> *dst = a.nl + static_cast<size_t>(m) * 2 * C * N;
+    for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
+        const int t2 = i % TY, fk = i / TY;
+        dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * (TY + 1) + t2];
     }
 }
 
@@ -337,7 +342,7 @@ template <typename R, int N> constexpr size_t column_smem() {
 }
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (N + 4 * G::TY * G::SC + G::C * (G::TY + 1) + G::GROUPS * G::BUF);
+    return sizeof(cx<R>) * (N + 2 * G::TY * G::SC + 2 * G::C * (G::TY + 1) + G::GROUPS * G::BUF);
 }
 
 } // namespace hzlb

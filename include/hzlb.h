@@ -157,6 +157,67 @@ HZLB_API int hzlb_enkf_analysis(hzlb_ensemble *h, const uint32_t *x, const uint3
                        const double *values, const double *sd, size_t p,
                        const double *perturbations);
 
+/* ---- drop-in drivers for the reference's ensemble entry points ---------------------- */
+/* hzl::Parameters (include/hzl/solver.hpp:15-23). */
+typedef struct {
+    double viscosity, friction, forcing_sigma, forcing_tau;
+    int forcing_min, forcing_max;
+} hzlb_parameters;
+/* hzl::Observation (include/hzl/inference.hpp:33-36). */
+typedef struct {
+    uint64_t step;
+    uint32_t x, y;
+    double value, standard_deviation;
+} hzlb_observation;
+/* hzl::Dataset (include/hzl/inference.hpp:37-46). */
+typedef struct {
+    int n;
+    double dt;
+    int stochastic, forcing_min, forcing_max;
+    size_t count;
+    const hzlb_observation *observations;
+} hzlb_dataset;
+/* hzl::FilterRecord without the field (include/hzl/filter.hpp:5-9). */
+typedef struct {
+    uint64_t step;
+    double log_likelihood_increment, effective_particles, maximum_weight;
+} hzlb_filter_record;
+/* hzl::EnKFOptions (include/hzl/filter.hpp:43-50). */
+typedef struct {
+    double inflation, localization_radius;
+    uint64_t forecast_steps, forecast_every;
+} hzlb_enkf_options;
+/* hzl::EnsembleFilterRecord without the field (include/hzl/filter.hpp:37-42). */
+typedef struct {
+    uint64_t step;
+    double forecast_sensor_rmse, posterior_spread;
+    int is_forecast;
+} hzlb_enkf_record;
+
+/* hzl::ensemble(n, p, dt, steps, count, workers, seed) (include/hzl/inference.hpp:85-86,
+ * src/inference.cpp:555-590): member i starts from "zero" with OU forcing seeded by
+ * stream_seed(seed, i); out receives count x {time, energy, enstrophy, dissipation,
+ * injection, cfl_rate} in member order.  All members advance together on the device. */
+HZLB_API int hzlb_run_ensemble(int n, const hzlb_parameters *params, double dt, uint64_t steps,
+                               uint64_t count, uint64_t seed, int precision, int device,
+                               double *out);
+/* hzl::bootstrap_filter(data, p, particles, seed, retain_states) (include/hzl/filter.hpp:17-18,
+ * src/filter.cpp:38-126).  mean_vorticity (optional): capacity x n*n complex, the weighted
+ * mean physical vorticity per record. */
+HZLB_API int hzlb_bootstrap_filter(const hzlb_dataset *data, const hzlb_parameters *params,
+                                   uint64_t particles, uint64_t seed, int retain_states,
+                                   int precision, int device, double *log_likelihood,
+                                   uint64_t *resampling_events, hzlb_filter_record *records,
+                                   size_t capacity, size_t *nrecords, double *mean_vorticity);
+/* hzl::ensemble_kalman_filter(data, p, members, seed, options) (include/hzl/filter.hpp:52-54,
+ * src/filter.cpp:204-356): serial perturbed-observation updates of the joint (vorticity,
+ * forcing) state.  mean_vorticity (optional): capacity x n*n complex per record. */
+HZLB_API int hzlb_ensemble_kalman_filter(const hzlb_dataset *data, const hzlb_parameters *params,
+                                         uint64_t members, uint64_t seed,
+                                         const hzlb_enkf_options *options, int precision,
+                                         int device, hzlb_enkf_record *records, size_t capacity,
+                                         size_t *nrecords, double *mean_vorticity);
+
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */
 /* Gaussian random vorticity spectrum, E(k) ~ k^4 exp(-(k/6)^2), unit enstrophy, retained modes

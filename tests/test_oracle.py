@@ -1,0 +1,280 @@
+"""Pins the CPU oracle (oracle/hzl_oracle.c) before it is trusted as the checker:
+* bit-for-bit agreement with the reference's own CPU library (oracle/_ref) on the transform,
+  the OU-forced step, diagnostics, OU forcing streams, filters and POD;
+* the golden vectors in tests/golden/ (generated from that library by make_golden.py);
+* the reference's own verification assertions (tests/verification.cpp) re-run on the oracle;
+* published Philox4x32-10 known-answer vectors (Random123)."""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+from oracle.oracle import params6
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def test_philox_known_answers(oracle):
+    kat = [
+        ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
+        ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
+        ((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0),
+         (0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)),
+    ]
+    for ctr, key, expected in kat:
+        assert tuple(int(v) for v in oracle.philox(ctr, key)) == expected
+
+
+def test_stream_seed_matches_reference(oracle, reference):
+    for base, index in ((0, 0), (42, 7), (2026, 2 ** 64 - 1), (2 ** 63, 12345)):
+        assert oracle.stream_seed(base, index) == reference.stream_seed(base, index)
+
+
+@pytest.mark.parametrize("n", [8, 16, 32, 64, 128])
+def test_fft_bit_exact_with_reference(oracle, reference, n):
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n)) + 1j * rng.standard_normal((n, n))
+    for inverse in (False, True):
+        np.testing.assert_array_equal(oracle.fft(a, inverse), reference.fft(a, inverse))
+
+
+def test_fft_golden(oracle):
+    g = np.load(GOLDEN / "fft_n16.npz")
+    np.testing.assert_array_equal(oracle.fft(g["input"], False), g["forward"])
+    np.testing.assert_array_equal(oracle.fft(g["input"], True), g["inverse"])
+
+
+def test_fourier_normalisation(oracle):
+    """verification.cpp:28-43."""
+    n = 32
+    x = np.arange(n)
+    field = np.sin(3 * 2 * np.pi * x / n)[None, :] + 0.7 * np.cos(2 * 2 * np.pi * x / n)[:, None]
+    spec = oracle.fft(field.astype(np.complex128), False)
+    assert abs(spec[0, 3] - (0 - 0.5j)) < 1e-14
+    assert rel_l2(oracle.fft(spec, True), field) < 1e-14
+
+
+@pytest.mark.parametrize("name", ["multimode", "taylor-green", "zero"])
+def test_ou_step_bit_exact_with_reference(oracle, reference, name):
+    p = params6(0.01, 0.1, 0.2, 0.5, 2, 3)
+    a, b = oracle.solver(32, p, 123), reference.solver(32, p, 123)
+    a.initialize(name)
+    b.initialize(name)
+    a.step(0.01, 7)
+    b.step(0.01, 7)
+    w, f = a.state()
+    np.testing.assert_array_equal(w, b.coefficients())
+    np.testing.assert_array_equal(f, b.forcing())
+    np.testing.assert_array_equal(a.midpoint_forcing(), b.midpoint_forcing())
+    np.testing.assert_array_equal(a.diagnostics(), b.diagnostics())
+    np.testing.assert_array_equal(a.physical_vorticity(), b.physical_vorticity())
+
+
+def test_ou_step_golden(oracle):
+    g = np.load(GOLDEN / "step_ou_n16.npz")
+    s = oracle.solver(16, g["params"], int(g["seed"]))
+    s.initialize("multimode")
+    np.testing.assert_array_equal(s.state()[0], g["initial"])
+    s.step(float(g["dt"]), int(g["steps"]))
+    w, f = s.state()
+    np.testing.assert_array_equal(w, g["final"])
+    np.testing.assert_array_equal(f, g["forcing"])
+    np.testing.assert_array_equal(s.diagnostics(), g["diagnostics"])
+
+
+def test_config0_golden(oracle):
+    """The seeded-synthetic config (N=64, 1000 steps) run by the oracle agrees with the same
+    workload driven through the reference's Solver within 1e-12 (the reference path also
+    symmetrises conjugate pairs each step, so agreement is to roundoff, not bitwise)."""
+    g = np.load(GOLDEN / "config0_n64.npz")
+    n, steps, dt, nu, sigma, seed = (int(g["n"]), int(g["steps"]), float(g["dt"]), float(g["nu"]),
+                                     float(g["sigma"]), int(g["seed"]))
+    s = oracle.solver(n, params6(nu, 0.0, 0.0, 0.5, 1, 4), 0)
+    s.set_state(oracle.grf(n, seed, 0), np.zeros((n, n), np.complex128))
+    forcing = oracle.kolmogorov(n)
+    series = np.zeros((steps, 2))
+    for i in range(steps):
+        s.synthetic_step(dt, forcing, sigma, 4, seed, 0, i)
+        d = s.diagnostics()
+        series[i] = d[1], d[2]
+    assert rel_l2(s.state()[0], g["final"]) < 1e-12
+    np.testing.assert_allclose(series, g["series"], rtol=1e-12)
+
+
+def test_taylor_green_decay_and_order(oracle):
+    """verification.cpp:44-65."""
+    p = params6(0.7, 0.6, 0.0, 0.5, 2, 3)
+    errors = []
+    for dt in (0.04, 0.02, 0.01):
+        s = oracle.solver(16, p, 1)
+        s.initialize("taylor-green")
+        exact = s.state()[0] * np.exp(-2.0 * 0.4)
+        s.step(dt, int(round(0.4 / dt)))
+        errors.append(rel_l2(s.state()[0], exact))
+        d = s.diagnostics()
+        assert abs(d[1] / (np.pi ** 2 * np.exp(-4.0 * 0.4)) - 1) < 1e-6
+        assert abs(d[3] - 2 * 0.7 * d[2]) < 1e-13
+    assert errors[0] / errors[1] > 14 and errors[1] / errors[2] > 14
+
+
+def test_inviscid_conservation(oracle):
+    """verification.cpp:86-108."""
+    s = oracle.solver(32, params6(0.0, 0.0, 0.0, 0.5, 2, 3), 1)
+    s.initialize("multimode")
+    before = s.diagnostics()
+    s.step(0.005, 100)
+    after = s.diagnostics()
+    assert abs(after[1] / before[1] - 1) < 1e-9
+    assert abs(after[2] / before[2] - 1) < 1e-9
+    assert np.abs(s.physical_vorticity().imag).max() < 1e-12
+
+
+def test_ou_stationary_moments(oracle):
+    """verification.cpp:109-140: OU stationary variance sigma^2 tau/4 and one-step
+    correlation exp(-dt/tau) over 2048 replicas."""
+    p = params6(0.01, 0.1, 0.5, 0.3, 2, 3)
+    a, b = [], []
+    for j in range(2048):
+        s = oracle.solver(16, p, oracle.stream_seed(123, j))
+        a.append(s.state()[1][0, 2].real)
+        s.step(0.05)
+        b.append(s.state()[1][0, 2].real)
+    a, b = np.array(a), np.array(b)
+    var = 0.5 ** 2 * 0.3 / 4
+    tol = 5 * np.sqrt(2.0 / 2047)
+    assert abs(a.var(ddof=1) / var - 1) < tol and abs(b.var(ddof=1) / var - 1) < tol
+    corr = np.corrcoef(a, b)[0, 1]
+    assert abs(corr - np.exp(-0.05 / 0.3)) < 0.04
+
+
+def test_shell_forcing_matches_solver_midpoint(oracle, reference):
+    """verification.cpp:342-350: the reference ShellForcing reproduces the oracle solver's
+    midpoint forcing exactly (so host-uploaded forcing reproduces the CPU path)."""
+    p = params6(0.01, 0.1, 0.2, 0.5, 2, 3)
+    s = oracle.solver(16, p, 555)
+    s.initialize("zero")
+    sf = reference.shell_forcing(16, p, 555)
+    for _ in range(6):
+        s.step(0.01)
+        np.testing.assert_array_equal(sf.midpoint_step(0.01), s.midpoint_forcing())
+        np.testing.assert_array_equal(sf.coefficients(), s.state()[1])
+
+
+def _oracle_bootstrap(oracle, ds, p6, count, seed):
+    """The reference's bootstrap_filter (filter.cpp:38-126) assembled from oracle pieces."""
+    n = ds["n"]
+    parts = []
+    for i in range(count):
+        s = oracle.solver(n, p6, oracle.stream_seed(seed, i))
+        s.initialize("multimode")
+        parts.append(s)
+    weights = np.full(count, 1 / count)
+    # mt19937_64(stream_seed(seed, 2^64-1)) raw draws through the oracle's MT
+    from oracle.oracle import C as _C  # noqa: F401
+    mt = oracle.lib
+    import ctypes as C
+    buf = (C.c_uint8 * 4096)()
+    mt.ho_normal_init(buf, C.c_uint64(oracle.stream_seed(seed, 2 ** 64 - 1)))
+    mt.ho_mt_next.restype = C.c_uint64
+    ll, events, records, ancestors_log = 0.0, 0, [], []
+    steps = ds["steps"]
+    begin, current, group = 0, 0, 0
+    while begin < len(steps):
+        target = int(steps[begin])
+        end = begin
+        while end < len(steps) and steps[end] == target:
+            end += 1
+        logs = np.zeros(count)
+        for i, s in enumerate(parts):
+            for _ in range(current, target):
+                s.step(ds["dt"])
+            field = s.physical_vorticity()
+            v = np.log(weights[i]) if weights[i] > 0 else -np.inf
+            for o in range(begin, end):
+                r = (field[ds["y"][o], ds["x"][o]].real - ds["value"][o]) / ds["sd"][o]
+                v -= 0.5 * r * r + np.log(ds["sd"][o]) + 0.5 * np.log(2 * np.pi)
+            logs[i] = v
+        w, inc, ess, mw = oracle.pf_weights(logs)
+        ll += inc
+        records.append((target, inc, ess, mw))
+        weights = w
+        if ess < count / 2 and end < len(steps):
+            u = oracle.lib.ho_resampling_uniform(C.c_uint64(mt.ho_mt_next(buf)))
+            anc = oracle.systematic_resample(weights, u)
+            ancestors_log.append((weights.copy(), u, anc.copy()))
+            new = []
+            for i, a in enumerate(anc):
+                s = oracle.solver(n, p6, 0)
+                w_a, f_a = parts[a].state()
+                s.set_state(w_a, f_a)
+                s.reseed_future(oracle.stream_seed(seed, (group + 1) * count + i))
+                new.append(s)
+            parts = new
+            weights = np.full(count, 1 / count)
+            events += 1
+        current, begin, group = target, end, group + 1
+    return ll, events, np.array(records), ancestors_log
+
+
+def test_particle_filter_restatement_matches_reference(oracle, reference):
+    """The oracle's weight and systematic-resampling restatements reproduce the reference's
+    bootstrap_filter (log-likelihood, ESS history, resampling events) exactly."""
+    g = np.load(GOLDEN / "filters_n16.npz")
+    p6 = params6(0.03, 0.1, 0.2, 0.5, 2, 3)
+    ds = dict(n=16, dt=0.01, steps=g["steps"], x=g["x"], y=g["y"], value=g["value"], sd=g["sd"])
+    ll, events, records, _ = _oracle_bootstrap(oracle, ds, p6, 32, 555)
+    assert ll == float(g["pf_loglik"])
+    assert events == int(g["pf_events"])
+    np.testing.assert_array_equal(records, g["pf_records"])
+
+
+def test_resampling_edge_cases(oracle):
+    """Systematic resampling: degenerate weights pick one ancestor; uniform weights keep order;
+    u = 0 and u just below 1; every ancestor in range."""
+    m = 16
+    w = np.zeros(m)
+    w[5] = 1.0
+    assert (oracle.systematic_resample(w, 0.3) == 5).all()
+    w = np.full(m, 1 / m)
+    np.testing.assert_array_equal(oracle.systematic_resample(w, 0.5), np.arange(m))
+    rng = np.random.default_rng(1)
+    w = rng.random(2048) ** 8
+    w /= w.sum()
+    for u in (0.0, 1 - 2 ** -53):
+        a = oracle.systematic_resample(w, u)
+        assert a.min() >= 0 and a.max() < 2048 and (np.diff(a.astype(int)) >= 0).all()
+
+
+def test_fit_pod_matches_reference_and_golden(oracle, reference):
+    g = np.load(GOLDEN / "pod_n16.npz")
+    mean, modes, sv, cap = oracle.fit_pod(g["snapshots"], 4, 0.9999999)
+    np.testing.assert_allclose(mean.reshape(g["mean"].shape), g["mean"], rtol=0, atol=1e-15)
+    np.testing.assert_allclose(sv, g["singular_values"], rtol=1e-12)
+    np.testing.assert_allclose(np.abs(modes), np.abs(g["modes"]), atol=1e-10)
+    assert abs(cap - float(g["captured"])) < 1e-12
+    # analytic rank-2 snapshots (verification.cpp:273-282)
+    t = 2 * np.pi * np.arange(30) / 30
+    snaps = np.stack([1 + np.sin(t), 2 + 2 * np.cos(t), np.full(30, 3.0)], axis=1).astype(complex)
+    mean, modes, sv, cap = oracle.fit_pod(snaps, 3, 1.0)
+    assert len(modes) == 2
+    gram = np.real(np.conj(modes) @ modes.T)
+    np.testing.assert_allclose(gram, np.eye(2), atol=1e-12)
+
+
+def test_grf_initial_field(oracle):
+    n = 128
+    w = oracle.grf(n, 42, 0)
+    area = 4 * np.pi ** 2
+    assert abs(area / 2 * np.sum(np.abs(w) ** 2) - 1) < 1e-13
+    # Hermitian symmetry and the 2/3 truncation
+    y, x = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    np.testing.assert_array_equal(w[(n - y) % n, (n - x) % n], np.conj(w))
+    k = np.where(np.arange(n) < n // 2, np.arange(n), np.arange(n) - n)
+    outside = (3 * np.abs(k)[None, :] >= n) | (3 * np.abs(k)[:, None] >= n)
+    assert not w[outside].any() and w[0, 0] == 0
+    # different members differ; same member is reproducible
+    assert not np.array_equal(w, oracle.grf(n, 42, 1))
+    np.testing.assert_array_equal(w, oracle.grf(n, 42, 0))

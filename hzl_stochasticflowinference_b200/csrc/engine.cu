@@ -43,9 +43,11 @@ template <typename R> class EngineT final : public Engine {
         cuda_check(prepare_kernels<R>(n_), "configure kernels");
         cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "create stream");
         const size_t cb = sizeof(cx<R>);
-        omega_.ensure(cb * compact_ * M_, "allocate GPU state");
-        ystage_.ensure(cb * compact_ * M_, "allocate GPU stage input");
-        acc_.ensure(cb * compact_ * M_, "allocate GPU RK accumulator");
+        // +16 bytes: the column pass copies whole 16-byte chunks and may read one entry past
+        // the last member
+        omega_.ensure(cb * compact_ * M_ + 16, "allocate GPU state");
+        ystage_.ensure(cb * compact_ * M_ + 16, "allocate GPU stage input");
+        acc_.ensure(cb * compact_ * M_ + 16, "allocate GPU RK accumulator");
         w_.ensure(cb * 2 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU velocity columns");
         nl_.ensure(cb * 2 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU product rows");
         if (fcount_)

@@ -3,6 +3,8 @@
 #include "launch.h"
 #include "physical.cuh"
 
+#include <algorithm>
+
 namespace hzlb {
 namespace {
 
@@ -11,8 +13,11 @@ template <typename R, int N> struct L {
     static constexpr size_t col_smem = hzlb::column_smem<R, N>();
     static constexpr size_t row_smem = hzlb::row_smem<R, N>();
     static constexpr size_t prow_smem = sizeof(cx<R>) * (N + G::GROUPS * G::BUF);
+    static constexpr size_t pcol_smem = sizeof(cx<R>) * (N + G::LPB * G::BUF);
     static_assert(row_smem <= 227 * 1024, "row kernel shared memory");
 
+    // persistent grids: resident blocks per SM x SMs, per device
+    static inline int col_resident[64] = {}, row_resident[64] = {};
     static cudaError_t prepare() {
         cudaError_t e = cudaFuncSetAttribute(column_kernel<R, N>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -20,21 +25,47 @@ template <typename R, int N> struct L {
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(row_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(row_smem));
+        int dev = 0, sms = 0, cb = 0, rb = 0;
+        if (e == cudaSuccess)
+            e = cudaGetDevice(&dev);
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cb, column_kernel<R, N>,
+                                                              G::COL_THREADS, col_smem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rb, row_kernel<R, N>,
+                                                              G::ROW_THREADS, row_smem);
+        if (e == cudaSuccess && (cb < 1 || rb < 1))
+            e = cudaErrorInvalidConfiguration;
+        if (e == cudaSuccess && dev < 64) {
+            col_resident[dev] = cb * sms;
+            row_resident[dev] = rb * sms;
+        }
         return e;
+    }
+    static int resident(const int *table) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        return dev < 64 && table[dev] > 0 ? table[dev] : 148;
     }
     static dim3 col_grid(int members) { return dim3(members, (G::C + G::LPB - 1) / G::LPB); }
     static dim3 row_grid(int members) { return dim3(members, N / G::TY); }
     static cudaError_t column(const ColumnArgs<R> &a, cudaStream_t s) {
-        column_kernel<R, N><<<col_grid(a.members), G::COL_THREADS, col_smem, s>>>(a);
+        const int items = a.members * G::NCG;
+        const int grid = std::min(items, resident(col_resident));
+        column_kernel<R, N><<<grid, G::COL_THREADS, col_smem, s>>>(a, items);
         return cudaGetLastError();
     }
     static cudaError_t row(const RowArgs<R> &a, cudaStream_t s) {
-        row_kernel<R, N><<<row_grid(a.members), G::ROW_THREADS, row_smem, s>>>(a);
+        const int items = a.members * (N / G::TY);
+        const int grid = std::min(items, resident(row_resident));
+        row_kernel<R, N><<<grid, G::ROW_THREADS, row_smem, s>>>(a, items);
         return cudaGetLastError();
     }
     static cudaError_t physical(const cx<R> *field, long long stride, cx<R> *cols, R *phys,
                                 const cx<R> *tw, int members, cudaStream_t s) {
-        field_column_inverse<R, N><<<col_grid(members), G::COL_THREADS, col_smem, s>>>(
+        field_column_inverse<R, N><<<col_grid(members), G::COL_THREADS, pcol_smem, s>>>(
             field, stride, cols, tw);
         field_row_inverse<R, N><<<row_grid(members), G::ROW_THREADS, prow_smem, s>>>(cols, phys, tw);
         return cudaGetLastError();

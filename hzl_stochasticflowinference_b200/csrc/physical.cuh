@@ -13,7 +13,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                          const cx<R> *tw_g) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
     cx<R> *lines = tw + N;
     for (int i = threadIdx.x; i < N; i += blockDim.x)
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     field_row_inverse(const cx<R> *cols, R *phys, const cx<R> *tw_g) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
     cx<R> *lines = tw + N;
     for (int i = threadIdx.x; i < N; i += blockDim.x)
@@ -85,14 +85,14 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     }
 }
 
-// max over the grid of |u| + |v| per member from the velocity columns W (fields 0, 1),
+// max over the grid of |u| + |v| per member from the velocity rows W ([m][y][field][kx]),
 // written as the bit pattern of a nonnegative double (monotone as an unsigned integer).
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     velocity_max(const cx<R> *w, unsigned long long *vmax_bits, const cx<R> *tw_g) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
     cx<R> *lines = tw + N;
     for (int i = threadIdx.x; i < N; i += blockDim.x)
@@ -100,26 +100,27 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     __syncthreads();
     const int g = threadIdx.x / T, t = threadIdx.x % T, m = blockIdx.x;
     const bool active = g < TY / 2;
-    const cx<R> *u = w + static_cast<size_t>(m) * 2 * C * N, *v = u + static_cast<size_t>(C) * N;
+    const cx<R> *wm = w + static_cast<size_t>(m) * N * 2 * C;   // rows [y][field][kx]
     double best = 0;
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
         const int y = blockIdx.y * TY + (active ? 2 * g + h : 0);
+        const cx<R> *u = wm + static_cast<size_t>(y) * 2 * C, *v = u + C;
         cx<R> z[E];
 #pragma unroll
         for (int r = 0; r < E; ++r) {
             const int p = t + r * T;
             cx<R> za = mk<R>(0, 0), zb = mk<R>(0, 0);
             if (p <= K) {
-                za = u[static_cast<size_t>(p) * N + y];
-                zb = v[static_cast<size_t>(p) * N + y];
+                za = u[p];
+                zb = v[p];
                 if (p == 0) {
                     za.y = 0;
                     zb.y = 0;
                 }
             } else if (p >= N - K) {
-                za = conj(u[static_cast<size_t>(N - p) * N + y]);
-                zb = conj(v[static_cast<size_t>(N - p) * N + y]);
+                za = conj(u[N - p]);
+                zb = conj(v[N - p]);
             }
             z[r] = mk<R>(za.x - zb.y, za.y + zb.x);
         }

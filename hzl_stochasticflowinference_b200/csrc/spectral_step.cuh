@@ -11,20 +11,26 @@
 // five: inverse u, v (one packed complex transform per row) and forward v^2 - u^2, u v (one
 // packed complex transform per row).
 //
-// One RK stage is two kernels:
-//   column kernel  (per member x kx column): forward column FFTs of the two product spectra,
-//                  RK stage epilogue (dealias mask, viscosity/friction, forcing, accumulator,
-//                  noise on the last stage), then u^ = i ky psi^, v^ = -i kx psi^ of the next
-//                  stage input and their inverse column FFTs;
-//   row kernel     (per member x tile of y rows): inverse row FFT of u + i v, the products
-//                  v^2 - u^2 and u v, the CFL check on stage 1, and the forward row FFT of
-//                  (v^2 - u^2) + i (u v), keeping kx = 0..K of each.
+// One RK stage is two persistent kernels, each streaming its inputs into shared memory with
+// bulk asynchronous copies (cp.async.bulk + mbarrier) one work item ahead of the compute:
+//   column kernel  (work item = member x group of LPB kx columns): forward column FFTs of the
+//                  two product spectra, the RK stage epilogue (dealias mask, viscosity and
+//                  friction, forcing, accumulator, Euler-Maruyama noise on the last stage),
+//                  then u^ = i ky psi^, v^ = -i kx psi^ of the next stage input and their
+//                  inverse column FFTs, written out row-major through shared memory;
+//   row kernel     (work item = member x tile of TY rows): inverse row FFT of u + i v, the
+//                  products v^2 - u^2 and u v, the CFL check on stage 1, and the forward row
+//                  FFT of (v^2 - u^2) + i (u v), keeping kx = 0..K of each.
 // HBM layouts (complex R):
 //   state / stage input / accumulator  [m][kx][j]          (K+1) x (2K+1) per member
-//   velocity columns W                 [m][field][kx][y]   2 x (K+1) x N   (u^, v^)
-//   product rows NL                    [m][field][kx][y]   2 x (K+1) x N   (v^2-u^2, u v)
+//   velocity rows W                    [m][y][field][kx]   N x 2 x (K+1)   (u^, v^ per row)
+//   product columns NL                 [m][field][kx][y]   2 x (K+1) x N   (v^2-u^2, u v)
+// so each row tile of W and each column group of NL is one contiguous bulk copy.
 #pragma once
+#include "async_copy.cuh"
 #include "fft.cuh"
+
+#include <type_traits>
 
 namespace hzlb {
 
@@ -35,14 +41,21 @@ template <typename R, int N> struct Cfg {
     static constexpr int K = (N - 1) / 3;
     static constexpr int C = K + 1;          // retained kx columns
     static constexpr int LD = 2 * K + 1;     // compact column length
-    static constexpr int LPB = T >= 64 ? 1 : 64 / T;  // column lines per block
+    static constexpr int BUF = N + N / E;    // padded FFT line buffer
+    // column kernel: LPB lines (columns) per block, 64 threads at least
+    static constexpr int LPB = T >= 64 ? 1 : 64 / T;
     static constexpr int COL_THREADS = LPB * T;
-    static constexpr int TY_RAW = 128 / T;   // rows per row-kernel block, one row per group
+    static constexpr int NCG = (C + LPB - 1) / LPB;   // column groups per member
+    // state window per array: LPB columns plus one entry of 16-byte alignment slack, rounded
+    // up to whole 16-byte chunks
+    static constexpr int PER16 = 16 / (2 * static_cast<int>(sizeof(R)));
+    static constexpr int ST_STRIDE = (LPB * LD + PER16 + PER16 - 1) / PER16 * PER16;
+    // row kernel: TY rows per block, one row per group of T threads, 128 threads at least
+    static constexpr int TY_RAW = 128 / T;
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
     static constexpr int GROUPS = TY * T >= 32 ? TY : 32 / T;
     static constexpr int ROW_THREADS = GROUPS * T;
-    static constexpr int SC = C | 1;         // odd row stride of the W tile (bank spread)
-    static constexpr int BUF = N + N / E;
+    static constexpr int TILE = TY * 2 * C;           // row tile, complex entries
 };
 
 struct StepControl {
@@ -53,7 +66,7 @@ struct StepControl {
 
 template <typename R> struct ColumnArgs {
     const cx<R> *nl;        // [M][2][C][N]
-    cx<R> *w;               // [M][2][C][N]
+    cx<R> *w;               // [M][N][2][C]
     cx<R> *omega;           // [M][C][LD]
     cx<R> *ystage;          // [M][C][LD]
     cx<R> *acc;             // [M][C][LD]
@@ -63,7 +76,7 @@ template <typename R> struct ColumnArgs {
     const cx<R> *tw;        // N twiddles
     double nu, alpha, dt;
     int stage;              // 0 start, 1..3 intermediate, 4 final
-    int emit;               // write W (derivative columns) for the next stage input
+    int emit;               // write W (velocity rows) for the next stage input
     double noise_scale;     // sigma sqrt(dt)/sqrt(2); 0 disables
     int noise_kmax2;
     unsigned long long seed;
@@ -73,7 +86,7 @@ template <typename R> struct ColumnArgs {
 };
 
 template <typename R> struct RowArgs {
-    const cx<R> *w;       // [M][2][C][N]
+    const cx<R> *w;       // [M][N][2][C]
     cx<R> *nl;            // [M][2][C][N]
     const cx<R> *tw;
     double cfl_scale;     // dt * N / (2 pi); > 0 enables the stage-1 CFL check
@@ -81,157 +94,286 @@ template <typename R> struct RowArgs {
     int members;
 };
 
+// Band of FFT positions p = t + r T (t = 0..T-1) relative to the retained set |k| <= K:
+// LOW all p <= K, HIGH all p >= N-K (negative wave numbers), ZERO none retained, else MIXED.
+template <int N, int T, int r> struct Band {
+    static constexpr int K = (N - 1) / 3, lo = r * T, hi = r * T + T - 1;
+    static constexpr bool low = hi <= K;
+    static constexpr bool high = lo >= N - K;
+    static constexpr bool zero = lo > K && hi < N - K;
+    static constexpr bool mixed = !(low || high || zero);
+};
+template <int I, int E, class F> __device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (I < E) {
+        f(std::integral_constant<int, I>{});
+        static_for<I + 1, E>(f);
+    }
+}
 // Compact index j of FFT position p in a column (or -1 if p is outside the retained band).
 template <int N> __device__ __forceinline__ int compact_j(int p) {
     constexpr int K = (N - 1) / 3, LD = 2 * K + 1;
     return p <= K ? p : (p >= N - K ? p - (N - LD) : -1);
 }
+template <int N, int T, int r> __device__ __forceinline__ int band_j(int p) {
+    using B = Band<N, T, r>;
+    constexpr int LD = 2 * B::K + 1;
+    if constexpr (B::low)
+        return p;
+    else if constexpr (B::high)
+        return p - (N - LD);
+    else if constexpr (B::zero)
+        return -1;
+    else
+        return compact_j<N>(p);
+}
+
+// Block-uniform bounded wait: thread 0 polls, the outcome is shared through `flag`, then
+// every thread observes the completed phase.  Returns false on every thread on timeout.
+__device__ __forceinline__ bool block_wait(uint64_t *bar, uint32_t parity, volatile int *flag) {
+    if (threadIdx.x == 0)
+        *flag = mbar_wait_bounded(bar, parity) ? 1 : 0;
+    __syncthreads();
+    const bool ok = *flag != 0;
+    if (ok)
+        mbar_wait_bounded(bar, parity);
+    return ok;
+}
 
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
-    column_kernel(const ColumnArgs<R> a) {
+    column_kernel(const ColumnArgs<R> a, int items) {
     using G = Cfg<R, N>;
-    constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD, K = G::K;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *lines = tw + N;
+    constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD, K = G::K, LPB = G::LPB;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cx<R> *nlbuf = reinterpret_cast<cx<R> *>(smem_raw);          // [2][2][LPB][N]
+    cx<R> *stbuf = nlbuf + 2 * 2 * LPB * N;                        // [3][ST_STRIDE]
+    cx<R> *lines = stbuf + 3 * G::ST_STRIDE;                       // [LPB][BUF]
+    cx<R> *tw = lines + LPB * G::BUF;                              // [N]
+    __shared__ __align__(8) uint64_t bars[3];                      // nl[0], nl[1], state
+    __shared__ int flags[2];
+    __shared__ unsigned long long step_sh;
+
+    const bool forward = a.stage > 0;
+    const int nst = a.stage <= 1 ? 1 : 3;   // state arrays read: w_n (and stage input, acc)
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        mbar_init_fence();
+        step_sh = a.ctl->step;
+    }
     for (int i = threadIdx.x; i < N; i += blockDim.x)
         tw[i] = a.tw[i];
-    __shared__ unsigned long long step_sh;
-    if (threadIdx.x == 0)
-        step_sh = a.ctl->step;
     __syncthreads();
 
+    auto issue_nl = [&](int it, int b) {
+        const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
+        const int nl = min(LPB, C - kx0);
+        const uint32_t bytes = static_cast<uint32_t>(nl * N * sizeof(cx<R>));
+        mbar_arrive_expect(&bars[b], 2 * bytes);
+        for (int f = 0; f < 2; ++f)
+            bulk_copy_g2s(nlbuf + (b * 2 + f) * LPB * N,
+                          a.nl + ((static_cast<size_t>(m) * 2 + f) * C + kx0) * N, bytes, &bars[b]);
+    };
+    // state window of a column group: starts `shift` entries early so that the copy is
+    // 16-byte aligned, and covers whole 16-byte chunks
+    auto window = [&](int it, int &shift, uint32_t &bytes) -> size_t {
+        const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
+        const int nl = min(LPB, C - kx0);
+        const size_t off = (static_cast<size_t>(m) * C + kx0) * LD;
+        shift = static_cast<int>(off % G::PER16);
+        const int count = (shift + nl * LD + G::PER16 - 1) / G::PER16 * G::PER16;
+        bytes = static_cast<uint32_t>(count * sizeof(cx<R>));
+        return off - shift;
+    };
+    auto issue_state = [&](int it) {
+        int shift;
+        uint32_t bytes;
+        const size_t base = window(it, shift, bytes);
+        mbar_arrive_expect(&bars[2], nst * bytes);
+        bulk_copy_g2s(stbuf, a.omega + base, bytes, &bars[2]);
+        if (nst == 3) {
+            bulk_copy_g2s(stbuf + G::ST_STRIDE, a.ystage + base, bytes, &bars[2]);
+            bulk_copy_g2s(stbuf + 2 * G::ST_STRIDE, a.acc + base, bytes, &bars[2]);
+        }
+    };
+
     const int line = threadIdx.x / T, t = threadIdx.x % T;
-    const int kx = blockIdx.y * G::LPB + line;
-    const int m = blockIdx.x;
-    const bool valid = kx < C;
-    const int kxc = valid ? kx : 0;
     cx<R> *sm = lines + line * G::BUF;
-    const size_t cbase = (static_cast<size_t>(m) * C + kxc) * LD;
-    const R kxr = static_cast<R>(kxc);
+    if (threadIdx.x == 0 && forward && static_cast<int>(blockIdx.x) < items)
+        issue_nl(blockIdx.x, 0);
+    bool timed_out = false;
+    int k = 0;
+    for (int it = blockIdx.x; it < items; it += gridDim.x, ++k) {
+        const int b = k & 1;
+        const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
+        const int kx = kx0 + line;
+        const bool valid = kx < C;
+        const int kxc = valid ? kx : 0;
+        if (threadIdx.x == 0) {
+            fence_proxy_async_shared();
+            issue_state(it);
+            if (forward && it + static_cast<int>(gridDim.x) < items)
+                issue_nl(it + gridDim.x, b ^ 1);
+        }
+        int shift;
+        uint32_t sbytes;
+        window(it, shift, sbytes);
+        const cx<R> *s_w = stbuf + shift + line * LD, *s_y = s_w + G::ST_STRIDE,
+                    *s_a = s_w + 2 * G::ST_STRIDE;
+        const size_t cbase = (static_cast<size_t>(m) * C + kxc) * LD;
+        const R kxr = static_cast<R>(kxc);
 
-    cx<R> y[E];   // next stage input at this thread's positions (zero outside the band)
-    cx<R> v[E];
-    if (a.stage == 0) {
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int j = compact_j<N>(t + r * T);
-            y[r] = (valid && j >= 0) ? a.omega[cbase + j] : mk<R>(0, 0);
-        }
-    } else {
-        // forward column FFTs of the product spectra (unnormalised; 1/N^2 below):
-        // A^ = -kx ky P^ - (kx^2 - ky^2) Q^ with P = v^2 - u^2, Q = u v
-        const cx<R> *src = a.nl + (static_cast<size_t>(m) * 2 * C + kxc) * N;
-        cx<R> adv[E];
-#pragma unroll
-        for (int r = 0; r < E; ++r)
-            v[r] = valid ? src[t + r * T] : mk<R>(0, 0);
-        fft_line<N, E, -1, R>(v, sm, tw, t);
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int j = compact_j<N>(t + r * T);
-            const int ky = j <= K ? j : j - LD;
-            adv[r] = scale(static_cast<R>(-kxc * ky), v[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < E; ++r)
-            v[r] = valid ? src[static_cast<size_t>(C) * N + t + r * T] : mk<R>(0, 0);
-        fft_line<N, E, -1, R>(v, sm, tw, t);
-        const R inv_n2 = static_cast<R>(1.0 / (static_cast<double>(N) * N));
-        const R nu = static_cast<R>(a.nu), alpha = static_cast<R>(a.alpha),
-                dt = static_cast<R>(a.dt);
-        bool bad = false;
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const int j = compact_j<N>(t + r * T);
-            y[r] = mk<R>(0, 0);
-            if (!valid || j < 0)
-                continue;
-            const int ky = j <= K ? j : j - LD;
-            const R k2 = static_cast<R>(kxc * kxc + ky * ky);
-            const size_t idx = cbase + j;
-            const cx<R> wn = a.omega[idx];
-            const cx<R> ys = a.stage == 1 ? wn : a.ystage[idx];
-            // rhs: active ? -A^ - (nu k^2 + alpha) w + f : 0   (solver.cpp:197-202)
-            cx<R> k = mk<R>(0, 0);
-            if (!(kxc == 0 && j == 0)) {
-                const cx<R> nl = scale(inv_n2, adv[r] - scale(static_cast<R>(kxc * kxc - ky * ky), v[r]));
-                const R rate = nu * k2 + alpha;
-                k = mk<R>(-nl.x, -nl.y) - scale(rate, ys);
-                if (kxc < a.forcing_cols)
-                    k = k + a.forcing[static_cast<size_t>(m) * a.forcing_stride +
-                                      static_cast<size_t>(kxc) * LD + j];
+        cx<R> y[E];   // next stage input at this thread's positions (zero outside the band)
+        cx<R> v[E];
+        if (!forward) {
+            if (!block_wait(&bars[2], k & 1, &flags[1])) {
+                timed_out = true;
+                break;
             }
-            if (a.stage == 1) {
-                a.acc[idx] = k;
-                y[r] = wn + scale(dt / 2, k);
-                a.ystage[idx] = y[r];
-            } else if (a.stage == 2) {
-                a.acc[idx] = a.acc[idx] + scale(static_cast<R>(2.0), k);
-                y[r] = wn + scale(dt / 2, k);
-                a.ystage[idx] = y[r];
-            } else if (a.stage == 3) {
-                a.acc[idx] = a.acc[idx] + scale(static_cast<R>(2.0), k);
-                y[r] = wn + scale(dt, k);
-                a.ystage[idx] = y[r];
-            } else {
-                // w += dt/6 (k1 + 2 k2 + 2 k3 + k4)   (solver.cpp:233-234)
-                cx<R> w1 = wn + scale(dt / 6, a.acc[idx] + k);
-                if (a.noise_scale > 0 && kxc * kxc + ky * ky >= 1 &&
-                    kxc * kxc + ky * ky <= a.noise_kmax2) {
-                    double xi1, xi2;
-                    const bool rep = kxc > 0 || ky > 0;
-                    philox_normal_pair(a.seed, a.member_base + m, step_sh,
-                                       mode_code(kxc, rep ? ky : -ky), xi1, xi2);
-                    const double s = a.noise_scale;
-                    w1 = w1 + mk<R>(static_cast<R>(s * xi1),
-                                    static_cast<R>(rep ? s * xi2 : -(s * xi2)));
-                }
-                bad |= !(isfinite(w1.x) && isfinite(w1.y));
-                a.omega[idx] = w1;
-                y[r] = w1;
+            static_for<0, E>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
+                const int j = band_j<N, T, r>(t + r * T);
+                y[r] = (valid && j >= 0) ? s_w[j] : mk<R>(0, 0);
+            });
+        } else {
+            if (!block_wait(&bars[b], (k >> 1) & 1, &flags[0])) {
+                timed_out = true;
+                break;
             }
-        }
-        if (bad)
-            atomicOr(&a.ctl->status, STATUS_NONFINITE);
-    }
-
-    if (a.emit) {
-        // velocity of the next stage input (solver.cpp:177-185): u^ = i ky psi^,
-        // v^ = -i kx psi^ with psi^ = w^/k^2, then inverse column FFTs
-        cx<R> *dst = a.w + (static_cast<size_t>(m) * 2 * C + kxc) * N;
-#pragma unroll 1
-        for (int f = 0; f < 2; ++f) {
+            // forward column FFTs of the product spectra (unnormalised; 1/N^2 below):
+            // A^ = -kx ky P^ - (kx^2 - ky^2) Q^ with P = v^2 - u^2, Q = u v
+            const cx<R> *srcP = nlbuf + (b * 2 + 0) * LPB * N + line * N;
+            const cx<R> *srcQ = srcP + LPB * N;
+            cx<R> adv[E];
 #pragma unroll
-            for (int r = 0; r < E; ++r) {
-                const int j = compact_j<N>(t + r * T);
-                cx<R> z = mk<R>(0, 0);
-                if (j >= 0) {
+            for (int r = 0; r < E; ++r)
+                v[r] = srcP[t + r * T];
+            fft_line<N, E, -1, R>(v, sm, tw, t);
+            static_for<0, E>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
+                const int p = t + r * T;
+                const int ky = Band<N, T, r>::low ? p : (Band<N, T, r>::high ? p - N : (p <= K ? p : p - N));
+                adv[r] = scale(static_cast<R>(-kxc * ky), v[r]);
+            });
+#pragma unroll
+            for (int r = 0; r < E; ++r)
+                v[r] = srcQ[t + r * T];
+            fft_line<N, E, -1, R>(v, sm, tw, t);
+            if (!block_wait(&bars[2], k & 1, &flags[1])) {
+                timed_out = true;
+                break;
+            }
+            const R inv_n2 = static_cast<R>(1.0 / (static_cast<double>(N) * N));
+            const R nu = static_cast<R>(a.nu), alpha = static_cast<R>(a.alpha),
+                    dt = static_cast<R>(a.dt);
+            bool bad = false;
+            static_for<0, E>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
+                y[r] = mk<R>(0, 0);
+                const int j = band_j<N, T, r>(t + r * T);
+                if (valid && j >= 0) {
                     const int ky = j <= K ? j : j - LD;
-                    const R kyr = static_cast<R>(ky);
                     const R k2 = static_cast<R>(kxc * kxc + ky * ky);
-                    const cx<R> psi = k2 > 0 ? mk<R>(y[r].x / k2, y[r].y / k2) : mk<R>(0, 0);
-                    z = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
+                    const cx<R> wn = s_w[j];
+                    const cx<R> ys = a.stage == 1 ? wn : s_y[j];
+                    // rhs: active ? -A^ - (nu k^2 + alpha) w + f : 0   (solver.cpp:197-202)
+                    cx<R> kk = mk<R>(0, 0);
+                    if (!(kxc == 0 && j == 0)) {
+                        const cx<R> nl =
+                            scale(inv_n2, adv[r] - scale(static_cast<R>(kxc * kxc - ky * ky), v[r]));
+                        const R rate = nu * k2 + alpha;
+                        kk = mk<R>(-nl.x, -nl.y) - scale(rate, ys);
+                        if (kxc < a.forcing_cols)
+                            kk = kk + a.forcing[static_cast<size_t>(m) * a.forcing_stride +
+                                                static_cast<size_t>(kxc) * LD + j];
+                    }
+                    const size_t idx = cbase + j;
+                    if (a.stage == 1) {
+                        a.acc[idx] = kk;
+                        y[r] = wn + scale(dt / 2, kk);
+                        a.ystage[idx] = y[r];
+                    } else if (a.stage == 2) {
+                        a.acc[idx] = s_a[j] + scale(static_cast<R>(2.0), kk);
+                        y[r] = wn + scale(dt / 2, kk);
+                        a.ystage[idx] = y[r];
+                    } else if (a.stage == 3) {
+                        a.acc[idx] = s_a[j] + scale(static_cast<R>(2.0), kk);
+                        y[r] = wn + scale(dt, kk);
+                        a.ystage[idx] = y[r];
+                    } else {
+                        // w += dt/6 (k1 + 2 k2 + 2 k3 + k4)   (solver.cpp:233-234)
+                        cx<R> w1 = wn + scale(dt / 6, s_a[j] + kk);
+                        const int kk2 = kxc * kxc + ky * ky;
+                        if (a.noise_scale > 0 && kk2 >= 1 && kk2 <= a.noise_kmax2) {
+                            double xi1, xi2;
+                            const bool rep = kxc > 0 || ky > 0;
+                            philox_normal_pair(a.seed, a.member_base + m, step_sh,
+                                               mode_code(kxc, rep ? ky : -ky), xi1, xi2);
+                            const double s = a.noise_scale;
+                            w1 = w1 + mk<R>(static_cast<R>(s * xi1),
+                                            static_cast<R>(rep ? s * xi2 : -(s * xi2)));
+                        }
+                        bad |= !(isfinite(w1.x) && isfinite(w1.y));
+                        a.omega[idx] = w1;
+                        y[r] = w1;
+                    }
                 }
-                v[r] = z;
-            }
-            fft_line<N, E, +1, R>(v, sm, tw, t);
-            if (valid) {
+            });
+            if (bad)
+                atomicOr(&a.ctl->status, STATUS_NONFINITE);
+        }
+
+        if (a.emit) {
+            // velocity of the next stage input (solver.cpp:177-185): u^ = i ky psi^,
+            // v^ = -i kx psi^ with psi^ = w^/k^2; inverse column FFTs, staged in shared memory
+            // (reusing this item's product buffer) as rows [y][field][line]
+            __syncthreads();   // every line is done with the product buffer
+            cx<R> *wst = nlbuf + b * 2 * LPB * N;
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                static_for<0, E>([&](auto rc) {
+                    constexpr int r = decltype(rc)::value;
+                    cx<R> z = mk<R>(0, 0);
+                    const int j = band_j<N, T, r>(t + r * T);
+                    if (j >= 0) {
+                        const int ky = j <= K ? j : j - LD;
+                        const R kyr = static_cast<R>(ky);
+                        const R k2 = static_cast<R>(kxc * kxc + ky * ky);
+                        const cx<R> psi = k2 > 0 ? mk<R>(y[r].x / k2, y[r].y / k2) : mk<R>(0, 0);
+                        z = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
+                    }
+                    v[r] = z;
+                });
+                fft_line<N, E, +1, R>(v, sm, tw, t);
 #pragma unroll
                 for (int r = 0; r < E; ++r)
-                    dst[static_cast<size_t>(f) * C * N + t + r * T] = v[r];
+                    wst[((t + r * T) * 2 + f) * LPB + line] = v[r];
+            }
+            __syncthreads();
+            const int nl = min(LPB, C - kx0);
+            cx<R> *dst = a.w + static_cast<size_t>(m) * N * 2 * C + kx0;
+            for (int i = threadIdx.x; i < N * 2 * LPB; i += blockDim.x) {
+                const int l = i % LPB, yf = i / LPB;
+                if (l < nl)
+                    dst[static_cast<size_t>(yf) * C + l] = wst[i];
             }
         }
+        fence_proxy_async_shared();   // this thread's shared-memory accesses precede the next bulk copies
+        __syncthreads();              // buffers of this item are free for the next copies
+    }
+    if (timed_out) {
+        if (threadIdx.x == 0)
+            atomicOr(&a.ctl->status, STATUS_TIMEOUT);
+        return;   // uniform across the block
     }
 
     if (a.stage == 4) {
         // the last block to finish advances the device step counter (every block read it
         // before arriving, so no block sees the new value)
-        __syncthreads();
         if (threadIdx.x == 0) {
             __threadfence();
-            const unsigned total = gridDim.x * gridDim.y;
+            const unsigned total = gridDim.x;
             const unsigned prev = atomicAdd(&a.ctl->arrivals, 1u);
             if (prev == total - 1) {
                 a.ctl->arrivals = 0;
@@ -251,98 +393,143 @@ template <int N, int E, typename R>
 __device__ __forceinline__ void packed_row_inverse(cx<R> (&z)[E], const cx<R> *A, const cx<R> *B,
                                                    cx<R> *sm, const cx<R> *tw, int t) {
     constexpr int T = N / E, K = (N - 1) / 3;
-#pragma unroll
-    for (int r = 0; r < E; ++r) {
+    static_for<0, E>([&](auto rc) {
+        constexpr int r = decltype(rc)::value;
+        using Bd = Band<N, T, r>;
         const int p = t + r * T;
         cx<R> za = mk<R>(0, 0), zb = mk<R>(0, 0);
-        if (p <= K) {
+        if constexpr (Bd::low) {
             za = A[p];
             zb = B[p];
-            if (p == 0) {
+            if (r == 0 && p == 0) {
                 za.y = 0;
                 zb.y = 0;
             }
-        } else if (p >= N - K) {
+        } else if constexpr (Bd::high) {
             za = conj(A[N - p]);
             zb = conj(B[N - p]);
+        } else if constexpr (Bd::mixed) {
+            if (p <= K) {
+                za = A[p];
+                zb = B[p];
+                if (p == 0) {
+                    za.y = 0;
+                    zb.y = 0;
+                }
+            } else if (p >= N - K) {
+                za = conj(A[N - p]);
+                zb = conj(B[N - p]);
+            }
         }
         z[r] = mk<R>(za.x - zb.y, za.y + zb.x);
-    }
+    });
     fft_line<N, E, +1, R>(z, sm, tw, t);
 }
 
 template <typename R, int N>
-__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowArgs<R> a) {
+__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowArgs<R> a, int items) {
     using G = Cfg<R, N>;
-    constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY, SC = G::SC;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *wt = tw + N;                      // [2][TY][SC]
-    cx<R> *nlt = wt + 2 * TY * SC;           // [2][C][TY+1]
-    cx<R> *lines = nlt + 2 * C * (TY + 1);   // [GROUPS][BUF]
-    const int m = blockIdx.x, y0 = blockIdx.y * TY;
+    constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cx<R> *tiles = reinterpret_cast<cx<R> *>(smem_raw);   // [2][TY][2][C]
+    cx<R> *nlt = tiles + 2 * G::TILE;                      // [2][C][TY+1]
+    cx<R> *lines = nlt + 2 * C * (TY + 1);                 // [GROUPS][BUF]
+    cx<R> *tw = lines + G::GROUPS * G::BUF;                // [N]
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int flag;
+    constexpr int tiles_per_member = N / TY;
+    constexpr uint32_t tile_bytes = G::TILE * sizeof(cx<R>);
+    static_assert(tile_bytes % 16 == 0, "bulk copies move 16-byte multiples");
+
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
     for (int i = threadIdx.x; i < N; i += blockDim.x)
         tw[i] = a.tw[i];
-    // load the velocity tile: for each (field, kx) a run of TY consecutive rows
-    const cx<R> *src = a.w + static_cast<size_t>(m) * 2 * C * N;
-    for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
-        const int ty = i % TY, fk = i / TY, f = fk / C, kx = fk % C;
-        wt[(f * TY + ty) * SC + kx] = src[static_cast<size_t>(fk) * N + y0 + ty];
-    }
     __syncthreads();
+    auto issue = [&](int it, int b) {
+        const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
+        mbar_arrive_expect(&bars[b], tile_bytes);
+        bulk_copy_g2s(tiles + b * G::TILE, a.w + (static_cast<size_t>(m) * N + y0) * 2 * C,
+                      tile_bytes, &bars[b]);
+    };
+    if (threadIdx.x == 0 && static_cast<int>(blockIdx.x) < items)
+        issue(blockIdx.x, 0);
 
     const int g = threadIdx.x / T, t = threadIdx.x % T;
     const bool active = g < TY;
     const int ty = active ? g : 0;
     cx<R> *sm = lines + g * G::BUF;
-    cx<R> z[E];
-    packed_row_inverse<N, E, R>(z, wt + (0 * TY + ty) * SC, wt + (1 * TY + ty) * SC, sm, tw, t);
-    R vmax = 0;
-#pragma unroll
-    for (int r = 0; r < E; ++r) {
-        const R u = z[r].x, v = z[r].y;
-        vmax = fmax(vmax, fabs(u) + fabs(v));
-        z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
-    }
-    if (a.cfl_scale > 0) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-            vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-        if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
-            atomicOr(&a.ctl->status, STATUS_CFL);
-    }
-    fft_line<N, E, -1, R>(z, sm, tw, t);
-#pragma unroll
-    for (int r = 0; r < E; ++r)
-        sm[pad<E>(t + r * T)] = z[r];
-    __syncwarp();
-    if (active) {
+    int k = 0;
+    for (int it = blockIdx.x; it < items; it += gridDim.x, ++k) {
+        const int b = k & 1;
+        const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
+        if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items) {
+            fence_proxy_async_shared();
+            issue(it + gridDim.x, b ^ 1);
+        }
+        if (!block_wait(&bars[b], (k >> 1) & 1, &flag)) {
+            if (threadIdx.x == 0)
+                atomicOr(&a.ctl->status, STATUS_TIMEOUT);
+            return;   // uniform across the block
+        }
+        const cx<R> *row = tiles + b * G::TILE + ty * 2 * C;
+        cx<R> z[E];
+        packed_row_inverse<N, E, R>(z, row, row + C, sm, tw, t);
+        R vmax = 0;
 #pragma unroll
         for (int r = 0; r < E; ++r) {
-            const int p = t + r * T;
-            if (p <= K) {
-                const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
-                const cx<R> sa = zk + zc, sb = zk - zc;
-                nlt[p * (TY + 1) + ty] = mk<R>(sa.x / 2, sa.y / 2);                  // P^
-                nlt[(C + p) * (TY + 1) + ty] = mk<R>(sb.y / 2, -sb.x / 2);           // Q^
-            }
+            const R u = z[r].x, v = z[r].y;
+            vmax = fmax(vmax, fabs(u) + fabs(v));
+            z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
         }
-    }
-    __syncthreads();
-    cx<R> *dst = a.nl + static_cast<size_t>(m) * 2 * C * N;
-    for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
-        const int t2 = i % TY, fk = i / TY;
-        dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * (TY + 1) + t2];
+        if (a.cfl_scale > 0) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+            if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
+                atomicOr(&a.ctl->status, STATUS_CFL);
+        }
+        fft_line<N, E, -1, R>(z, sm, tw, t);
+#pragma unroll
+        for (int r = 0; r < E; ++r)
+            sm[pad<E>(t + r * T)] = z[r];
+        __syncwarp();
+        if (active) {
+            static_for<0, E>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
+                using Bd = Band<N, T, r>;
+                if constexpr (Bd::low || Bd::mixed) {
+                    const int p = t + r * T;
+                    if (Bd::low || p <= K) {
+                        const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
+                        const cx<R> sa = zk + zc, sb = zk - zc;
+                        nlt[p * (TY + 1) + ty] = mk<R>(sa.x / 2, sa.y / 2);          // P^
+                        nlt[(C + p) * (TY + 1) + ty] = mk<R>(sb.y / 2, -sb.x / 2);   // Q^
+                    }
+                }
+            });
+        }
+        __syncthreads();
+        cx<R> *dst = a.nl + static_cast<size_t>(m) * 2 * C * N;
+        for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
+            const int t2 = i % TY, fk = i / TY;
+            dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * (TY + 1) + t2];
+        }
+        fence_proxy_async_shared();
+        __syncthreads();
     }
 }
 
 template <typename R, int N> constexpr size_t column_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (N + G::LPB * G::BUF);
+    return sizeof(cx<R>) * (2 * 2 * G::LPB * N + 3 * G::ST_STRIDE + G::LPB * G::BUF + N);
 }
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (N + 2 * G::TY * G::SC + 2 * G::C * (G::TY + 1) + G::GROUPS * G::BUF);
+    return sizeof(cx<R>) * (2 * G::TILE + 2 * G::C * (G::TY + 1) + G::GROUPS * G::BUF + N);
 }
 
 } // namespace hzlb

@@ -50,6 +50,7 @@ template <typename R, int N> struct Cfg {
     // up to whole 16-byte chunks
     static constexpr int PER16 = 16 / (2 * static_cast<int>(sizeof(R)));
     static constexpr int ST_STRIDE = (LPB * LD + PER16 + PER16 - 1) / PER16 * PER16;
+    static constexpr int ST_WORDS = 3 * ST_STRIDE > 2 * LPB * N ? 3 * ST_STRIDE : 2 * LPB * N;
     // row kernel: TY rows per block, one row per group of T threads, 128 threads at least
     static constexpr int TY_RAW = 128 / T;
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
@@ -145,11 +146,13 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD, K = G::K, LPB = G::LPB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    cx<R> *nlbuf = reinterpret_cast<cx<R> *>(smem_raw);          // [2][2][LPB][N]
-    cx<R> *stbuf = nlbuf + 2 * 2 * LPB * N;                        // [3][ST_STRIDE]
-    cx<R> *lines = stbuf + 3 * G::ST_STRIDE;                       // [LPB][BUF]
+    // product input [2][LPB][N]; state window [3][ST_STRIDE], reused as the staging of the
+    // velocity rows [N][2][LPB] once the epilogue has consumed it
+    cx<R> *nlbuf = reinterpret_cast<cx<R> *>(smem_raw);
+    cx<R> *stbuf = nlbuf + 2 * LPB * N;
+    cx<R> *lines = stbuf + G::ST_WORDS;                            // [LPB][BUF]
     cx<R> *tw = lines + LPB * G::BUF;                              // [N]
-    __shared__ __align__(8) uint64_t bars[3];                      // nl[0], nl[1], state
+    __shared__ __align__(8) uint64_t bars[3];                      // nl, (unused), state
     __shared__ int flags[2];
     __shared__ unsigned long long step_sh;
 
@@ -166,14 +169,14 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         tw[i] = a.tw[i];
     __syncthreads();
 
-    auto issue_nl = [&](int it, int b) {
+    auto issue_nl = [&](int it) {
         const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
         const int nl = min(LPB, C - kx0);
         const uint32_t bytes = static_cast<uint32_t>(nl * N * sizeof(cx<R>));
-        mbar_arrive_expect(&bars[b], 2 * bytes);
+        mbar_arrive_expect(&bars[0], 2 * bytes);
         for (int f = 0; f < 2; ++f)
-            bulk_copy_g2s(nlbuf + (b * 2 + f) * LPB * N,
-                          a.nl + ((static_cast<size_t>(m) * 2 + f) * C + kx0) * N, bytes, &bars[b]);
+            bulk_copy_g2s(nlbuf + f * LPB * N,
+                          a.nl + ((static_cast<size_t>(m) * 2 + f) * C + kx0) * N, bytes, &bars[0]);
     };
     // state window of a column group: starts `shift` entries early so that the copy is
     // 16-byte aligned, and covers whole 16-byte chunks
@@ -201,11 +204,10 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     const int line = threadIdx.x / T, t = threadIdx.x % T;
     cx<R> *sm = lines + line * G::BUF;
     if (threadIdx.x == 0 && forward && static_cast<int>(blockIdx.x) < items)
-        issue_nl(blockIdx.x, 0);
+        issue_nl(blockIdx.x);
     bool timed_out = false;
     int k = 0;
     for (int it = blockIdx.x; it < items; it += gridDim.x, ++k) {
-        const int b = k & 1;
         const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
         const int kx = kx0 + line;
         const bool valid = kx < C;
@@ -213,8 +215,6 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         if (threadIdx.x == 0) {
             fence_proxy_async_shared();
             issue_state(it);
-            if (forward && it + static_cast<int>(gridDim.x) < items)
-                issue_nl(it + gridDim.x, b ^ 1);
         }
         int shift;
         uint32_t sbytes;
@@ -237,13 +237,13 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 y[r] = (valid && j >= 0) ? s_w[j] : mk<R>(0, 0);
             });
         } else {
-            if (!block_wait(&bars[b], (k >> 1) & 1, &flags[0])) {
+            if (!block_wait(&bars[0], k & 1, &flags[0])) {
                 timed_out = true;
                 break;
             }
             // forward column FFTs of the product spectra (unnormalised; 1/N^2 below):
             // A^ = -kx ky P^ - (kx^2 - ky^2) Q^ with P = v^2 - u^2, Q = u v
-            const cx<R> *srcP = nlbuf + (b * 2 + 0) * LPB * N + line * N;
+            const cx<R> *srcP = nlbuf + line * N;
             const cx<R> *srcQ = srcP + LPB * N;
             cx<R> adv[E];
 #pragma unroll
@@ -259,6 +259,11 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
 #pragma unroll
             for (int r = 0; r < E; ++r)
                 v[r] = srcQ[t + r * T];
+            // every line has its product inputs in registers: stream the next item's in
+            fence_proxy_async_shared();
+            __syncthreads();
+            if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items)
+                issue_nl(it + gridDim.x);
             fft_line<N, E, -1, R>(v, sm, tw, t);
             if (!block_wait(&bars[2], k & 1, &flags[1])) {
                 timed_out = true;
@@ -327,9 +332,10 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         if (a.emit) {
             // velocity of the next stage input (solver.cpp:177-185): u^ = i ky psi^,
             // v^ = -i kx psi^ with psi^ = w^/k^2; inverse column FFTs, staged in shared memory
-            // (reusing this item's product buffer) as rows [y][field][line]
-            __syncthreads();   // every line is done with the product buffer
-            cx<R> *wst = nlbuf + b * 2 * LPB * N;
+            // (reusing the state window) as rows [y][field][line]
+            fence_proxy_async_shared();
+            __syncthreads();   // every line is done with the state window
+            cx<R> *wst = stbuf;
 #pragma unroll 1
             for (int f = 0; f < 2; ++f) {
                 static_for<0, E>([&](auto rc) {
@@ -525,7 +531,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
 
 template <typename R, int N> constexpr size_t column_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (2 * 2 * G::LPB * N + 3 * G::ST_STRIDE + G::LPB * G::BUF + N);
+    return sizeof(cx<R>) * (2 * G::LPB * N + G::ST_WORDS + G::LPB * G::BUF + N);
 }
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;

@@ -39,6 +39,10 @@ DT = 2.5e-4
 SIGMA = 0.05
 SEED = 42
 METRIC = "ensemble member-steps/s at 256^2"
+# DRAM bytes (read + write) per member per launch, from one ncu capture of 256 members at
+# 256^2 FP32 (profiles/row_kernel_256sq_fp32.md, profiles/column_kernel_256sq_fp32.md); the
+# traffic grows in proportion to the members processed, so a full launch is this x members.
+NCU_TRAFFIC_PER_MEMBER = {"row_kernel": 527182.0, "column_kernel": 846284.0}
 
 
 def peaks():
@@ -239,12 +243,7 @@ def main():
     peak, peak_kind = peaks()
     dom = ("column_kernel", col_gbs, col_bytes, col_ms) if col_ms >= row_ms else \
         ("row_kernel", row_gbs, row_bytes, row_ms)
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        tj = json.loads(tf.read_text())
-        if dom[0] in tj:
-            traffic = tj[dom[0]]["bytes_per_member"] * M
+    traffic = NCU_TRAFFIC_PER_MEMBER[dom[0]] * M
 
     # ---- e2e: host state in/out around every step ---------------------------------
     state_bytes = M * ens.compact_size * cb

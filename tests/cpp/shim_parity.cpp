@@ -1,0 +1,64 @@
+// The reference's own GPU parity check (src/cuda_benchmark.cpp:37-80) run against the B200
+// hzl::CudaSolver shim: the reference CPU Solver and the GPU solver start from the same
+// multimode coefficients, the GPU receives the reference ShellForcing midpoint forcing each
+// step, and the relative L2 difference of the final coefficients is printed (the reference
+// gate is 1e-9).  Usage: shim_parity GRID STEPS DT [SIGMA]
+#include "hzl/cuda_solver.hpp"
+
+#include <cmath>
+#include <cstdlib>
+#include <iostream>
+#include <stdexcept>
+
+int main(int argc, char **argv) {
+    try {
+        if (argc != 4 && argc != 5) {
+            std::cerr << "usage: shim_parity GRID STEPS DT [SIGMA]\n";
+            return 1;
+        }
+        const auto n = static_cast<std::size_t>(std::atol(argv[1]));
+        const auto steps = static_cast<std::size_t>(std::atol(argv[2]));
+        const double dt = std::atof(argv[3]);
+        hzl::Parameters p;
+        p.forcing_sigma = argc == 5 ? std::atof(argv[4]) : 0;
+        p.viscosity = 0.001;
+        hzl::Solver cpu(n, p, 0);
+        cpu.initialize("multimode");
+        hzl::CudaSolver gpu(n, p, cpu.coefficients());
+        hzl::ShellForcing forcing(n, p, 0);
+        for (std::size_t i = 0; i < steps; ++i) {
+            if (p.forcing_sigma > 0)
+                gpu.step(dt, forcing.midpoint_step(dt));
+            else
+                gpu.step(dt);
+        }
+        gpu.synchronize();
+        const auto result = gpu.coefficients();
+        for (std::size_t i = 0; i < steps; ++i)
+            cpu.step(dt);
+        double num = 0, den = 0;
+        for (std::size_t i = 0; i < result.size(); ++i) {
+            num += std::norm(result[i] - cpu.coefficients()[i]);
+            den += std::norm(cpu.coefficients()[i]);
+        }
+        // error semantics: sigma != 0 without forcing must throw invalid_argument
+        bool threw = false;
+        if (p.forcing_sigma > 0) {
+            try {
+                gpu.step(dt);
+            } catch (const std::invalid_argument &) {
+                threw = true;
+            }
+        } else {
+            threw = true;
+        }
+        std::cout.precision(17);
+        std::cout << "{\"n\":" << n << ",\"steps\":" << steps << ",\"relative_l2_error\":"
+                  << std::sqrt(num / den) << ",\"invalid_argument_on_missing_forcing\":"
+                  << (threw ? "true" : "false") << "}\n";
+        return std::sqrt(num / den) <= 1e-9 && threw ? 0 : 2;
+    } catch (const std::exception &e) {
+        std::cerr << "error: " << e.what() << '\n';
+        return 1;
+    }
+}

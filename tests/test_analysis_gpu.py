@@ -1,0 +1,124 @@
+"""Device analysis primitives through the C ABI: observation operator, particle weights and
+systematic resampling (bit-exact with the oracle given identical weights and uniform), member
+gather, inflation, and the batched perturbed-observation EnKF analysis (equal to the
+reference's serial scalar update for one observation; equal to the ensemble-space FP64 formula
+for many)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+from hzl_stochasticflowinference_b200 import sharding
+from oracle.oracle import params6
+
+pytestmark = pytest.mark.gpu
+
+
+def _ensemble(hzlb, n, members, precision=8, seed=3):
+    e = hzlb.Ensemble(hzlb.Config(n=n, members=members, precision=precision, nu=1e-3))
+    w = np.array([hzlb.grf_spectrum(n, seed, m) for m in range(members)])
+    e.set_state(w)
+    return e, w
+
+
+def test_observe_matches_oracle(hzlb, oracle):
+    n, members = 32, 4
+    e, w = _ensemble(hzlb, n, members)
+    xs, ys = np.array([0, 3, 31, 17]), np.array([5, 0, 31, 9])
+    got = e.observe(xs, ys)
+    for m in range(members):
+        phys = oracle.fft(w[m], inverse=True).real
+        np.testing.assert_allclose(got[m], phys[ys, xs], rtol=0, atol=1e-14)
+
+
+def test_device_resampling_bit_exact(hzlb, oracle):
+    e, _ = _ensemble(hzlb, 16, 2048, precision=4)
+    rng = np.random.default_rng(11)
+    for count in (2048,):
+        w = rng.random(count) ** 6
+        w /= w.sum()
+        for u in (0.0, 0.123456789, 1 - 2 ** -53):
+            np.testing.assert_array_equal(e.resample(w, u), oracle.systematic_resample(w, u))
+
+
+def test_gather_members(hzlb):
+    n, members = 16, 5
+    e, w = _ensemble(hzlb, n, members)
+    before = e.get_state_compact()
+    anc = np.array([4, 4, 0, 2, 1], np.uint32)
+    e.gather(anc)
+    np.testing.assert_array_equal(e.get_state_compact(), before[anc])
+
+
+def test_pf_loglik_matches_reference_formula(hzlb, oracle):
+    n, members = 32, 3
+    e, w = _ensemble(hzlb, n, members)
+    xs, ys = np.array([1, 2]), np.array([3, 4])
+    vals, sd = np.array([0.1, -0.2]), np.array([0.3, 0.5])
+    lw = e.pf_loglik(xs, ys, vals, sd, np.log(np.full(members, 1 / members)))
+    for m in range(members):
+        phys = oracle.fft(w[m], inverse=True).real
+        v = np.log(1 / members)
+        for o in range(2):
+            r = (phys[ys[o], xs[o]] - vals[o]) / sd[o]
+            v -= 0.5 * r * r + np.log(sd[o]) + 0.5 * np.log(2 * np.pi)
+        assert abs(lw[m] - v) < 1e-12 * abs(v)
+
+
+def test_inflation(hzlb):
+    n, members = 16, 6
+    e, w = _ensemble(hzlb, n, members)
+    c = e.get_state_compact()
+    e.inflate(1.05)
+    mean = c.mean(axis=0)
+    np.testing.assert_allclose(e.get_state_compact(), mean + 1.05 * (c - mean), rtol=1e-13,
+                               atol=1e-16)
+
+
+def test_enkf_single_observation_equals_serial_update(hzlb, oracle):
+    """One scalar observation: the batched analysis equals the reference's serial update
+    (filter.cpp:265-321), restated by the oracle, given the same perturbations."""
+    n, members = 32, 16
+    e, w = _ensemble(hzlb, n, members)
+    xs, ys = np.array([7]), np.array([11])
+    value, sd = np.array([0.05]), np.array([0.2])
+    eps = np.random.default_rng(2).normal(size=(members, 1))
+    pred = e.observe(xs, ys)[:, 0]
+    solvers = []
+    for m in range(members):
+        s = oracle.solver(n, params6(1e-3, 0.0, 0.0, 0.5, 2, 3), 0)
+        s.set_state(w[m], np.zeros((n, n), np.complex128))
+        solvers.append(s)
+    import ctypes as C
+    arr = (C.c_void_p * members)(*[s.h.value for s in solvers])
+    pred_c = np.ascontiguousarray(pred)
+    eps_c = np.ascontiguousarray(eps[:, 0])
+    oracle.check(oracle.lib.ho_enkf_scalar_update(members, arr, pred_c.ctypes.data_as(C.POINTER(C.c_double)),
+                                                  float(value[0]), float(sd[0]),
+                                                  eps_c.ctypes.data_as(C.POINTER(C.c_double))))
+    e.enkf_analysis(xs, ys, value, sd, eps)
+    got = e.get_state()
+    for m in range(members):
+        assert rel_l2(got[m], solvers[m].state()[0]) < 1e-12
+
+
+@pytest.mark.parametrize("precision,tol", [(8, 1e-11), (4, 2e-5)])
+def test_enkf_batch_many_observations(hzlb, precision, tol):
+    """p = 64 observations at once against X + A W with W from the FP64 ensemble-space formula."""
+    n, members, p = 64, 48, 64
+    e, w = _ensemble(hzlb, n, members, precision=precision)
+    rng = np.random.default_rng(9)
+    xs, ys = rng.integers(0, n, p), rng.integers(0, n, p)
+    vals, sd = rng.normal(0, 0.1, p), np.full(p, 0.1)
+    eps = rng.normal(size=(members, p))
+    hx = e.observe(xs, ys)
+    x = e.get_state_compact().astype(np.complex128)
+    W = sharding.enkf_weight_matrix(hx, vals, sd, eps)
+    expect = x + ((x - x.mean(axis=0)).T @ W).T
+    e.enkf_analysis(xs, ys, vals, sd, eps)
+    got = e.get_state_compact().astype(np.complex128)
+    assert rel_l2(got, expect) < tol
+    # the analysis pulls the ensemble mean towards the observations
+    after = e.observe(xs, ys).mean(axis=0)
+    assert np.linalg.norm(after - vals) < np.linalg.norm(hx.mean(axis=0) - vals)

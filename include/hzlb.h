@@ -218,6 +218,25 @@ HZLB_API int hzlb_ensemble_kalman_filter(const hzlb_dataset *data, const hzlb_pa
                                          int device, hzlb_enkf_record *records, size_t capacity,
                                          size_t *nrecords, double *mean_vorticity);
 
+/* ---- stepping without device allocation ------------------------------------------- */
+/* No counterpart in the reference.  For callers that may not allocate GPU memory while they
+ * run (device memory owned and budgeted by the application's own pool, or a hot loop where an
+ * allocation and its possible failure are not acceptable): the same RK4 step as hzlb_step,
+ * with every scratch buffer taken from one device array of HZLB_NOALLOC_SCRATCH_BYTES built
+ * into the library (held on every GPU that loads the library's device code until exit).
+ * state: device pointer, members x hzlb_compact_size() complex entries in the compact layout
+ * of the configured precision, advanced in place by nsteps steps of dt; forcing: device
+ * pointer in the compact forcing layout (columns kx <= forcing_kmax, one field or one per
+ * member) or NULL; first_step: noise counter of the first step; stream: a cudaStream_t or
+ * NULL; status: if non-NULL, the call waits for the stream and stores the HZLB_STATUS_* bits.
+ * Sizes whose scratch exceeds the limit are HZLB_EINVAL.  The first call on a device resolves
+ * the array's device address and configures the kernels; make it before any stream capture.
+ * Calls share the array, so calls that overlap on the GPU race: serialise them. */
+#define HZLB_NOALLOC_SCRATCH_BYTES (32u << 20)
+HZLB_API int hzlb_step_noalloc(const hzlb_config *config, double dt, uint64_t nsteps,
+                               uint64_t first_step, void *state, const void *forcing, void *stream,
+                               uint32_t *status);
+
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */
 /* Gaussian random vorticity spectrum, E(k) ~ k^4 exp(-(k/6)^2), unit enstrophy, retained modes

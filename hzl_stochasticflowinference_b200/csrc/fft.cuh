@@ -75,13 +75,49 @@ template <int N, int E> struct FftShape {
     static_assert(T >= 1 && T <= 32, "a line must fit in one warp");
 };
 
-// One Stockham pass with stride NS; recursion over the remaining passes.
+// Between-pass twiddles laid out per pass as [q][r-1][t] (t fastest), so the T threads of a
+// line read consecutive entries (no bank conflicts, unlike reading W_N^(k r) with stride r).
+template <int N, int E, int NS> struct PassTw {
+    static constexpr int T = N / E;
+    static constexpr int RAD = (E < N / NS) ? E : N / NS;
+    static constexpr int NB = E / RAD;
+    static constexpr bool LAST = NS * RAD == N;
+    static constexpr int own = NS > 1 ? NB * (RAD - 1) * T : 0;   // entries of this pass
+    static constexpr int rest() {
+        if constexpr (LAST)
+            return 0;
+        else
+            return PassTw<N, E, NS * RAD>::own + PassTw<N, E, NS * RAD>::rest();
+    }
+    static constexpr int total = own + rest();                     // this and later passes
+};
+template <int N, int E> constexpr int pass_twiddle_entries() { return PassTw<N, E, 1>::total; }
+
+// Fills the per-pass table (cooperatively, all threads of the block) from the base table
+// base[k] = W_N^k = exp(-2 pi i k / N).
+template <int N, int E, typename R, int NS = 1>
+__device__ __forceinline__ void load_pass_twiddles(cx<R> *dst, const cx<R> *base) {
+    using P = PassTw<N, E, NS>;
+    if constexpr (NS > 1) {
+        for (int e = threadIdx.x; e < P::own; e += blockDim.x) {
+            const int t = e % P::T, qr = e / P::T, r = qr % (P::RAD - 1) + 1, q = qr / (P::RAD - 1);
+            const int j = t + q * P::T, k = j & (NS - 1);
+            dst[e] = base[(k * r) * (N / (NS * P::RAD))];
+        }
+    }
+    if constexpr (!P::LAST)
+        load_pass_twiddles<N, E, R, NS * P::RAD>(dst + P::own, base);
+}
+
+// One Stockham pass with stride NS; recursion over the remaining passes.  `tw` points at this
+// pass's entries of the per-pass twiddle table.
 template <int N, int E, int SIGN, typename R, int NS>
 __device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *tw, int t) {
     constexpr int T = N / E;
-    constexpr int RAD = (E < N / NS) ? E : N / NS;
-    constexpr int NB = E / RAD;
-    constexpr bool LAST = NS * RAD == N;
+    using P = PassTw<N, E, NS>;
+    constexpr int RAD = P::RAD;
+    constexpr int NB = P::NB;
+    constexpr bool LAST = P::LAST;
 #pragma unroll
     for (int q = 0; q < NB; ++q) {
         const int j = t + q * T;
@@ -93,7 +129,7 @@ __device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *
         if constexpr (NS > 1) {
 #pragma unroll
             for (int r = 1; r < RAD; ++r) {
-                cx<R> w = tw[(k * r) * (N / (NS * RAD))];
+                cx<R> w = tw[(q * (RAD - 1) + (r - 1)) * T + t];
                 if constexpr (SIGN > 0)
                     w.y = -w.y;
                 u[r] = cmul(u[r], w);
@@ -117,13 +153,14 @@ __device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *
         for (int r = 0; r < E; ++r)
             v[r] = sm[pad<E>(t + r * T)];
         __syncwarp();
-        fft_pass<N, E, SIGN, R, NS * RAD>(v, sm, tw, t);
+        fft_pass<N, E, SIGN, R, NS * RAD>(v, sm, tw + P::own, t);
     }
 }
 
 // Unnormalised DFT of one line: X[k] = sum_n x[n] exp(SIGN 2 pi i n k / N).
 // Thread t (0 <= t < N/E) holds x[t + r*(N/E)] in v[r] on entry and X[t + r*(N/E)] on exit.
-// Every lane of the warp must call this together (warp-synchronous exchanges).
+// `tw` is the per-pass twiddle table (load_pass_twiddles).  Every lane of the warp must call
+// this together (warp-synchronous exchanges).
 template <int N, int E, int SIGN, typename R>
 __device__ __forceinline__ void fft_line(cx<R> (&v)[E], cx<R> *sm, const cx<R> *tw, int t) {
     (void)FftShape<N, E>::T;

@@ -12,8 +12,8 @@ template <typename R, int N> struct L {
     using G = Cfg<R, N>;
     static constexpr size_t col_smem = hzlb::column_smem<R, N>();
     static constexpr size_t row_smem = hzlb::row_smem<R, N>();
-    static constexpr size_t prow_smem = sizeof(cx<R>) * (N + G::GROUPS * G::BUF);
-    static constexpr size_t pcol_smem = sizeof(cx<R>) * (N + G::LPB * G::BUF);
+    static constexpr size_t prow_smem = sizeof(cx<R>) * (G::TWE + G::GROUPS * G::BUF);
+    static constexpr size_t pcol_smem = sizeof(cx<R>) * (G::TWE + G::LPB * G::BUF);
     static_assert(row_smem <= 227 * 1024, "row kernel shared memory");
 
     // persistent grids: resident blocks per SM x SMs, per device

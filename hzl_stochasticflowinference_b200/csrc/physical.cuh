@@ -15,9 +15,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *lines = tw + N;
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        tw[i] = tw_g[i];
+    cx<R> *lines = tw + G::TWE;
+    load_pass_twiddles<N, G::E, R>(tw, tw_g);
     __syncthreads();
     const int line = threadIdx.x / T, t = threadIdx.x % T;
     const int kx = blockIdx.y * G::LPB + line, m = blockIdx.x;
@@ -48,9 +47,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *lines = tw + N;
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        tw[i] = tw_g[i];
+    cx<R> *lines = tw + G::TWE;
+    load_pass_twiddles<N, G::E, R>(tw, tw_g);
     __syncthreads();
     const int g = threadIdx.x / T, t = threadIdx.x % T, m = blockIdx.x;
     const bool active = g < TY / 2;
@@ -94,9 +92,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *lines = tw + N;
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        tw[i] = tw_g[i];
+    cx<R> *lines = tw + G::TWE;
+    load_pass_twiddles<N, G::E, R>(tw, tw_g);
     __syncthreads();
     const int g = threadIdx.x / T, t = threadIdx.x % T, m = blockIdx.x;
     const bool active = g < TY / 2;

@@ -50,13 +50,16 @@ template <typename R, int N> struct Cfg {
     // up to whole 16-byte chunks
     static constexpr int PER16 = 16 / (2 * static_cast<int>(sizeof(R)));
     static constexpr int ST_STRIDE = (LPB * LD + PER16 + PER16 - 1) / PER16 * PER16;
-    static constexpr int ST_WORDS = 3 * ST_STRIDE > 2 * LPB * N ? 3 * ST_STRIDE : 2 * LPB * N;
+    static constexpr int ST_WORDS = 3 * ST_STRIDE > N * (2 * LPB + 1) ? 3 * ST_STRIDE : N * (2 * LPB + 1);
     // row kernel: TY rows per block, one row per group of T threads, 128 threads at least
     static constexpr int TY_RAW = 128 / T;
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
     static constexpr int GROUPS = TY * T >= 32 ? TY : 32 / T;
     static constexpr int ROW_THREADS = GROUPS * T;
     static constexpr int TILE = TY * 2 * C;           // row tile, complex entries
+    static constexpr int TWE = pass_twiddle_entries<N, E>() > 0 ? pass_twiddle_entries<N, E>() : 1;
+    // velocity staging [y][field][line] with an odd row stride (bank spread)
+    static constexpr int WSY = 2 * LPB + 1;
 };
 
 struct StepControl {
@@ -151,7 +154,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     cx<R> *nlbuf = reinterpret_cast<cx<R> *>(smem_raw);
     cx<R> *stbuf = nlbuf + 2 * LPB * N;
     cx<R> *lines = stbuf + G::ST_WORDS;                            // [LPB][BUF]
-    cx<R> *tw = lines + LPB * G::BUF;                              // [N]
+    cx<R> *tw = lines + LPB * G::BUF;                              // [TWE] per-pass twiddles
     __shared__ __align__(8) uint64_t bars[3];                      // nl, (unused), state
     __shared__ int flags[2];
     __shared__ unsigned long long step_sh;
@@ -165,8 +168,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         mbar_init_fence();
         step_sh = a.ctl->step;
     }
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        tw[i] = a.tw[i];
+    load_pass_twiddles<N, E, R>(tw, a.tw);
     __syncthreads();
 
     auto issue_nl = [&](int it) {
@@ -354,7 +356,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 fft_line<N, E, +1, R>(v, sm, tw, t);
 #pragma unroll
                 for (int r = 0; r < E; ++r)
-                    wst[((t + r * T) * 2 + f) * LPB + line] = v[r];
+                    wst[(t + r * T) * G::WSY + f * LPB + line] = v[r];
             }
             __syncthreads();
             const int nl = min(LPB, C - kx0);
@@ -362,7 +364,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             for (int i = threadIdx.x; i < N * 2 * LPB; i += blockDim.x) {
                 const int l = i % LPB, yf = i / LPB;
                 if (l < nl)
-                    dst[static_cast<size_t>(yf) * C + l] = wst[i];
+                    dst[static_cast<size_t>(yf) * C + l] = wst[(yf >> 1) * G::WSY + (yf & 1) * LPB + l];
             }
         }
         fence_proxy_async_shared();   // this thread's shared-memory accesses precede the next bulk copies
@@ -440,7 +442,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
     cx<R> *tiles = reinterpret_cast<cx<R> *>(smem_raw);   // [2][TY][2][C]
     cx<R> *nlt = tiles + 2 * G::TILE;                      // [2][C][TY+1]
     cx<R> *lines = nlt + 2 * C * (TY + 1);                 // [GROUPS][BUF]
-    cx<R> *tw = lines + G::GROUPS * G::BUF;                // [N]
+    cx<R> *tw = lines + G::GROUPS * G::BUF;                // [TWE] per-pass twiddles
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int flag;
     constexpr int tiles_per_member = N / TY;
@@ -452,8 +454,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         mbar_init(&bars[1], 1);
         mbar_init_fence();
     }
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        tw[i] = a.tw[i];
+    load_pass_twiddles<N, E, R>(tw, a.tw);
     __syncthreads();
     auto issue = [&](int it, int b) {
         const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
@@ -531,11 +532,11 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
 
 template <typename R, int N> constexpr size_t column_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (2 * G::LPB * N + G::ST_WORDS + G::LPB * G::BUF + N);
+    return sizeof(cx<R>) * (2 * G::LPB * N + G::ST_WORDS + G::LPB * G::BUF + G::TWE);
 }
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (2 * G::TILE + 2 * G::C * (G::TY + 1) + G::GROUPS * G::BUF + N);
+    return sizeof(cx<R>) * (2 * G::TILE + 2 * G::C * (G::TY + 1) + G::GROUPS * G::BUF + G::TWE);
 }
 
 } // namespace hzlb

@@ -50,7 +50,7 @@ template <typename R, int N> struct Cfg {
     // up to whole 16-byte chunks
     static constexpr int PER16 = 16 / (2 * static_cast<int>(sizeof(R)));
     static constexpr int ST_STRIDE = (LPB * LD + PER16 + PER16 - 1) / PER16 * PER16;
-    static constexpr int ST_WORDS = 3 * ST_STRIDE > N * (2 * LPB + 1) ? 3 * ST_STRIDE : N * (2 * LPB + 1);
+    static constexpr int ST_WORDS = 3 * ST_STRIDE > 2 * LPB * N ? 3 * ST_STRIDE : 2 * LPB * N;
     // row kernel: TY rows per block, one row per group of T threads, 128 threads at least
     static constexpr int TY_RAW = 128 / T;
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
@@ -58,9 +58,17 @@ template <typename R, int N> struct Cfg {
     static constexpr int ROW_THREADS = GROUPS * T;
     static constexpr int TILE = TY * 2 * C;           // row tile, complex entries
     static constexpr int TWE = pass_twiddle_entries<N, E>() > 0 ? pass_twiddle_entries<N, E>() : 1;
-    // velocity staging [y][field][line] with an odd row stride (bank spread)
-    static constexpr int WSY = 2 * LPB + 1;
 };
+
+// XOR swizzle of a [row][S] staging array (S a power of two): entry c of row y is stored at
+// y*S + (c ^ swz(y)), which spreads 16 consecutive rows of one column over distinct 8-byte bank
+// slots while keeping each row contiguous (a permutation within the row).
+template <int S> __device__ __forceinline__ int swz(int y) {
+    if constexpr (S <= 16)
+        return ((y * S) >> 4) & (S - 1);
+    else
+        return y & 15;
+}
 
 struct StepControl {
     unsigned long long step;   // index of the step being taken (noise counter)
@@ -338,33 +346,47 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             fence_proxy_async_shared();
             __syncthreads();   // every line is done with the state window
             cx<R> *wst = stbuf;
+            // psi^ = w^ / k^2 once per mode (k = 0 gives 0), then u^ and v^ from it
+            static_for<0, E>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
+                const int j = band_j<N, T, r>(t + r * T);
+                cx<R> psi = mk<R>(0, 0);
+                if (j >= 0) {
+                    const int ky = j <= K ? j : j - LD;
+                    const int k2 = kxc * kxc + ky * ky;
+                    if (k2 > 0) {
+                        const R inv = static_cast<R>(1) / static_cast<R>(k2);
+                        psi = mk<R>(y[r].x * inv, y[r].y * inv);
+                    }
+                }
+                y[r] = psi;
+            });
 #pragma unroll 1
             for (int f = 0; f < 2; ++f) {
                 static_for<0, E>([&](auto rc) {
                     constexpr int r = decltype(rc)::value;
-                    cx<R> z = mk<R>(0, 0);
-                    const int j = band_j<N, T, r>(t + r * T);
-                    if (j >= 0) {
-                        const int ky = j <= K ? j : j - LD;
-                        const R kyr = static_cast<R>(ky);
-                        const R k2 = static_cast<R>(kxc * kxc + ky * ky);
-                        const cx<R> psi = k2 > 0 ? mk<R>(y[r].x / k2, y[r].y / k2) : mk<R>(0, 0);
-                        z = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
-                    }
-                    v[r] = z;
+                    const int p = t + r * T;
+                    const int ky = Band<N, T, r>::low ? p : (Band<N, T, r>::high ? p - N : (p <= K ? p : p - N));
+                    const R kyr = static_cast<R>(ky);
+                    const cx<R> psi = y[r];
+                    v[r] = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
                 });
                 fft_line<N, E, +1, R>(v, sm, tw, t);
 #pragma unroll
-                for (int r = 0; r < E; ++r)
-                    wst[(t + r * T) * G::WSY + f * LPB + line] = v[r];
+                for (int r = 0; r < E; ++r) {
+                    const int yy = t + r * T;
+                    wst[yy * 2 * LPB + ((f * LPB + line) ^ swz<2 * LPB>(yy))] = v[r];
+                }
             }
             __syncthreads();
             const int nl = min(LPB, C - kx0);
             cx<R> *dst = a.w + static_cast<size_t>(m) * N * 2 * C + kx0;
             for (int i = threadIdx.x; i < N * 2 * LPB; i += blockDim.x) {
                 const int l = i % LPB, yf = i / LPB;
+                const int yy = yf >> 1;
                 if (l < nl)
-                    dst[static_cast<size_t>(yf) * C + l] = wst[(yf >> 1) * G::WSY + (yf & 1) * LPB + l];
+                    dst[static_cast<size_t>(yf) * C + l] =
+                        wst[yy * 2 * LPB + (((yf & 1) * LPB + l) ^ swz<2 * LPB>(yy))];
             }
         }
         fence_proxy_async_shared();   // this thread's shared-memory accesses precede the next bulk copies
@@ -439,9 +461,10 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    cx<R> *tiles = reinterpret_cast<cx<R> *>(smem_raw);   // [2][TY][2][C]
-    cx<R> *nlt = tiles + 2 * G::TILE;                      // [2][C][TY+1]
-    cx<R> *lines = nlt + 2 * C * (TY + 1);                 // [GROUPS][BUF]
+    // input tiles [2][TY][2][C]; once a tile is packed into registers its buffer holds the
+    // product spectra [2C][TY] (swizzled rows) until they are stored
+    cx<R> *tiles = reinterpret_cast<cx<R> *>(smem_raw);
+    cx<R> *lines = tiles + 2 * G::TILE;                    // [GROUPS][BUF]
     cx<R> *tw = lines + G::GROUPS * G::BUF;                // [TWE] per-pass twiddles
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int flag;
@@ -503,7 +526,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
 #pragma unroll
         for (int r = 0; r < E; ++r)
             sm[pad<E>(t + r * T)] = z[r];
-        __syncwarp();
+        __syncthreads();   // every group has packed its row: the tile buffer takes the products
+        cx<R> *nlt = tiles + b * G::TILE;
         if (active) {
             static_for<0, E>([&](auto rc) {
                 constexpr int r = decltype(rc)::value;
@@ -513,8 +537,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
                     if (Bd::low || p <= K) {
                         const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
                         const cx<R> sa = zk + zc, sb = zk - zc;
-                        nlt[p * (TY + 1) + ty] = mk<R>(sa.x / 2, sa.y / 2);          // P^
-                        nlt[(C + p) * (TY + 1) + ty] = mk<R>(sb.y / 2, -sb.x / 2);   // Q^
+                        nlt[p * TY + (ty ^ swz<TY>(p))] = mk<R>(sa.x / 2, sa.y / 2);          // P^
+                        nlt[(C + p) * TY + (ty ^ swz<TY>(C + p))] = mk<R>(sb.y / 2, -sb.x / 2);   // Q^
                     }
                 }
             });
@@ -523,7 +547,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         cx<R> *dst = a.nl + static_cast<size_t>(m) * 2 * C * N;
         for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
             const int t2 = i % TY, fk = i / TY;
-            dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * (TY + 1) + t2];
+            dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * TY + (t2 ^ swz<TY>(fk))];
         }
         fence_proxy_async_shared();
         __syncthreads();
@@ -536,7 +560,7 @@ template <typename R, int N> constexpr size_t column_smem() {
 }
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (2 * G::TILE + 2 * G::C * (G::TY + 1) + G::GROUPS * G::BUF + G::TWE);
+    return sizeof(cx<R>) * (2 * G::TILE + G::GROUPS * G::BUF + G::TWE);
 }
 
 } // namespace hzlb

@@ -218,6 +218,16 @@ HZLB_API int hzlb_ensemble_kalman_filter(const hzlb_dataset *data, const hzlb_pa
                                          int device, hzlb_enkf_record *records, size_t capacity,
                                          size_t *nrecords, double *mean_vorticity);
 
+/* ---- tensor-core contractions ------------------------------------------------------ */
+/* C[M x N] = alpha * opA * opB^T + beta * C on the tcgen05 tensor cores with FP32 accumulation
+ * (device pointers, asynchronous on `stream`).  dtype 2: A and B are BF16; dtype 4: A and B are
+ * FP32 read as TF32.  opA is M x K: A[m*lda + k] when a_kcontig, else A[k*lda + m]; opB is
+ * N x K likewise.  Used by the learned forecast and the ensemble-space analysis products; no
+ * counterpart in the reference (whose filter updates are per-scalar loops). */
+HZLB_API int hzlb_gemm(int M, int N, int K, int dtype, const void *A, long long lda, int a_kcontig,
+                       const void *B, long long ldb, int b_kcontig, float *C, long long ldc,
+                       float alpha, float beta, void *stream);
+
 /* ---- stepping without device allocation ------------------------------------------- */
 /* No counterpart in the reference.  For callers that may not allocate GPU memory while they
  * run (device memory owned and budgeted by the application's own pool, or a hot loop where an

@@ -1,6 +1,7 @@
 // Ensemble engine: owns the device state of one handle and schedules the kernels.
 #include "engine.h"
 #include "filters.cuh"
+#include "umma_gemm.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -627,19 +628,57 @@ template <typename R> class EngineT final : public Engine {
         cholesky_solve<<<(M_ + 127) / 128, 128, 0, stream_>>>(P, pi, d, M_);
         enkf_weights<<<dim3((M_ + 15) / 16, (M_ + 15) / 16), dim3(16, 16), 0, stream_>>>(ha, d, M_, pi, W);
         cuda_check(cudaGetLastError(), "launch EnKF analysis");
-        // X_a = X + (X - mean) W, written to the stage buffer then committed
         cx<R> *mean = acc_.as<cx<R>>();   // free between steps
         const int mb = static_cast<int>(std::min<size_t>((compact_ + 255) / 256, 4096));
         ensemble_mean<R><<<mb, 256, 0, stream_>>>(omega_.as<cx<R>>(), static_cast<long long>(compact_),
                                                   M_, mean);
-        const dim3 ug(static_cast<unsigned>((compact_ + 63) / 64), (M_ + 15) / 16);
-        anomaly_update<R><<<ug, 64, 0, stream_>>>(omega_.as<cx<R>>(), mean, W,
-                                                  static_cast<long long>(compact_), M_,
-                                                  ystage_.as<cx<R>>());
-        cuda_check(cudaGetLastError(), "launch EnKF update");
-        cuda_check(cudaMemcpyAsync(omega_.ptr, ystage_.ptr, sizeof(cx<R>) * compact_ * M_,
-                                   cudaMemcpyDeviceToDevice, stream_),
-                   "commit EnKF update");
+        if constexpr (sizeof(R) == 4) {
+            // X_a = X + A W on the tensor cores: A = X - mean and W split for 3xTF32
+            // (hi*hi + hi*lo + lo*hi), accumulated into X in place
+            const long long n = 2 * static_cast<long long>(compact_);
+            float *x = reinterpret_cast<float *>(omega_.ptr);
+            float *ahi = reinterpret_cast<float *>(ystage_.ptr);
+            float *alo = reinterpret_cast<float *>(w_.ptr);   // velocity rows: free between steps
+            float *mf = reinterpret_cast<float *>(nl_.ptr);
+            cuda_check(cudaMemcpyAsync(mf, mean, sizeof(float) * n, cudaMemcpyDeviceToDevice, stream_),
+                       "stage ensemble mean");
+            split_.ensure(sizeof(float) * 2 * static_cast<size_t>(M_) * M_, "allocate weight split");
+            float *whi = split_.as<float>(), *wlo = whi + static_cast<size_t>(M_) * M_;
+            anomaly_split_tf32<<<2048, 256, 0, stream_>>>(x, mf, n, M_, ahi, alo);
+            split_tf32<<<256, 256, 0, stream_>>>(W, static_cast<long long>(M_) * M_, whi, wlo);
+            cuda_check(cudaGetLastError(), "launch 3xTF32 split");
+            const float *wa[3] = {whi, whi, wlo};
+            const float *aa[3] = {ahi, alo, ahi};
+            for (int i = 0; i < 3; ++i) {
+                tc::GemmArgs g{};
+                g.M = M_;
+                g.N = static_cast<int>(n);
+                g.K = M_;
+                g.A = wa[i];           // opA[m][a] = W[a][m]
+                g.lda = M_;
+                g.a_kcontig = 0;
+                g.B = aa[i];           // opB[e][a] = A[a][e]
+                g.ldb = n;
+                g.b_kcontig = 0;
+                g.C = x;
+                g.ldc = n;
+                g.alpha = 1.0f;
+                g.beta = 1.0f;
+                g.epilogue = tc::EPI_NONE;
+                g.status = &ctl_.as<StepControl>()->status;
+                cuda_check(gemm(g, 4, stream_), "launch tensor-core EnKF update");
+            }
+        } else {
+            // FP64 path: X_a = X + (X - mean) W with FP64 accumulation
+            const dim3 ug(static_cast<unsigned>((compact_ + 63) / 64), (M_ + 15) / 16);
+            anomaly_update<R><<<ug, 64, 0, stream_>>>(omega_.as<cx<R>>(), mean, W,
+                                                      static_cast<long long>(compact_), M_,
+                                                      ystage_.as<cx<R>>());
+            cuda_check(cudaGetLastError(), "launch EnKF update");
+            cuda_check(cudaMemcpyAsync(omega_.ptr, ystage_.ptr, sizeof(cx<R>) * compact_ * M_,
+                                       cudaMemcpyDeviceToDevice, stream_),
+                       "commit EnKF update");
+        }
         int host_info = 0;
         cuda_check(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, stream_),
                    "read Cholesky status");
@@ -660,7 +699,7 @@ template <typename R> class EngineT final : public Engine {
     size_t compact_ = 0;
     cudaStream_t stream_ = nullptr;
     DeviceBuffer omega_, ystage_, acc_, w_, nl_, forcing_, ctl_, tw_, phys_, scratch_d_, vbits_,
-        obs_xy_, obs_, anc_, enkf_, aux_;
+        obs_xy_, obs_, anc_, enkf_, aux_, split_;
     PinnedBuffer staging_, fstage_[2];
     cudaEvent_t fevent_[2] = {nullptr, nullptr};
     int fbuf_next_ = 0;

@@ -106,6 +106,12 @@ class Engine {
 
 std::unique_ptr<Engine> make_engine(const hzlb_config &c);
 
+// Tensor-core GEMM launcher (gemm.cu); dtype 2 = BF16 operands, 4 = FP32 read as TF32.
+namespace tc {
+struct GemmArgs;
+}
+cudaError_t gemm(const tc::GemmArgs &g, int dtype, cudaStream_t s);
+
 // Message returned by hzlb_last_error() on this thread.
 void set_last_error(const std::string &message);
 

@@ -230,6 +230,35 @@ __global__ void anomaly_update(const cx<R> *x, const cx<R> *mean, const double *
 } // namespace hzlb
 
 namespace hzlb {
+// Round-to-nearest FP32 -> TF32 (10-bit mantissa), kept in an FP32 container.
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+// Split for 3xTF32 products: A = hi + lo with hi exactly representable in TF32; the products
+// hi*hi + hi*lo + lo*hi recover FP32-level accuracy on the tensor cores.
+// Anomalies a = x - mean of the member-major state (members x n reals).
+__global__ void anomaly_split_tf32(const float *x, const float *mean, long long n, int members,
+                                   float *hi, float *lo) {
+    const long long total = n * members;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float a = x[i] - mean[i % n];
+        const float h = to_tf32(a);
+        hi[i] = h;
+        lo[i] = a - h;
+    }
+}
+__global__ void split_tf32(const double *w, long long count, float *hi, float *lo) {
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float v = static_cast<float>(w[i]);
+        const float h = to_tf32(v);
+        hi[i] = h;
+        lo[i] = v - h;
+    }
+}
 // out[e] = sum over members (in member order) of w[m] x[m][e], or of x[m][e] / divisor when
 // divisor > 0 (the reference's mean accumulates coefficient / count, filter.cpp:238-243).
 template <typename R>

@@ -35,6 +35,7 @@ STATUS_CFL, STATUS_NONFINITE, STATUS_TIMEOUT = 1, 2, 4
 
 _dp = C.POINTER(C.c_double)
 _u32p = C.POINTER(C.c_uint32)
+_fp = C.POINTER(C.c_float)
 
 
 class hzlb_config(C.Structure):
@@ -146,6 +147,15 @@ def library() -> C.CDLL:
                                                   C.c_int, C.c_int, C.POINTER(hzlb_enkf_record),
                                                   C.c_size_t, C.POINTER(C.c_size_t), _dp]),
         "hzlb_kolmogorov_forcing": (C.c_int, [C.c_int, C.c_double, C.c_int, _dp]),
+        "hzlb_mlp_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                      C.POINTER(vp)]),
+        "hzlb_mlp_destroy": (None, [vp]),
+        "hzlb_mlp_param_count": (C.c_size_t, [vp]),
+        "hzlb_mlp_set_params": (C.c_int, [vp, _fp]),
+        "hzlb_mlp_get_params": (C.c_int, [vp, _fp, _fp]),
+        "hzlb_mlp_set_scales": (C.c_int, [vp, _fp, _fp]),
+        "hzlb_mlp_forward": (C.c_int, [vp, vp, C.c_int, vp, vp]),
+        "hzlb_mlp_train_step": (C.c_int, [vp, vp, vp, C.c_int, C.c_float, _dp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -487,3 +497,86 @@ def ensemble_kalman_filter(ds: dict, p: Parameters, members: int, seed: int,
     rec = np.array([[recs[i].step, recs[i].forecast_sensor_rmse, recs[i].posterior_spread,
                      recs[i].is_forecast] for i in range(k)])
     return dict(records=rec.reshape(-1, 4), means=means[:k].copy())
+
+
+class Mlp:
+    """Learned reduced forecast network (hzlb_mlp_*): r POD coefficients plus q noise-mode
+    amplitudes -> r coefficients one window later, BF16 on the tcgen05 tensor cores.  Batches
+    are CUDA tensors (torch) of FP32, row-major [batch][features]."""
+
+    def __init__(self, r: int, q: int, hidden: int, max_batch: int, seed: int = 0,
+                 device: int = 0):
+        self._lib = library()
+        self._h = C.c_void_p()
+        _check(self._lib.hzlb_mlp_create(r, q, hidden, max_batch, device, seed,
+                                         C.byref(self._h)))
+        self.r, self.q, self.hidden, self.max_batch = r, q, hidden, max_batch
+        self.count = int(self._lib.hzlb_mlp_param_count(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.hzlb_mlp_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def layout(self) -> dict:
+        """Offsets and shapes of W1, W2, W3, b1, b2, b3 in the parameter vector."""
+        i, h, r = self.r + self.q, self.hidden, self.r
+        shapes = [("W1", (h, i)), ("W2", (h, h)), ("W3", (r, h)), ("b1", (h,)), ("b2", (h,)),
+                  ("b3", (r,))]
+        out, off = {}, 0
+        for name, shp in shapes:
+            size = int(np.prod(shp))
+            out[name] = (off, shp)
+            off += size
+        return out
+
+    def unpack(self, flat: np.ndarray) -> dict:
+        return {k: flat[o:o + int(np.prod(s))].reshape(s) for k, (o, s) in self.layout().items()}
+
+    def pack(self, parts: dict) -> np.ndarray:
+        flat = np.zeros(self.count, np.float32)
+        for k, (o, s) in self.layout().items():
+            flat[o:o + int(np.prod(s))] = np.asarray(parts[k], np.float32).ravel()
+        return flat
+
+    def set_params(self, flat) -> None:
+        a = np.ascontiguousarray(flat, np.float32)
+        if a.size != self.count:
+            raise ValueError(f"expected {self.count} parameters")
+        _check(self._lib.hzlb_mlp_set_params(self._h, a.ctypes.data_as(_fp)))
+
+    def params(self, grads: bool = False):
+        p = np.zeros(self.count, np.float32)
+        g = np.zeros(self.count, np.float32) if grads else None
+        _check(self._lib.hzlb_mlp_get_params(self._h, p.ctypes.data_as(_fp),
+                                             g.ctypes.data_as(_fp) if grads else None))
+        return (p, g) if grads else p
+
+    def set_scales(self, s_in, s_out) -> None:
+        a = np.ascontiguousarray(s_in, np.float32)
+        b = np.ascontiguousarray(s_out, np.float32)
+        if a.size != self.r + self.q or b.size != self.r:
+            raise ValueError("scale sizes must be r+q and r")
+        _check(self._lib.hzlb_mlp_set_scales(self._h, a.ctypes.data_as(_fp), b.ctypes.data_as(_fp)))
+
+    @staticmethod
+    def _dev(t, cols: int):
+        if not (t.is_cuda and t.dtype.is_floating_point and t.element_size() == 4 and
+                t.is_contiguous() and t.dim() == 2 and t.shape[1] == cols):
+            raise ValueError(f"expected a contiguous CUDA float32 [batch][{cols}] tensor")
+        return C.c_void_p(t.data_ptr())
+
+    def forward(self, x, out=None):
+        import torch
+        if out is None:
+            out = torch.empty((x.shape[0], self.r), dtype=torch.float32, device=x.device)
+        _check(self._lib.hzlb_mlp_forward(self._h, self._dev(x, self.r + self.q), x.shape[0],
+                                          self._dev(out, self.r), None))
+        return out
+
+    def train_step(self, x, target, lr: float) -> float:
+        loss = C.c_double()
+        _check(self._lib.hzlb_mlp_train_step(self._h, self._dev(x, self.r + self.q),
+                                             self._dev(target, self.r), x.shape[0], lr,
+                                             C.byref(loss)))
+        return loss.value

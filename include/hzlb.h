@@ -247,6 +247,35 @@ HZLB_API int hzlb_step_noalloc(const hzlb_config *config, double dt, uint64_t ns
                                uint64_t first_step, void *state, const void *forcing, void *stream,
                                uint32_t *status);
 
+/* ---- learned reduced forecast (no counterpart in the reference, which has no learned model;
+ * its reduced forecast is the Galerkin ROM of reduced.cpp:137-209) ----------------------
+ * A multilayer perceptron advancing r POD coefficients over one forecast window:
+ *   y = a + s_out * (W3 gelu(W2 gelu(W1 (x / s_in) + b1) + b2) + b3),   x = (a, xi)
+ * x: r coefficients a followed by q noise-mode amplitudes xi; hidden width H (multiple of 16);
+ * gelu is the tanh form.  Weights and activations are BF16 with FP32 accumulation on the
+ * tcgen05 tensor cores; FP32 master parameters with Adam (beta1 0.9, beta2 0.999, eps 1e-8).
+ * Parameter vector (FP32): W1 [H][r+q], W2 [H][H], W3 [r][H], b1 [H], b2 [H], b3 [r];
+ * creation initialises W1, W2 ~ N(0, 1.96/fan_in), W3 ~ N(0, 0.01/fan_in), biases 0, scales 1
+ * from `seed`.  Batches are row-major [batch][features] device arrays of FP32. */
+typedef struct hzlb_mlp hzlb_mlp;
+HZLB_API int hzlb_mlp_create(int r, int q, int hidden, int max_batch, int device, uint64_t seed,
+                             hzlb_mlp **out);
+HZLB_API void hzlb_mlp_destroy(hzlb_mlp *h);
+HZLB_API size_t hzlb_mlp_param_count(const hzlb_mlp *h);
+/* host arrays of hzlb_mlp_param_count floats; grads (may be NULL) receives the gradient of the
+ * last training step */
+HZLB_API int hzlb_mlp_set_params(hzlb_mlp *h, const float *params);
+HZLB_API int hzlb_mlp_get_params(hzlb_mlp *h, float *params, float *grads);
+/* host arrays: s_in [r+q], s_out [r] */
+HZLB_API int hzlb_mlp_set_scales(hzlb_mlp *h, const float *s_in, const float *s_out);
+/* y [batch][r] = forward(x [batch][r+q]); device pointers.  stream NULL: the handle's stream,
+ * waited for; otherwise enqueued on `stream` without waiting. */
+HZLB_API int hzlb_mlp_forward(hzlb_mlp *h, const float *x, int batch, float *y, void *stream);
+/* One Adam step on the mean squared error of forward(x) against target [batch][r] (device
+ * pointers); *loss = that error before the update.  lr = 0 computes the gradient only. */
+HZLB_API int hzlb_mlp_train_step(hzlb_mlp *h, const float *x, const float *target, int batch,
+                                 float lr, double *loss);
+
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */
 /* Gaussian random vorticity spectrum, E(k) ~ k^4 exp(-(k/6)^2), unit enstrophy, retained modes

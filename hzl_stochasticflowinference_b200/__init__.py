@@ -132,6 +132,10 @@ def library() -> C.CDLL:
         "hzlb_gather_members": (C.c_int, [vp, _u32p]),
         "hzlb_inflate": (C.c_int, [vp, C.c_double]),
         "hzlb_enkf_analysis": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp]),
+        "hzlb_enkf_analysis_nis": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp,
+                                             C.c_uint64, C.c_uint64, C.c_double, _dp,
+                                             C.POINTER(C.c_int)]),
+        "hzlb_state_device": (C.c_int, [vp, C.POINTER(vp)]),
         "hzlb_grf_spectrum": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, _dp]),
         "hzlb_run_ensemble": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), C.c_double,
                                         C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_int,
@@ -363,6 +367,24 @@ class Ensemble:
         e = _f64(perturbations).reshape(self.members, len(x))
         _check(self._lib.hzlb_enkf_analysis(self._h, _pu(x), _pu(y), _p(v), _p(s), len(x),
                                             _p(e)))
+
+    def enkf_analysis_nis(self, x, y, values, sd, perturbations=None, seed: int = 0,
+                          cycle: int = 0, nis_limit: float = 0.0):
+        """Analysis with the normalised innovation statistic; returns (nis, applied).
+        perturbations None: drawn on the device from Philox (seed, member, cycle)."""
+        x, y, v, s = _u32(x), _u32(y), _f64(values), _f64(sd)
+        e = None if perturbations is None else _f64(perturbations).reshape(self.members, len(x))
+        nis, applied = C.c_double(), C.c_int()
+        _check(self._lib.hzlb_enkf_analysis_nis(self._h, _pu(x), _pu(y), _p(v), _p(s), len(x),
+                                                None if e is None else _p(e), seed, cycle,
+                                                nis_limit, C.byref(nis), C.byref(applied)))
+        return nis.value, bool(applied.value)
+
+    def state_device(self) -> int:
+        """Device address of the compact state (see hzlb_state_device)."""
+        ptr = C.c_void_p()
+        _check(self._lib.hzlb_state_device(self._h, C.byref(ptr)))
+        return ptr.value
 
 
 def pf_weights(log_weights):

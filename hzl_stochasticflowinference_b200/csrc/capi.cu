@@ -225,7 +225,34 @@ int hzlb_enkf_analysis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
             need(sd, "sd");
             need(perturbations, "perturbations");
         }
-        engine(h).enkf(x, y, values, sd, p, perturbations);
+        engine(h).enkf(hzlb::EnkfRequest{x, y, values, sd, p, perturbations, 0, 0, 0.0});
+    });
+}
+int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
+                           const double *values, const double *sd, size_t p,
+                           const double *perturbations, uint64_t perturbation_seed,
+                           uint64_t cycle, double nis_limit, double *nis, int *applied) {
+    return guarded([&] {
+        if (p) {
+            need(x, "x");
+            need(y, "y");
+            need(values, "values");
+            need(sd, "sd");
+        }
+        if (!std::isfinite(nis_limit))
+            hzlb::raise(HZLB_EINVAL, "innovation statistic limit must be finite");
+        const hzlb::EnkfResult r = engine(h).enkf(hzlb::EnkfRequest{
+            x, y, values, sd, p, perturbations, perturbation_seed, cycle, nis_limit});
+        if (nis)
+            *nis = r.nis;
+        if (applied)
+            *applied = r.applied;
+    });
+}
+int hzlb_state_device(hzlb_ensemble *h, void **state) {
+    return guarded([&] {
+        need(state, "state");
+        *state = engine(h).state_device();
     });
 }
 

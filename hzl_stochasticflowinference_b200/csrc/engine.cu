@@ -1,5 +1,6 @@
 // Ensemble engine: owns the device state of one handle and schedules the kernels.
 #include "engine.h"
+#include "dense64.cuh"
 #include "filters.cuh"
 #include "umma_gemm.cuh"
 
@@ -591,47 +592,91 @@ template <typename R> class EngineT final : public Engine {
             raise(HZLB_EINVAL, "EnKF inflation must be >= 1");
         if (inflation == 1)
             return;
-        const int blocks = static_cast<int>(std::min<size_t>((compact_ + 255) / 256, 4096));
-        inflate_kernel<R><<<blocks, 256, 0, stream_>>>(omega_.as<cx<R>>(),
-                                                       static_cast<long long>(compact_), M_, inflation);
+        const long long nr = 2 * static_cast<long long>(compact_);
+        R *mean = acc_.as<R>();   // free between steps
+        member_mean<R><<<static_cast<unsigned>((nr + 31) / 32), dim3(32, 8), 0, stream_>>>(
+            reinterpret_cast<const R *>(omega_.ptr), nr, M_, mean);
+        inflate_kernel<R><<<2048, 256, 0, stream_>>>(reinterpret_cast<R *>(omega_.ptr), mean, nr, M_,
+                                                     inflation);
         cuda_check(cudaGetLastError(), "launch inflation");
         w_valid_ = false;
     }
-    void enkf(const uint32_t *x, const uint32_t *y, const double *values, const double *sd,
-              size_t p, const double *eps) override {
+    void *state_device() override {
+        w_valid_ = false;
+        return omega_.ptr;
+    }
+    EnkfResult enkf(const EnkfRequest &q) override {
         if (M_ < 2)
             raise(HZLB_EINVAL, "EnKF requires at least two ensemble members");
+        const size_t p = q.p;
         if (p == 0)
-            return;
+            return EnkfResult{0.0, 0};
         for (size_t o = 0; o < p; ++o)
-            if (!std::isfinite(values[o]) || !std::isfinite(sd[o]) || sd[o] <= 0)
+            if (!std::isfinite(q.values[o]) || !std::isfinite(q.sd[o]) || q.sd[o] <= 0)
                 raise(HZLB_EINVAL, "observations must be finite and have positive uncertainty");
-        observe_device(x, y, p);
-        const size_t mp = static_cast<size_t>(M_) * p;
-        enkf_.ensure(sizeof(double) * (2 * p + 3 * mp + p * p + static_cast<size_t>(M_) * M_) + 64,
-                     "allocate EnKF workspace");
-        double *ybuf = enkf_.as<double>(), *sdbuf = ybuf + p, *eps_d = sdbuf + p, *ha = eps_d + mp,
-               *d = ha + mp, *P = d + mp, *W = P + p * p;
-        int *info = reinterpret_cast<int *>(W + static_cast<size_t>(M_) * M_);
-        cuda_check(cudaMemcpyAsync(ybuf, values, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
-                   "upload observations");
-        cuda_check(cudaMemcpyAsync(sdbuf, sd, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
-                   "upload observation errors");
-        cuda_check(cudaMemcpyAsync(eps_d, eps, sizeof(double) * mp, cudaMemcpyHostToDevice, stream_),
-                   "upload perturbations");
+        if (p > (1u << 20))
+            raise(HZLB_EINVAL, "too many observations for one analysis");
+        observe_device(q.x, q.y, p);
         const int pi = static_cast<int>(p);
-        enkf_innovations<<<(pi + 127) / 128, 128, 0, stream_>>>(obs_.as<double>(), ybuf, sdbuf, eps_d,
-                                                                M_, pi, ha, d);
-        enkf_gram<<<dim3((pi + 15) / 16, (pi + 15) / 16), dim3(16, 16), 0, stream_>>>(ha, sdbuf, M_,
-                                                                                      pi, P);
-        cholesky_kernel<<<1, 1024, 0, stream_>>>(P, pi, info);
-        cholesky_solve<<<(M_ + 127) / 128, 128, 0, stream_>>>(P, pi, d, M_);
-        enkf_weights<<<dim3((M_ + 15) / 16, (M_ + 15) / 16), dim3(16, 16), 0, stream_>>>(ha, d, M_, pi, W);
-        cuda_check(cudaGetLastError(), "launch EnKF analysis");
+        const size_t mp = static_cast<size_t>(M_) * p, m1p = mp + p;
+        const size_t nblk = (p + d64::NB - 1) / d64::NB;
+        const size_t eps_n = q.perturbations ? mp : 0;
+        const size_t doubles = 3 * p + eps_n + mp + 2 * m1p + p * p + nblk * d64::NB * d64::NB +
+                               static_cast<size_t>(M_) * M_ + 1;
+        enkf_.ensure(sizeof(double) * doubles + 64, "allocate EnKF workspace");
+        double *ybuf = enkf_.as<double>(), *sdbuf = ybuf + p, *hmean = sdbuf + p,
+               *eps_d = hmean + p, *ha = eps_d + eps_n, *d = ha + mp, *yw = d + m1p,
+               *P = yw + m1p, *inv = P + p * p, *W = inv + nblk * d64::NB * d64::NB,
+               *nis_d = W + static_cast<size_t>(M_) * M_;
+        int *info = reinterpret_cast<int *>(nis_d + 1);
+        cuda_check(cudaMemcpyAsync(ybuf, q.values, sizeof(double) * p, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "upload observations");
+        cuda_check(cudaMemcpyAsync(sdbuf, q.sd, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
+                   "upload observation errors");
+        if (q.perturbations)
+            cuda_check(cudaMemcpyAsync(eps_d, q.perturbations, sizeof(double) * mp,
+                                       cudaMemcpyHostToDevice, stream_),
+                       "upload perturbations");
+        cuda_check(cudaMemsetAsync(info, 0, sizeof(int), stream_), "clear Cholesky status");
+        member_mean<double><<<(pi + 31) / 32, dim3(32, 8), 0, stream_>>>(obs_.as<double>(), pi, M_,
+                                                                       hmean);
+        enkf_innovations<<<1024, 256, 0, stream_>>>(
+            obs_.as<double>(), hmean, ybuf, sdbuf, q.perturbations ? eps_d : nullptr,
+            q.perturbation_seed, static_cast<uint32_t>(cfg_.member_base), q.cycle, M_, pi, ha, d);
+        cuda_check(cudaGetLastError(), "launch EnKF innovations");
+        // S = HA^T HA / (M-1) + R (lower triangle), FP64
+        cuda_check(d64::gemm(d64::GemmArgs{pi, pi, M_, 1.0 / (M_ - 1), 0.0, ha, 1, pi, ha, pi, 1,
+                                           P, pi},
+                             stream_, true),
+                   "launch innovation covariance");
+        add_obs_variance<<<(pi + 127) / 128, 128, 0, stream_>>>(P, sdbuf, pi);
+        cuda_check(d64::cholesky(P, pi, inv, info, stream_), "launch innovation Cholesky");
+        // Z = S^{-1} D for the M perturbed innovations and the mean innovation
+        cuda_check(d64::cholesky_solve_rows(P, pi, inv, d, yw, M_ + 1, stream_),
+                   "launch innovation solve");
+        innovation_statistic<<<1, 256, 0, stream_>>>(ybuf, hmean, d + mp, pi, nis_d);
+        cuda_check(cudaGetLastError(), "launch innovation statistic");
+        double nis = 0;
+        int host_info = 0;
+        cuda_check(cudaMemcpyAsync(&nis, nis_d, sizeof(double), cudaMemcpyDeviceToHost, stream_),
+                   "read innovation statistic");
+        cuda_check(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, stream_),
+                   "read Cholesky status");
+        cuda_check(cudaStreamSynchronize(stream_), "EnKF innovation solve");
+        if (host_info != 0)
+            raise(HZLB_ERUNTIME, "EnKF innovation covariance is not positive definite");
+        if (q.nis_limit > 0 && !(nis <= q.nis_limit))
+            return EnkfResult{nis, 0};
+        // W[a][m] = sum_o HA[a][o] Z[m][o] / (M-1)
+        cuda_check(d64::gemm(d64::GemmArgs{M_, M_, pi, 1.0 / (M_ - 1), 0.0, ha, pi, 1, d, 1, pi,
+                                           W, M_},
+                             stream_),
+                   "launch ensemble weights");
         cx<R> *mean = acc_.as<cx<R>>();   // free between steps
-        const int mb = static_cast<int>(std::min<size_t>((compact_ + 255) / 256, 4096));
-        ensemble_mean<R><<<mb, 256, 0, stream_>>>(omega_.as<cx<R>>(), static_cast<long long>(compact_),
-                                                  M_, mean);
+        member_mean<R><<<static_cast<unsigned>((2 * compact_ + 31) / 32), dim3(32, 8), 0, stream_>>>(
+            reinterpret_cast<const R *>(omega_.ptr), static_cast<long long>(2 * compact_), M_,
+            reinterpret_cast<R *>(mean));
         if constexpr (sizeof(R) == 4) {
             // X_a = X + A W on the tensor cores: A = X - mean and W split for 3xTF32
             // (hi*hi + hi*lo + lo*hi), accumulated into X in place
@@ -644,8 +689,10 @@ template <typename R> class EngineT final : public Engine {
                        "stage ensemble mean");
             split_.ensure(sizeof(float) * 2 * static_cast<size_t>(M_) * M_, "allocate weight split");
             float *whi = split_.as<float>(), *wlo = whi + static_cast<size_t>(M_) * M_;
-            anomaly_split_tf32<<<2048, 256, 0, stream_>>>(x, mf, n, M_, ahi, alo);
-            split_tf32<<<256, 256, 0, stream_>>>(W, static_cast<long long>(M_) * M_, whi, wlo);
+            const dim3 tb(32, 8);
+            anomaly_split_tf32_t<<<dim3(static_cast<unsigned>((n + 31) / 32), (M_ + 31) / 32), tb, 0,
+                                   stream_>>>(x, mf, n, M_, ahi, alo);
+            split_tf32_t<<<dim3((M_ + 31) / 32, (M_ + 31) / 32), tb, 0, stream_>>>(W, M_, whi, wlo);
             cuda_check(cudaGetLastError(), "launch 3xTF32 split");
             const float *wa[3] = {whi, whi, wlo};
             const float *aa[3] = {ahi, alo, ahi};
@@ -654,12 +701,12 @@ template <typename R> class EngineT final : public Engine {
                 g.M = M_;
                 g.N = static_cast<int>(n);
                 g.K = M_;
-                g.A = wa[i];           // opA[m][a] = W[a][m]
+                g.A = wa[i];           // opA[m][a] = W[a][m], stored transposed
                 g.lda = M_;
-                g.a_kcontig = 0;
-                g.B = aa[i];           // opB[e][a] = A[a][e]
-                g.ldb = n;
-                g.b_kcontig = 0;
+                g.a_kcontig = 1;
+                g.B = aa[i];           // opB[e][a] = A[a][e], stored transposed
+                g.ldb = M_;
+                g.b_kcontig = 1;
                 g.C = x;
                 g.ldc = n;
                 g.alpha = 1.0f;
@@ -679,13 +726,9 @@ template <typename R> class EngineT final : public Engine {
                                        cudaMemcpyDeviceToDevice, stream_),
                        "commit EnKF update");
         }
-        int host_info = 0;
-        cuda_check(cudaMemcpyAsync(&host_info, info, sizeof(int), cudaMemcpyDeviceToHost, stream_),
-                   "read Cholesky status");
         cuda_check(cudaStreamSynchronize(stream_), "EnKF analysis");
         w_valid_ = false;
-        if (host_info != 0)
-            raise(HZLB_ERUNTIME, "EnKF innovation covariance is not positive definite");
+        return EnkfResult{nis, 1};
     }
 
   private:

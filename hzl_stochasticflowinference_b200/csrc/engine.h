@@ -66,6 +66,21 @@ struct PinnedBuffer {
     template <typename T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// One perturbed-observation EnKF analysis of p point observations.
+struct EnkfRequest {
+    const uint32_t *x, *y;          // grid indices of the observations
+    const double *values, *sd;      // observed values and their standard deviations
+    size_t p;
+    const double *perturbations;    // host members x p standard normals, or null: device Philox
+    uint64_t perturbation_seed;     // Philox key when perturbations is null
+    uint64_t cycle;                 // Philox counter when perturbations is null
+    double nis_limit;               // > 0: leave the state unchanged when the statistic exceeds it
+};
+struct EnkfResult {
+    double nis;                     // dbar^T S^{-1} dbar / p of the forecast ensemble
+    int applied;                    // 1 if the state was updated
+};
+
 class Engine {
   public:
     virtual ~Engine() = default;
@@ -83,8 +98,10 @@ class Engine {
     virtual void resample(const double *w, size_t count, double u, uint32_t *anc) = 0;
     virtual void gather(const uint32_t *ancestors) = 0;
     virtual void inflate(double inflation) = 0;
-    virtual void enkf(const uint32_t *x, const uint32_t *y, const double *values, const double *sd,
-                      size_t p, const double *perturbations) = 0;
+    virtual EnkfResult enkf(const EnkfRequest &request) = 0;
+    // device address of the compact state (members x compact_size complex entries); the
+    // caller may modify it until its next call on this ensemble
+    virtual void *state_device() = 0;
     virtual size_t compact_size() const = 0;
     virtual int members() const = 0;
     virtual void *stream() const = 0;

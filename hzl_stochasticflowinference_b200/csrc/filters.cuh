@@ -1,6 +1,7 @@
 // Filter analysis kernels: systematic resampling, member gather, ensemble inflation and the
-// perturbed-observation EnKF (innovation Gram, FP64 Cholesky and triangular solves, ensemble
-// weight matrix, and the anomaly update X_a = X + A W).
+// element-wise parts of the perturbed-observation EnKF (innovations, perturbations, the
+// innovation statistic and the anomaly update X_a = X + A W); its FP64 Gram, Cholesky and
+// solves are in dense64.cuh.
 #pragma once
 #include "common.cuh"
 
@@ -47,137 +48,94 @@ __global__ void gather_blocks(const cx<R> *src, cx<R> *dst, const unsigned *anc,
         d[e] = s[e];
 }
 
-// x_m <- mean + inflation (x_m - mean) for every entry (filter.cpp:238-252).
+// Member means of a member-major array (members x n values of T): out[e] = sum_m x[m][e] / M.
+// Blocks of (32, 8): 32 columns, eight warps over interleaved member slices, FP64 sums
+// combined in shared memory.  Grid x = ceil(n / 32).
+template <typename T>
+__global__ void member_mean(const T *x, long long n, int members, T *out) {
+    __shared__ double part[8][33];
+    const long long e = static_cast<long long>(blockIdx.x) * 32 + threadIdx.x;
+    double s = 0;
+    if (e < n)
+        for (int m = threadIdx.y; m < members; m += 8)
+            s += static_cast<double>(x[static_cast<long long>(m) * n + e]);
+    part[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && e < n) {
+        double t = 0;
+        for (int w = 0; w < 8; ++w)
+            t += part[w][threadIdx.x];
+        out[e] = static_cast<T>(t / members);
+    }
+}
+
+// x_m <- mean + inflation (x_m - mean) for every entry (filter.cpp:238-252), with the member
+// mean from member_mean; x is viewed as members x n reals.
 template <typename R>
-__global__ void inflate_kernel(cx<R> *x, long long block, int members, double inflation) {
-    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
-         e += static_cast<long long>(gridDim.x) * blockDim.x) {
-        double mr = 0, mi = 0;
-        for (int m = 0; m < members; ++m) {
-            mr += static_cast<double>(x[static_cast<size_t>(m) * block + e].x) / members;
-            mi += static_cast<double>(x[static_cast<size_t>(m) * block + e].y) / members;
-        }
-        for (int m = 0; m < members; ++m) {
-            cx<R> &v = x[static_cast<size_t>(m) * block + e];
-            v.x = static_cast<R>(mr + inflation * (static_cast<double>(v.x) - mr));
-            v.y = static_cast<R>(mi + inflation * (static_cast<double>(v.y) - mi));
-        }
+__global__ void inflate_kernel(R *x, const R *mean, long long n, int members, double inflation) {
+    const long long total = n * members;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const double m = static_cast<double>(mean[i % n]);
+        x[i] = static_cast<R>(m + inflation * (static_cast<double>(x[i]) - m));
     }
 }
 
 // ---- EnKF ---------------------------------------------------------------------------
-// HA[m][o] = HX[m][o] - mean_m HX[.][o];  D[m][o] = y_o + sd_o eps[m][o] - HX[m][o].
-__global__ void enkf_innovations(const double *hx, const double *y, const double *sd,
-                                 const double *eps, int members, int p, double *ha, double *d) {
-    const int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= p)
-        return;
-    double mean = 0;
-    for (int m = 0; m < members; ++m)
-        mean += hx[static_cast<size_t>(m) * p + o] / members;
-    for (int m = 0; m < members; ++m) {
-        const size_t i = static_cast<size_t>(m) * p + o;
-        ha[i] = hx[i] - mean;
-        d[i] = y[o] + sd[o] * eps[i] - hx[i];
+// Observation perturbation of member m, observation o, analysis `cycle`: a standard normal
+// from the Philox stream keyed by (seed, member); the counter's step word carries the cycle
+// with a domain tag in its high half so these draws never coincide with forcing noise.
+__device__ __forceinline__ double enkf_perturbation(uint64_t seed, uint32_t member, uint64_t cycle,
+                                                    int o) {
+    double xi1, xi2;
+    philox_normal_pair(seed, member, cycle ^ (0x454E4B46ull << 32), static_cast<uint32_t>(o >> 1),
+                       xi1, xi2);
+    return (o & 1) ? xi2 : xi1;
+}
+// HA[m][o] = HX[m][o] - mean[o];  D[m][o] = y_o + sd_o eps[m][o] - HX[m][o] for m < M and the
+// mean innovation D[M][o] = y_o - mean[o].  eps: host-supplied M x p normals, or (eps == null)
+// enkf_perturbation(seed, member_base + m, cycle, o).
+__global__ void enkf_innovations(const double *hx, const double *mean, const double *y,
+                                 const double *sd, const double *eps, uint64_t seed,
+                                 uint32_t member_base, uint64_t cycle, int members, int p,
+                                 double *ha, double *d) {
+    const long long total = static_cast<long long>(members + 1) * p;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int m = static_cast<int>(i / p), o = static_cast<int>(i % p);
+        if (m == members) {
+            d[i] = y[o] - mean[o];
+            continue;
+        }
+        const double e = eps ? eps[i] : enkf_perturbation(seed, member_base + m, cycle, o);
+        ha[i] = hx[i] - mean[o];
+        d[i] = y[o] + sd[o] * e - hx[i];
     }
 }
-// P[a][b] = sum_m HA[m][a] HA[m][b] / (M-1) + (a == b) sd_a^2   (FP64, p x p)
-__global__ void enkf_gram(const double *ha, const double *sd, int members, int p, double *P) {
-    __shared__ double ta[16][17], tb[16][17];
-    const int a = blockIdx.y * 16 + threadIdx.y, b = blockIdx.x * 16 + threadIdx.x;
+// P[a][a] += sd_a^2 (observation error on the diagonal of the innovation covariance)
+__global__ void add_obs_variance(double *P, const double *sd, int p) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < p)
+        P[static_cast<size_t>(a) * p + a] += sd[a] * sd[a];
+}
+// Normalised innovation statistic dbar^T S^{-1} dbar / p with dbar = y - mean, given
+// z = S^{-1} dbar (one block).
+__global__ void innovation_statistic(const double *y, const double *mean, const double *z, int p,
+                                     double *out) {
+    __shared__ double part[32];
     double s = 0;
-    for (int m0 = 0; m0 < members; m0 += 16) {
-        const int ma = m0 + threadIdx.x, mb = m0 + threadIdx.y;
-        const int ra = blockIdx.y * 16 + threadIdx.y, rb = blockIdx.x * 16 + threadIdx.x;
-        ta[threadIdx.y][threadIdx.x] = (ma < members && ra < p) ? ha[static_cast<size_t>(ma) * p + ra] : 0;
-        tb[threadIdx.y][threadIdx.x] = (mb < members && rb < p) ? ha[static_cast<size_t>(mb) * p + rb] : 0;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            s += ta[threadIdx.y][k] * tb[k][threadIdx.x];
-        __syncthreads();
-    }
-    if (a < p && b < p)
-        P[static_cast<size_t>(a) * p + b] = s / (members - 1) + (a == b ? sd[a] * sd[a] : 0.0);
-}
-// In-place Cholesky P = L L^T (lower triangle), one block, column by column (right-looking).
-// info[0] is set to the first nonpositive pivot + 1 (0 on success).
-__global__ void cholesky_kernel(double *P, int p, int *info) {
-    __shared__ double pivot;
-    if (threadIdx.x == 0)
-        info[0] = 0;
-    for (int k = 0; k < p; ++k) {
-        if (threadIdx.x == 0) {
-            const double d = P[static_cast<size_t>(k) * p + k];
-            if (!(d > 0) && info[0] == 0)
-                info[0] = k + 1;
-            pivot = d > 0 ? sqrt(d) : 1.0;
-            P[static_cast<size_t>(k) * p + k] = pivot;
-        }
-        __syncthreads();
-        for (int i = k + 1 + threadIdx.x; i < p; i += blockDim.x)
-            P[static_cast<size_t>(i) * p + k] /= pivot;
-        __syncthreads();
-        // trailing update of the lower triangle: P[i][j] -= L[i][k] L[j][k], k < j <= i;
-        // one warp per row i, lanes over j
-        const int warp = threadIdx.x / 32, lane = threadIdx.x % 32, warps = blockDim.x / 32;
-        for (int i = k + 1 + warp; i < p; i += warps) {
-            const double lik = P[static_cast<size_t>(i) * p + k];
-            for (int j = k + 1 + lane; j <= i; j += 32)
-                P[static_cast<size_t>(i) * p + j] -= lik * P[static_cast<size_t>(j) * p + k];
-        }
-        __syncthreads();
-    }
-}
-// Solve L L^T z = d for every member's innovation vector (row m of D, in place).
-__global__ void cholesky_solve(const double *L, int p, double *D, int members) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= members)
-        return;
-    double *z = D + static_cast<size_t>(m) * p;
-    for (int i = 0; i < p; ++i) {
-        double s = z[i];
-        for (int k = 0; k < i; ++k)
-            s -= L[static_cast<size_t>(i) * p + k] * z[k];
-        z[i] = s / L[static_cast<size_t>(i) * p + i];
-    }
-    for (int i = p - 1; i >= 0; --i) {
-        double s = z[i];
-        for (int k = i + 1; k < p; ++k)
-            s -= L[static_cast<size_t>(k) * p + i] * z[k];
-        z[i] = s / L[static_cast<size_t>(i) * p + i];
-    }
-}
-// W[a][m] = sum_o HA[a][o] Z[m][o] / (M-1)   (members x members, FP64)
-__global__ void enkf_weights(const double *ha, const double *z, int members, int p, double *W) {
-    __shared__ double ta[16][17], tb[16][17];
-    const int a = blockIdx.y * 16 + threadIdx.y, m = blockIdx.x * 16 + threadIdx.x;
-    double s = 0;
-    for (int o0 = 0; o0 < p; o0 += 16) {
-        const int oa = o0 + threadIdx.x, ob = o0 + threadIdx.y;
-        ta[threadIdx.y][threadIdx.x] = (a < members && oa < p) ? ha[static_cast<size_t>(a) * p + oa] : 0;
-        const int mb = blockIdx.x * 16 + threadIdx.x;
-        tb[threadIdx.y][threadIdx.x] = (mb < members && ob < p) ? z[static_cast<size_t>(mb) * p + ob] : 0;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 16; ++k)
-            s += ta[threadIdx.y][k] * tb[k][threadIdx.x];
-        __syncthreads();
-    }
-    if (a < members && m < members)
-        W[static_cast<size_t>(a) * members + m] = s / (members - 1);
-}
-// Column means of the ensemble state: mean[e] = sum_m X[m][e] / M.
-template <typename R>
-__global__ void ensemble_mean(const cx<R> *x, long long block, int members, cx<R> *mean) {
-    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
-         e += static_cast<long long>(gridDim.x) * blockDim.x) {
-        double mr = 0, mi = 0;
-        for (int m = 0; m < members; ++m) {
-            mr += static_cast<double>(x[static_cast<size_t>(m) * block + e].x) / members;
-            mi += static_cast<double>(x[static_cast<size_t>(m) * block + e].y) / members;
-        }
-        mean[e] = mk<R>(static_cast<R>(mr), static_cast<R>(mi));
+    for (int o = threadIdx.x; o < p; o += blockDim.x)
+        s += (y[o] - mean[o]) * z[o];
+    for (int k = 16; k > 0; k >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, k);
+    if ((threadIdx.x & 31) == 0)
+        part[threadIdx.x / 32] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x / 32); ++w)
+            t += part[w];
+        *out = t / p;
     }
 }
 // X_a[m][e] = X[m][e] + sum_a (X[a][e] - mean[e]) W[a][m]: a (members x 2*block) by
@@ -238,25 +196,53 @@ __device__ __forceinline__ float to_tf32(float x) {
 }
 // Split for 3xTF32 products: A = hi + lo with hi exactly representable in TF32; the products
 // hi*hi + hi*lo + lo*hi recover FP32-level accuracy on the tensor cores.
-// Anomalies a = x - mean of the member-major state (members x n reals).
-__global__ void anomaly_split_tf32(const float *x, const float *mean, long long n, int members,
-                                   float *hi, float *lo) {
-    const long long total = n * members;
-    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const float a = x[i] - mean[i % n];
-        const float h = to_tf32(a);
-        hi[i] = h;
-        lo[i] = a - h;
+// The operands of the update product X += A W are written transposed, member index
+// contiguous, so it is the K dimension of both tensor-core operands; 32 x 32 tiles pass through
+// shared memory so reads and writes stay coalesced.  Launch with blockDim (32, 8).
+// Anomalies a[m][e] = x[m][e] - mean[e] of the member-major state (members x n reals) ->
+// hiT[e][m], loT[e][m].
+__global__ void anomaly_split_tf32_t(const float *x, const float *mean, long long n, int members,
+                                     float *hiT, float *loT) {
+    __shared__ float t[32][33];
+    const long long e0 = static_cast<long long>(blockIdx.x) * 32;
+    const int m0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int m = m0 + r;
+        const long long e = e0 + threadIdx.x;
+        t[r][threadIdx.x] = (m < members && e < n) ? x[static_cast<long long>(m) * n + e] - mean[e]
+                                                   : 0.0f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const long long e = e0 + r;
+        const int m = m0 + threadIdx.x;
+        if (e < n && m < members) {
+            const float a = t[threadIdx.x][r];
+            const float h = to_tf32(a);
+            hiT[e * members + m] = h;
+            loT[e * members + m] = a - h;
+        }
     }
 }
-__global__ void split_tf32(const double *w, long long count, float *hi, float *lo) {
-    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const float v = static_cast<float>(w[i]);
-        const float h = to_tf32(v);
-        hi[i] = h;
-        lo[i] = v - h;
+// Ensemble weights W[a][m] (members x members, FP64) -> hiT[m][a], loT[m][a].
+__global__ void split_tf32_t(const double *w, int members, float *hiT, float *loT) {
+    __shared__ float t[32][33];
+    const int a0 = blockIdx.x * 32, m0 = blockIdx.y * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int a = a0 + r, m = m0 + threadIdx.x;
+        t[r][threadIdx.x] = (a < members && m < members)
+                                ? static_cast<float>(w[static_cast<long long>(a) * members + m])
+                                : 0.0f;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int m = m0 + r, a = a0 + threadIdx.x;
+        if (a < members && m < members) {
+            const float v = t[threadIdx.x][r];
+            const float h = to_tf32(v);
+            hiT[static_cast<long long>(m) * members + a] = h;
+            loT[static_cast<long long>(m) * members + a] = v - h;
+        }
     }
 }
 // out[e] = sum over members (in member order) of w[m] x[m][e], or of x[m][e] / divisor when

@@ -4,13 +4,15 @@
 //
 // opA / opB are BF16 (kind::f16) or FP32 read as TF32 (kind::tf32), each given either
 // K-contiguous ([rows][K]) or rows-contiguous ([K][rows]).  One CTA (4 warps) computes a
-// 128 x BN tile: all threads stage 128 x 64-byte (A) and BN x 64-byte (B) slabs of K into shared
-// memory in the canonical K-major core-matrix layout (8 rows x 16 bytes per core matrix, no
-// swizzle); one elected thread issues the MMAs (two per slab, 32 bytes of K each) and commits
-// them to an mbarrier; the slabs are double-buffered so staging overlaps the tensor cores.  The
+// 128 x BN tile.  K advances in slabs of 128 bytes per row held in a STAGES-deep ring of shared
+// memory buffers in the canonical K-major core-matrix layout (8 rows x 16 bytes per core matrix,
+// no swizzle).  K-contiguous, 16-byte aligned operands are copied with cp.async (16-byte chunks,
+// zero-filled past the matrix edges), STAGES - 1 slabs ahead of the tensor cores; other layouts
+// are staged by plain loads.  One elected thread issues the MMAs (four per slab, 32 bytes of K
+// each) and commits them to the slab buffer's mbarrier, which gates the buffer's refill.  The
 // accumulator lives in TMEM (BN 32-bit columns) and is read back with tcgen05.ld (warp w owns
 // lanes 32w..32w+31 = rows) for the epilogue.  Every mbarrier wait is bounded; on expiry the
-// CTA records STATUS_TIMEOUT, frees its TMEM and returns.
+// CTA records STATUS_TIMEOUT, drains its copies, frees its TMEM and returns.
 #pragma once
 #include "async_copy.cuh"
 #include "common.cuh"
@@ -113,7 +115,18 @@ struct GemmArgs {
 };
 
 constexpr int BM = 128;
-constexpr int SLAB = 64;   // bytes of K per staged slab (2 MMAs of 32 bytes)
+constexpr int SLAB = 128;   // bytes of K per staged slab (4 MMAs of 32 bytes)
+constexpr int CPR = SLAB / 16;   // 16-byte chunks per row of a slab
+constexpr int STAGES = 3;
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, int bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 template <typename TIn> __device__ __forceinline__ float to_f(TIn v);
 template <> __device__ __forceinline__ float to_f<float>(float v) { return v; }
@@ -121,34 +134,42 @@ template <> __device__ __forceinline__ float to_f<__nv_bfloat16>(__nv_bfloat16 v
     return __bfloat162float(v);
 }
 
-// Stages rows [row0, row0 + ROWS) x K-bytes [kb0, kb0 + SLAB) of an operand into the
-// core-matrix layout: chunk c (16 bytes) of row r at ((r/8) * 4 + c) * 128 + (r%8) * 16.
+// Stages rows [row0, row0 + ROWS) x K-elements [k0, k0 + SLAB / sizeof(TIn)) of an operand
+// into the core-matrix layout: chunk c (16 bytes) of row r at ((r/8) * CPR + c) * 128 + (r%8) * 16.
+// Lane l of each warp takes row 8g + l%8 and chunk 4h + l/8, so a warp writes 512 contiguous
+// bytes of shared memory and reads 64 contiguous bytes of each of 8 rows.  `fast`: K-contiguous
+// with 16-byte aligned rows, copied by cp.async (the caller commits and waits); otherwise plain
+// loads and stores.
 template <typename TIn, int ROWS>
 __device__ __forceinline__ void stage_slab(unsigned char *dst, const TIn *src, long long ld,
-                                           bool kcontig, int rows, int K, int row0, int k0) {
+                                           bool kcontig, bool fast, int rows, int K, int row0,
+                                           int k0) {
     constexpr int EPC = 16 / sizeof(TIn);   // elements per 16-byte chunk
-    for (int q = threadIdx.x; q < ROWS * 4; q += blockDim.x) {
-        const int r = q % ROWS, c = q / ROWS;
+    for (int q = threadIdx.x; q < ROWS * CPR; q += blockDim.x) {
+        const int l = q % 32, wq = q / 32;
+        const int r = (wq / (CPR / 4)) * 8 + l % 8, c = (wq % (CPR / 4)) * 4 + l / 8;
         const int gr = row0 + r, gk = k0 + c * EPC;
-        alignas(16) TIn vals[EPC];
-        if (kcontig && gr < rows && gk + EPC <= K &&
-            (reinterpret_cast<uintptr_t>(src + gr * ld + gk) & 15) == 0) {
-            const uint4 raw = *reinterpret_cast<const uint4 *>(src + gr * ld + gk);
-            *reinterpret_cast<uint4 *>(vals) = raw;
-        } else {
-#pragma unroll
-            for (int e = 0; e < EPC; ++e) {
-                const int kk = gk + e;
-                TIn v;
-                if (gr < rows && kk < K)
-                    v = kcontig ? src[gr * ld + kk] : src[static_cast<long long>(kk) * ld + gr];
-                else
-                    v = TIn(0.0f);
-                vals[e] = v;
-            }
+        unsigned char *d = dst + ((r / 8) * CPR + c) * 128 + (r % 8) * 16;
+        if (fast) {
+            const int left = gr < rows ? (K - gk) * static_cast<int>(sizeof(TIn)) : 0;
+            const int bytes = left < 0 ? 0 : (left > 16 ? 16 : left);
+            const TIn *from = bytes > 0 ? src + static_cast<long long>(gr) * ld + gk : src;
+            cp_async16(smem_u32(d), from, bytes);
+            continue;
         }
-        *reinterpret_cast<uint4 *>(dst + ((r / 8) * 4 + c) * 128 + (r % 8) * 16) =
-            *reinterpret_cast<const uint4 *>(vals);
+        alignas(16) TIn vals[EPC];
+#pragma unroll
+        for (int e = 0; e < EPC; ++e) {
+            const int kk = gk + e;
+            TIn v;
+            if (gr < rows && kk < K)
+                v = kcontig ? src[static_cast<long long>(gr) * ld + kk]
+                            : src[static_cast<long long>(kk) * ld + gr];
+            else
+                v = TIn(0.0f);
+            vals[e] = v;
+        }
+        *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(vals);
     }
 }
 
@@ -165,24 +186,28 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
     constexpr int EPS = SLAB / sizeof(TIn);   // K elements per slab
     constexpr uint32_t A_BYTES = BM * SLAB, B_BYTES = BN * SLAB;
     constexpr uint32_t IDESC = instr_desc(TF32 ? 2u : 1u, BM, BN);
+    constexpr uint32_t SBO = CPR * 128;       // byte distance between 8-row core-matrix groups
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *sa = smem;                          // [2][A_BYTES]
-    unsigned char *sb = smem + 2 * A_BYTES;            // [2][B_BYTES]
-    __shared__ __align__(8) uint64_t bars[3];          // slab 0, slab 1 consumed; final
+    unsigned char *sa = smem;                          // [STAGES][A_BYTES]
+    unsigned char *sb = smem + STAGES * A_BYTES;       // [STAGES][B_BYTES]
+    __shared__ __align__(8) uint64_t bars[STAGES + 1];   // per-buffer MMA completion; final
     __shared__ uint32_t tmem_base;
     __shared__ int ok_sh;
 
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const TIn *A = static_cast<const TIn *>(g.A);
     const TIn *B = static_cast<const TIn *>(g.B);
+    const bool a_fast = g.a_kcontig && (reinterpret_cast<uintptr_t>(A) & 15) == 0 &&
+                        (g.lda * static_cast<long long>(sizeof(TIn))) % 16 == 0;
+    const bool b_fast = g.b_kcontig && (reinterpret_cast<uintptr_t>(B) & 15) == 0 &&
+                        (g.ldb * static_cast<long long>(sizeof(TIn))) % 16 == 0;
     const int warp = threadIdx.x / 32;
-    constexpr uint32_t NCOLS = BN < 32 ? 32 : (BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256)));
+    constexpr uint32_t NCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
     if (warp == 0)
         tmem_alloc(&tmem_base, NCOLS);
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        mbar_init(&bars[2], 1);
+        for (int i = 0; i <= STAGES; ++i)
+            mbar_init(&bars[i], 1);
         mbar_init_fence();
         ok_sh = 1;
     }
@@ -192,40 +217,53 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
     const uint32_t tmem = tmem_base;
 
     const int slabs = (g.K + EPS - 1) / EPS;
-    uint32_t uses[2] = {0, 0};
+    auto load = [&](int s) {
+        const int b = s % STAGES;
+        stage_slab<TIn, BM>(sa + b * A_BYTES, A, g.lda, g.a_kcontig, a_fast, g.M, g.K, m0, s * EPS);
+        stage_slab<TIn, BN>(sb + b * B_BYTES, B, g.ldb, g.b_kcontig, b_fast, g.N, g.K, n0, s * EPS);
+    };
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < slabs)
+            load(s);
+        cp_async_commit();
+    }
     bool ok = true;
     for (int s = 0; s < slabs; ++s) {
-        const int b = s & 1;
-        // the MMAs that read this buffer two slabs ago must be done before it is refilled
-        if (s >= 2) {
+        const int b = s % STAGES;
+        // slab s has landed: its copy group (and every earlier one) is complete
+        cp_async_wait<STAGES - 2>();
+        fence_proxy_async_shared();   // generic/async-copy writes -> visible to the tensor cores
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sa + b * A_BYTES), b0 = smem_u32(sb + b * B_BYTES);
+#pragma unroll
+            for (int h = 0; h < SLAB / 32; ++h)   // 32-byte K steps: core matrices 2h, 2h+1
+                mma<TF32>(tmem, smem_desc(a0 + h * 256, 128, SBO), smem_desc(b0 + h * 256, 128, SBO),
+                          IDESC, (s > 0 || h > 0) ? 1u : 0u);
+            mma_commit(&bars[b]);
+        }
+        // refill the buffer of slab s - 1 with slab s + STAGES - 1 once its MMAs are done
+        const int sn = s + STAGES - 1;
+        if (sn < slabs && s >= 1) {
             if (threadIdx.x == 0)
-                ok_sh = mbar_wait_bounded(&bars[b], (uses[b] - 1) & 1) ? ok_sh : 0;
+                ok_sh = mbar_wait_bounded(&bars[(s - 1) % STAGES], ((s - 1) / STAGES) & 1) ? ok_sh : 0;
             __syncthreads();
             if (!ok_sh) {
                 ok = false;
                 break;
             }
         }
-        stage_slab<TIn, BM>(sa + b * A_BYTES, A, g.lda, g.a_kcontig, g.M, g.K, m0, s * EPS);
-        stage_slab<TIn, BN>(sb + b * B_BYTES, B, g.ldb, g.b_kcontig, g.N, g.K, n0, s * EPS);
-        fence_proxy_async_shared();   // generic-proxy stores -> visible to the tensor cores
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            tc_fence_after();
-            const uint32_t a0 = smem_u32(sa + b * A_BYTES), b0 = smem_u32(sb + b * B_BYTES);
-#pragma unroll
-            for (int h = 0; h < 2; ++h)   // two 32-byte K steps: core matrices 2h, 2h+1
-                mma<TF32>(tmem, smem_desc(a0 + h * 256, 128, 512), smem_desc(b0 + h * 256, 128, 512),
-                          IDESC, (s > 0 || h > 0) ? 1u : 0u);
-            mma_commit(&bars[b]);
-        }
-        ++uses[b];
+        if (sn < slabs)
+            load(sn);
+        cp_async_commit();
     }
+    cp_async_wait<0>();
     // all issued MMAs complete (or, after a failed wait, a bounded wait for them) before the
     // accumulator is read or freed
     if (threadIdx.x == 0) {
-        mma_commit(&bars[2]);
-        const bool done = mbar_wait_bounded(&bars[2], 0);
+        mma_commit(&bars[STAGES]);
+        const bool done = mbar_wait_bounded(&bars[STAGES], 0);
         ok_sh = (ok && done) ? 1 : 0;
     }
     __syncthreads();
@@ -271,7 +309,7 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
 }
 
 template <typename TIn, int BN> constexpr size_t gemm_smem() {
-    return 2 * (BM * SLAB + BN * SLAB);
+    return STAGES * (BM * SLAB + BN * SLAB);
 }
 
 } // namespace tc

@@ -156,6 +156,24 @@ HZLB_API int hzlb_inflate(hzlb_ensemble *h, double inflation);
 HZLB_API int hzlb_enkf_analysis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
                        const double *values, const double *sd, size_t p,
                        const double *perturbations);
+/* No counterpart in the reference (it defines no innovation-consistency test).  The same
+ * analysis, returning the normalised innovation statistic of the forecast ensemble,
+ *   nis = dbar^T (HA HA^T/(M-1) + R)^{-1} dbar / p,   dbar = y - mean(HX),
+ * which is 1 in expectation for a consistent forecast.  With nis_limit > 0 and nis above it
+ * the state is left unchanged and *applied = 0 (the caller falls back to another forecast);
+ * otherwise the update is applied and *applied = 1.  perturbations: as above, or NULL to draw
+ * them on the device from the Philox stream keyed by (perturbation_seed, member_base + m)
+ * with counter (cycle, observation pair). */
+HZLB_API int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
+                                    const double *values, const double *sd, size_t p,
+                                    const double *perturbations, uint64_t perturbation_seed,
+                                    uint64_t cycle, double nis_limit, double *nis, int *applied);
+/* No counterpart in the reference.  Device address of the compact state (members x
+ * hzlb_compact_size complex entries of the configured precision, member-major), for device
+ * code that reads or modifies the ensemble in place (the learned reduced forecast).  Valid
+ * until the handle is destroyed; call it again before each modification so the next step
+ * does not reuse velocities cached from the old state. */
+HZLB_API int hzlb_state_device(hzlb_ensemble *h, void **state);
 
 /* ---- drop-in drivers for the reference's ensemble entry points ---------------------- */
 /* hzl::Parameters (include/hzl/solver.hpp:15-23). */

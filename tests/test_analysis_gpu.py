@@ -103,10 +103,12 @@ def test_enkf_single_observation_equals_serial_update(hzlb, oracle):
         assert rel_l2(got[m], solvers[m].state()[0]) < 1e-12
 
 
+@pytest.mark.parametrize("members,p", [(48, 64), (150, 200), (70, 333)])
 @pytest.mark.parametrize("precision,tol", [(8, 1e-11), (4, 2e-5)])
-def test_enkf_batch_many_observations(hzlb, precision, tol):
-    """p = 64 observations at once against X + A W with W from the FP64 ensemble-space formula."""
-    n, members, p = 64, 48, 64
+def test_enkf_batch_many_observations(hzlb, precision, tol, members, p):
+    """p observations at once against X + A W with W from the FP64 ensemble-space formula
+    (one, several and ragged Cholesky blocks of 64)."""
+    n = 64
     e, w = _ensemble(hzlb, n, members, precision=precision)
     rng = np.random.default_rng(9)
     xs, ys = rng.integers(0, n, p), rng.integers(0, n, p)
@@ -122,3 +124,62 @@ def test_enkf_batch_many_observations(hzlb, precision, tol):
     # the analysis pulls the ensemble mean towards the observations
     after = e.observe(xs, ys).mean(axis=0)
     assert np.linalg.norm(after - vals) < np.linalg.norm(hx.mean(axis=0) - vals)
+
+
+def _nis_reference(hx, vals, sd):
+    M = hx.shape[0]
+    ha = hx - hx.mean(axis=0)
+    S = ha.T @ ha / (M - 1) + np.diag(sd ** 2)
+    d = vals - hx.mean(axis=0)
+    return float(d @ np.linalg.solve(S, d) / len(vals))
+
+
+def test_innovation_statistic_and_rejection(hzlb):
+    """The normalised innovation statistic against numpy; above the limit the state is left
+    unchanged."""
+    n, members, p = 64, 96, 150
+    e, w = _ensemble(hzlb, n, members, precision=8)
+    rng = np.random.default_rng(4)
+    xs, ys = rng.integers(0, n, p), rng.integers(0, n, p)
+    sd = np.full(p, 0.1)
+    eps = rng.normal(size=(members, p))
+    for scale in (0.0, 5.0):
+        hx = e.observe(xs, ys)
+        vals = hx.mean(axis=0) + scale * rng.normal(size=p)
+        expect = _nis_reference(hx, vals, sd)
+        before = e.get_state_compact()
+        nis, applied = e.enkf_analysis_nis(xs, ys, vals, sd, eps, nis_limit=3.0)
+        assert abs(nis - expect) < 1e-9 * max(1.0, expect)
+        if expect > 3.0:
+            assert not applied
+            np.testing.assert_array_equal(e.get_state_compact(), before)
+        else:
+            assert applied
+
+
+@pytest.mark.parametrize("precision,tol", [(8, 1e-11), (4, 2e-5)])
+def test_device_perturbations_match_philox(hzlb, oracle, precision, tol):
+    """Perturbations drawn on the device equal the Philox draws restated by the oracle, so the
+    analysis equals the host-perturbation analysis with those draws."""
+    import ctypes as C
+    n, members, p = 32, 40, 70
+    seed, cycle = 1234, 7
+    a, w = _ensemble(hzlb, n, members, precision=precision)
+    b, _ = _ensemble(hzlb, n, members, precision=precision)
+    rng = np.random.default_rng(5)
+    xs, ys = rng.integers(0, n, p), rng.integers(0, n, p)
+    vals, sd = rng.normal(0, 0.1, p), np.full(p, 0.2)
+    eps = np.zeros((members, p))
+    x1, x2 = C.c_double(), C.c_double()
+    for m in range(members):
+        for o in range(0, p, 2):
+            oracle.lib.ho_philox_normal_pair(seed, m, cycle ^ (0x454E4B46 << 32), o >> 1,
+                                             C.byref(x1), C.byref(x2))
+            eps[m, o] = x1.value
+            if o + 1 < p:
+                eps[m, o + 1] = x2.value
+    na, _ = a.enkf_analysis_nis(xs, ys, vals, sd, None, seed=seed, cycle=cycle)
+    nb_, _ = b.enkf_analysis_nis(xs, ys, vals, sd, eps)
+    assert abs(na - nb_) < 1e-12 * max(1.0, abs(nb_))
+    assert rel_l2(a.get_state_compact().astype(np.complex128),
+                  b.get_state_compact().astype(np.complex128)) < tol

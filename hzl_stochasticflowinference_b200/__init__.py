@@ -160,6 +160,19 @@ def library() -> C.CDLL:
         "hzlb_mlp_set_scales": (C.c_int, [vp, _fp, _fp]),
         "hzlb_mlp_forward": (C.c_int, [vp, vp, C.c_int, vp, vp]),
         "hzlb_mlp_train_step": (C.c_int, [vp, vp, vp, C.c_int, C.c_float, _dp]),
+        "hzlb_mlp_shape": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "hzlb_fit_pod": (C.c_int, [C.c_size_t, C.c_size_t, _dp, C.c_size_t, C.c_double, C.c_int,
+                                   C.POINTER(C.c_size_t), _dp, _dp, _dp, _dp]),
+        "hzlb_pod_fit": (C.c_int, [C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, C.c_uint64,
+                                   C.c_int, C.POINTER(vp)]),
+        "hzlb_pod_destroy": (None, [vp]),
+        "hzlb_pod_info": (C.c_int, [vp, C.POINTER(C.c_int), _dp, _dp, _dp]),
+        "hzlb_pod_modes": (C.c_int, [vp, _fp, _fp]),
+        "hzlb_pod_project": (C.c_int, [vp, vp, C.c_int, vp, C.c_longlong, vp]),
+        "hzlb_noise_amplitudes": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
+                                            C.c_uint64, C.c_int, vp, C.c_longlong, vp]),
+        "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -379,6 +392,10 @@ class Ensemble:
                                                 None if e is None else _p(e), seed, cycle,
                                                 nis_limit, C.byref(nis), C.byref(applied)))
         return nis.value, bool(applied.value)
+
+    def learned_forecast(self, pod: "Pod", mlp: "Mlp", dt: float, steps: int) -> None:
+        """One window of the learned reduced forecast (hzlb_learned_forecast)."""
+        _check(self._lib.hzlb_learned_forecast(self._h, pod._h, mlp._h, dt, steps))
 
     def state_device(self) -> int:
         """Device address of the compact state (see hzlb_state_device)."""
@@ -602,3 +619,73 @@ class Mlp:
                                              self._dev(target, self.r), x.shape[0], lr,
                                              C.byref(loss)))
         return loss.value
+
+
+def fit_pod(snapshots, max_rank: int, fraction: float = 0.9999, device: int = 0) -> dict:
+    """hzl::fit_pod (src/reduced.cpp:36-136) on the GPU: snapshots (m, ...) complex."""
+    x = _c128(snapshots)
+    m = x.shape[0]
+    dim = x[0].size
+    mean = np.zeros(dim, np.complex128)
+    modes = np.zeros((max_rank, dim), np.complex128)
+    sv = np.zeros(max_rank)
+    rank, cap = C.c_size_t(), C.c_double()
+    _check(library().hzlb_fit_pod(m, dim, x.view(np.float64).ctypes.data_as(_dp), max_rank,
+                                  fraction, device, C.byref(rank), mean.view(np.float64).ctypes.data_as(_dp),
+                                  modes.view(np.float64).ctypes.data_as(_dp), _p(sv), C.byref(cap)))
+    r = rank.value
+    shape = x.shape[1:]
+    return dict(mean=mean.reshape(shape), modes=modes[:r].reshape((r,) + shape),
+                singular_values=sv[:r].copy(), captured=cap.value)
+
+
+class Pod:
+    """POD basis of compact FP32 ensemble snapshots on the device (hzlb_pod_*)."""
+
+    def __init__(self, n: int, snapshots, rank: int, oversample: int = 32, iterations: int = 60,
+                 seed: int = 0, device: int = 0):
+        self._lib = library()
+        self._h = C.c_void_p()
+        t = snapshots
+        if not (t.is_cuda and t.is_contiguous() and t.dtype.is_floating_point and
+                t.element_size() == 4 and t.dim() == 2):
+            raise ValueError("snapshots: contiguous CUDA float32 [count][2 * compact] tensor")
+        _check(self._lib.hzlb_pod_fit(n, t.shape[0], C.c_void_p(t.data_ptr()), rank, oversample,
+                                      iterations, seed, device, C.byref(self._h)))
+        self.n, self.rank = n, rank
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.hzlb_pod_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def info(self) -> dict:
+        r = C.c_int()
+        ev = np.zeros(self.rank)
+        cap, res = C.c_double(), C.c_double()
+        _check(self._lib.hzlb_pod_info(self._h, C.byref(r), _p(ev), C.byref(cap), C.byref(res)))
+        return dict(rank=r.value, eigenvalues=ev, captured=cap.value, residual=res.value)
+
+    def modes(self):
+        k = retained_k(self.n)
+        size = (k + 1) * (2 * k + 1)
+        modes = np.zeros((self.rank, 2 * size), np.float32)
+        mean = np.zeros(2 * size, np.float32)
+        _check(self._lib.hzlb_pod_modes(self._h, modes.ctypes.data_as(_fp), mean.ctypes.data_as(_fp)))
+        return modes, mean
+
+    def project(self, states, out=None):
+        import torch
+        if out is None:
+            out = torch.empty((states.shape[0], self.rank), dtype=torch.float32, device=states.device)
+        _check(self._lib.hzlb_pod_project(self._h, C.c_void_p(states.data_ptr()), states.shape[0],
+                                          C.c_void_p(out.data_ptr()), out.stride(0), None))
+        return out
+
+
+def noise_amplitudes(config: Config, dt: float, first_step: int, steps: int, count: int, out):
+    """Noise-mode amplitudes of a forecast window into out[count][>= 8] (CUDA float32)."""
+    cfg = config.to_c()
+    _check(library().hzlb_noise_amplitudes(C.byref(cfg), dt, first_step, steps, count,
+                                           C.c_void_p(out.data_ptr()), out.stride(0), None))
+    return out

@@ -249,6 +249,15 @@ int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *
             *applied = r.applied;
     });
 }
+int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
+                          uint64_t steps) {
+    int rc = HZLB_OK;
+    const int outer = guarded([&] {
+        auto &e = engine(h);
+        rc = hzlb::learned_forecast(e, e.config(), pod, mlp, 8, dt, steps);
+    });
+    return outer != HZLB_OK ? outer : rc;
+}
 int hzlb_state_device(hzlb_ensemble *h, void **state) {
     return guarded([&] {
         need(state, "state");

@@ -98,7 +98,7 @@ inline cudaError_t gemm(const GemmArgs &g, cudaStream_t s, bool lower = false) {
 // inv (ld NB).  info[0] = first nonpositive pivot + 1 (left at 0 on success).  L occupies the
 // lower triangle of A and L^{-1} the rest, transposed and shifted one column right:
 // (L^{-1})[i][c], i >= c, lives at A[c][i + 1].
-__global__ void __launch_bounds__(256) potrf_block(double *S, int p, int k0, int nb, double *inv,
+static __global__ void __launch_bounds__(256) potrf_block(double *S, int p, int k0, int nb, double *inv,
                                                   int *info) {
     __shared__ double A[NB][NB + 1];
     __shared__ double piv[NB];

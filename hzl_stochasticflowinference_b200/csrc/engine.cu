@@ -601,6 +601,7 @@ template <typename R> class EngineT final : public Engine {
         cuda_check(cudaGetLastError(), "launch inflation");
         w_valid_ = false;
     }
+    const hzlb_config &config() const override { return cfg_; }
     void *state_device() override {
         w_valid_ = false;
         return omega_.ptr;

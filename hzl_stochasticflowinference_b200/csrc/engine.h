@@ -102,6 +102,7 @@ class Engine {
     // device address of the compact state (members x compact_size complex entries); the
     // caller may modify it until its next call on this ensemble
     virtual void *state_device() = 0;
+    virtual const hzlb_config &config() const = 0;
     virtual size_t compact_size() const = 0;
     virtual int members() const = 0;
     virtual void *stream() const = 0;
@@ -128,6 +129,10 @@ namespace tc {
 struct GemmArgs;
 }
 cudaError_t gemm(const tc::GemmArgs &g, int dtype, cudaStream_t s);
+
+// One window of the learned reduced forecast (pod.cu) on an FP32 ensemble.
+int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp *mlp, int q,
+                     double dt, uint64_t steps);
 
 // Message returned by hzlb_last_error() on this thread.
 void set_last_error(const std::string &message);

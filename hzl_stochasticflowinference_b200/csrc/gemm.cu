@@ -17,7 +17,7 @@ template <typename TIn, int BN> cudaError_t launch(const tc::GemmArgs &g, cudaSt
             return e;
         configured[dev] = true;
     }
-    const dim3 grid((g.N + BN - 1) / BN, (g.M + tc::BM - 1) / tc::BM);
+    const dim3 grid((g.N + BN - 1) / BN, (g.M + tc::BM - 1) / tc::BM, g.splits > 1 ? g.splits : 1);
     tc::umma_gemm_kernel<TIn, BN><<<grid, 128, smem, s>>>(g);
     return cudaGetLastError();
 }

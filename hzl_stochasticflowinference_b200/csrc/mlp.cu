@@ -159,6 +159,16 @@ class Mlp {
             cudaStreamDestroy(stream_);
     }
     size_t count() const { return count_; }
+    void shape(int *r, int *q, int *hidden, int *max_batch) const {
+        if (r)
+            *r = R_;
+        if (q)
+            *q = I_ - R_;
+        if (hidden)
+            *hidden = H_;
+        if (max_batch)
+            *max_batch = B_;
+    }
     void *stream() const { return stream_; }
     void set_params(const float *host) {
         cuda_check(cudaMemcpyAsync(params_.ptr, host, count_ * sizeof(float), cudaMemcpyHostToDevice,
@@ -383,6 +393,13 @@ HZLB_API int hzlb_mlp_create(int r, int q, int hidden, int max_batch, int device
 }
 HZLB_API void hzlb_mlp_destroy(hzlb_mlp *h) { delete h; }
 HZLB_API size_t hzlb_mlp_param_count(const hzlb_mlp *h) { return h && h->mlp ? h->mlp->count() : 0; }
+HZLB_API int hzlb_mlp_shape(const hzlb_mlp *h, int *r, int *q, int *hidden, int *max_batch) {
+    return guarded_mlp([&] {
+        if (!h || !h->mlp)
+            hzlb::raise(HZLB_EINVAL, "null MLP handle");
+        h->mlp->shape(r, q, hidden, max_batch);
+    });
+}
 HZLB_API int hzlb_mlp_set_params(hzlb_mlp *h, const float *params) {
     return guarded_mlp([&] { get(h).set_params(params); });
 }

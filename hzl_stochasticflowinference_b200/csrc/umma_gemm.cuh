@@ -112,6 +112,12 @@ struct GemmArgs {
     float *pre;           // optional pre-activation output (EPI_BIAS_GELU), ldc
     int epilogue;
     unsigned int *status;
+    // split-K: with splits > 1, blockIdx.z takes K elements [z kchunk, (z+1) kchunk) (kchunk a
+    // multiple of the slab width, every split nonempty) and writes alpha * its partial product
+    // to partial[z][M][N] (no beta, bias or activation); the caller sums the slices.
+    int splits;
+    int kchunk;
+    float *partial;
 };
 
 constexpr int BM = 128;
@@ -197,6 +203,13 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const TIn *A = static_cast<const TIn *>(g.A);
     const TIn *B = static_cast<const TIn *>(g.B);
+    int K = g.K;
+    if (g.splits > 1) {
+        const int kb = blockIdx.z * g.kchunk;
+        K = g.K - kb < g.kchunk ? g.K - kb : g.kchunk;
+        A += g.a_kcontig ? static_cast<long long>(kb) : static_cast<long long>(kb) * g.lda;
+        B += g.b_kcontig ? static_cast<long long>(kb) : static_cast<long long>(kb) * g.ldb;
+    }
     const bool a_fast = g.a_kcontig && (reinterpret_cast<uintptr_t>(A) & 15) == 0 &&
                         (g.lda * static_cast<long long>(sizeof(TIn))) % 16 == 0;
     const bool b_fast = g.b_kcontig && (reinterpret_cast<uintptr_t>(B) & 15) == 0 &&
@@ -216,11 +229,11 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
     tc_fence_after();
     const uint32_t tmem = tmem_base;
 
-    const int slabs = (g.K + EPS - 1) / EPS;
+    const int slabs = (K + EPS - 1) / EPS;
     auto load = [&](int s) {
         const int b = s % STAGES;
-        stage_slab<TIn, BM>(sa + b * A_BYTES, A, g.lda, g.a_kcontig, a_fast, g.M, g.K, m0, s * EPS);
-        stage_slab<TIn, BN>(sb + b * B_BYTES, B, g.ldb, g.b_kcontig, b_fast, g.N, g.K, n0, s * EPS);
+        stage_slab<TIn, BM>(sa + b * A_BYTES, A, g.lda, g.a_kcontig, a_fast, g.M, K, m0, s * EPS);
+        stage_slab<TIn, BN>(sb + b * B_BYTES, B, g.ldb, g.b_kcontig, b_fast, g.N, K, n0, s * EPS);
     };
     for (int s = 0; s < STAGES - 1; ++s) {
         if (s < slabs)
@@ -282,6 +295,10 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
                     if (col >= g.N)
                         continue;
                     float x = g.alpha * v[i];
+                    if (g.splits > 1) {
+                        g.partial[(static_cast<long long>(blockIdx.z) * g.M + row) * g.N + col] = x;
+                        continue;
+                    }
                     const long long at = static_cast<long long>(row) * g.ldc + col;
                     if (g.beta != 0.0f && g.C)
                         x += g.beta * g.C[at];

@@ -280,6 +280,8 @@ HZLB_API int hzlb_mlp_create(int r, int q, int hidden, int max_batch, int device
                              hzlb_mlp **out);
 HZLB_API void hzlb_mlp_destroy(hzlb_mlp *h);
 HZLB_API size_t hzlb_mlp_param_count(const hzlb_mlp *h);
+/* r, q, hidden width and maximum batch of the network */
+HZLB_API int hzlb_mlp_shape(const hzlb_mlp *h, int *r, int *q, int *hidden, int *max_batch);
 /* host arrays of hzlb_mlp_param_count floats; grads (may be NULL) receives the gradient of the
  * last training step */
 HZLB_API int hzlb_mlp_set_params(hzlb_mlp *h, const float *params);
@@ -293,6 +295,58 @@ HZLB_API int hzlb_mlp_forward(hzlb_mlp *h, const float *x, int batch, float *y, 
  * pointers); *loss = that error before the update.  lr = 0 computes the gradient only. */
 HZLB_API int hzlb_mlp_train_step(hzlb_mlp *h, const float *x, const float *target, int batch,
                                  float lr, double *loss);
+
+/* ---- proper orthogonal decomposition (reduced.cpp:36-136) ---------------------------- */
+/* PODBasis fit_pod(snapshots, maximum_rank, variance_fraction) (reduced.hpp:16-17) on the
+ * GPU: m (2..512) snapshots of `dimension` complex entries (interleaved doubles), mean,
+ * Gram matrix of the centred snapshots (Re sum conj(a) b) in FP64 on the device, the
+ * reference's cyclic Jacobi eigensolver and truncation rules, modes X^T v / sqrt(lambda)
+ * orthonormalised as by its two Gram-Schmidt passes.  Outputs: *rank modes (modes: max_rank
+ * x dimension complex), mean (dimension complex), singular_values (max_rank), *captured.
+ * Errors as the reference: HZLB_EINVAL for its invalid_argument cases, HZLB_ERUNTIME for
+ * non-convergence, degenerate modes or no resolved mode. */
+HZLB_API int hzlb_fit_pod(size_t m, size_t dimension, const double *snapshots, size_t max_rank,
+                          double fraction, int device, size_t *rank, double *mean, double *modes,
+                          double *singular_values, double *captured);
+
+/* No counterpart in the reference (its fit is capped at 512 snapshots).  POD of `snapshots`
+ * FP32 fields of an n x n ensemble in the compact layout (device pointer, snapshots x
+ * hzlb_compact_size complex floats), with the reference's inner product (spectral_inner over
+ * the full spectrum of the real fields).  Gram matrix by 3xTF32 tensor-core products; the
+ * leading `rank` eigenpairs by subspace iteration on rank + oversample vectors (`iterations`
+ * sweeps, random start from `seed`) and a Rayleigh-Ritz step, or by Jacobi on the whole Gram
+ * matrix when snapshots <= 256.  The handle keeps the mean and modes for hzlb_pod_project and
+ * hzlb_learned_forecast. */
+typedef struct hzlb_pod hzlb_pod;
+HZLB_API int hzlb_pod_fit(int n, int snapshots, const void *data, int rank, int oversample,
+                          int iterations, uint64_t seed, int device, hzlb_pod **out);
+HZLB_API void hzlb_pod_destroy(hzlb_pod *h);
+/* rank, eigenvalues (rank doubles), captured variance fraction, and the largest relative
+ * eigen-residual |G v - lambda v| / lambda of the returned pairs */
+HZLB_API int hzlb_pod_info(hzlb_pod *h, int *rank, double *eigenvalues, double *captured,
+                           double *residual);
+/* host copies: modes (rank x compact complex floats, orthonormal under spectral_inner) and
+ * the mean (compact complex floats); either may be NULL */
+HZLB_API int hzlb_pod_modes(hzlb_pod *h, float *modes, float *mean);
+/* coefficients[i][j] (row stride ldc) = spectral_inner(mode j, state i - mean), the
+ * reference's PODBasis::project (reduced.cpp:16-26), for `count` compact FP32 states (device
+ * pointers).  stream NULL: the handle's stream, waited for. */
+HZLB_API int hzlb_pod_project(hzlb_pod *h, const void *states, int count, float *coefficients,
+                              long long ldc, void *stream);
+/* Noise-mode amplitudes of a forecast window for `count` members of an ensemble configured by
+ * `config`: for (kx, ky) = (1,0), (0,1), (1,1), (1,-1), the sum over steps [first_step,
+ * first_step + steps) of the noise increments hzlb_step adds to that mode, re and im:
+ * out[m][0..7] (device, row stride ldo).  stream NULL: waited for. */
+HZLB_API int hzlb_noise_amplitudes(const hzlb_config *config, double dt, uint64_t first_step,
+                                   uint64_t steps, int count, float *out, long long ldo,
+                                   void *stream);
+/* One window of the learned reduced forecast on an FP32 ensemble, in place of `steps` calls'
+ * worth of hzlb_step: a = project(state), x = (a, noise amplitudes of the window),
+ * state += modes (mlp(x) - a); the part of the state outside the POD space is carried
+ * unchanged.  Advances the ensemble's time and step counter by `steps`.  The network must
+ * have r = the POD rank, q = 8 and max_batch >= members. */
+HZLB_API int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
+                                   uint64_t steps);
 
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */

@@ -136,6 +136,7 @@ def library() -> C.CDLL:
                                              C.c_uint64, C.c_uint64, C.c_double, _dp,
                                              C.POINTER(C.c_int)]),
         "hzlb_state_device": (C.c_int, [vp, C.POINTER(vp)]),
+        "hzlb_ensemble_mean": (C.c_int, [vp, _dp]),
         "hzlb_grf_spectrum": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, _dp]),
         "hzlb_run_ensemble": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), C.c_double,
                                         C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_int,
@@ -172,7 +173,10 @@ def library() -> C.CDLL:
         "hzlb_pod_project": (C.c_int, [vp, vp, C.c_int, vp, C.c_longlong, vp]),
         "hzlb_noise_amplitudes": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
                                             C.c_uint64, C.c_int, vp, C.c_longlong, vp]),
-        "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64]),
+        "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, vp]),
+        "hzlb_ensemble_mean_device": (C.c_int, [vp, vp]),
+        "hzlb_add_window_noise": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
+                                            C.c_uint64, C.c_int, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -393,9 +397,25 @@ class Ensemble:
                                                 nis_limit, C.byref(nis), C.byref(applied)))
         return nis.value, bool(applied.value)
 
-    def learned_forecast(self, pod: "Pod", mlp: "Mlp", dt: float, steps: int) -> None:
-        """One window of the learned reduced forecast (hzlb_learned_forecast)."""
-        _check(self._lib.hzlb_learned_forecast(self._h, pod._h, mlp._h, dt, steps))
+    def learned_forecast(self, pod: "Pod", mlp: "Mlp", dt: float, steps: int,
+                         mean_increment=None) -> None:
+        """One window of the learned reduced forecast (hzlb_learned_forecast);
+        mean_increment: optional CUDA float32 tensor (compact field) moving the ensemble mean."""
+        ptr = None
+        if mean_increment is not None:
+            _torch_ready()
+            ptr = C.c_void_p(mean_increment.data_ptr())
+        _check(self._lib.hzlb_learned_forecast(self._h, pod._h, mlp._h, dt, steps, ptr))
+
+    def mean_device(self, out) -> None:
+        """Member mean of the compact state into out (CUDA tensor of the state's precision)."""
+        _check(self._lib.hzlb_ensemble_mean_device(self._h, C.c_void_p(out.data_ptr())))
+
+    def mean_compact(self) -> np.ndarray:
+        """Ensemble mean, compact layout, complex128."""
+        out = np.zeros(self.compact_size, np.complex128)
+        _check(self._lib.hzlb_ensemble_mean(self._h, out.view(np.float64).ctypes.data_as(_dp)))
+        return out
 
     def state_device(self) -> int:
         """Device address of the compact state (see hzlb_state_device)."""
@@ -538,6 +558,13 @@ def ensemble_kalman_filter(ds: dict, p: Parameters, members: int, seed: int,
     return dict(records=rec.reshape(-1, 4), means=means[:k].copy())
 
 
+def _torch_ready():
+    """The library runs on its own non-blocking streams: wait for torch's pending work on the
+    tensors passed in before handing them over."""
+    import torch
+    torch.cuda.current_stream().synchronize()
+
+
 class Mlp:
     """Learned reduced forecast network (hzlb_mlp_*): r POD coefficients plus q noise-mode
     amplitudes -> r coefficients one window later, BF16 on the tcgen05 tensor cores.  Batches
@@ -609,12 +636,14 @@ class Mlp:
         import torch
         if out is None:
             out = torch.empty((x.shape[0], self.r), dtype=torch.float32, device=x.device)
+        _torch_ready()
         _check(self._lib.hzlb_mlp_forward(self._h, self._dev(x, self.r + self.q), x.shape[0],
                                           self._dev(out, self.r), None))
         return out
 
     def train_step(self, x, target, lr: float) -> float:
         loss = C.c_double()
+        _torch_ready()
         _check(self._lib.hzlb_mlp_train_step(self._h, self._dev(x, self.r + self.q),
                                              self._dev(target, self.r), x.shape[0], lr,
                                              C.byref(loss)))
@@ -650,6 +679,7 @@ class Pod:
         if not (t.is_cuda and t.is_contiguous() and t.dtype.is_floating_point and
                 t.element_size() == 4 and t.dim() == 2):
             raise ValueError("snapshots: contiguous CUDA float32 [count][2 * compact] tensor")
+        _torch_ready()
         _check(self._lib.hzlb_pod_fit(n, t.shape[0], C.c_void_p(t.data_ptr()), rank, oversample,
                                       iterations, seed, device, C.byref(self._h)))
         self.n, self.rank = n, rank
@@ -678,7 +708,15 @@ class Pod:
         import torch
         if out is None:
             out = torch.empty((states.shape[0], self.rank), dtype=torch.float32, device=states.device)
-        _check(self._lib.hzlb_pod_project(self._h, C.c_void_p(states.data_ptr()), states.shape[0],
+        return self.project_ptr(states.data_ptr(), states.shape[0], out)
+
+    def project_ptr(self, ptr: int, count: int, out):
+        """Projections of `count` compact FP32 states at device address ptr into out (CUDA
+        float32, rows of stride out.stride(0))."""
+        if out.shape[0] != count or out.shape[1] < self.rank or out.stride(1) != 1:
+            raise ValueError("out must be [count][>= rank] with unit column stride")
+        _torch_ready()
+        _check(self._lib.hzlb_pod_project(self._h, C.c_void_p(ptr), count,
                                           C.c_void_p(out.data_ptr()), out.stride(0), None))
         return out
 
@@ -686,6 +724,16 @@ class Pod:
 def noise_amplitudes(config: Config, dt: float, first_step: int, steps: int, count: int, out):
     """Noise-mode amplitudes of a forecast window into out[count][>= 8] (CUDA float32)."""
     cfg = config.to_c()
+    _torch_ready()
     _check(library().hzlb_noise_amplitudes(C.byref(cfg), dt, first_step, steps, count,
                                            C.c_void_p(out.data_ptr()), out.stride(0), None))
     return out
+
+
+def add_window_noise(config: Config, dt: float, first_step: int, steps: int, count: int,
+                     ptr: int) -> None:
+    """Adds a window's noise increments to `count` compact FP32 states at device address ptr."""
+    cfg = config.to_c()
+    _torch_ready()
+    _check(library().hzlb_add_window_noise(C.byref(cfg), dt, first_step, steps, count,
+                                           C.c_void_p(ptr), None))

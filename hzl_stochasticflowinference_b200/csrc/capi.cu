@@ -250,13 +250,26 @@ int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *
     });
 }
 int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
-                          uint64_t steps) {
+                          uint64_t steps, const void *mean_increment) {
     int rc = HZLB_OK;
     const int outer = guarded([&] {
         auto &e = engine(h);
-        rc = hzlb::learned_forecast(e, e.config(), pod, mlp, 8, dt, steps);
+        rc = hzlb::learned_forecast(e, e.config(), pod, mlp, 8, dt, steps, mean_increment);
     });
     return outer != HZLB_OK ? outer : rc;
+}
+int hzlb_ensemble_mean_device(hzlb_ensemble *h, void *mean) {
+    return guarded([&] {
+        need(mean, "mean");
+        engine(h).mean_device(mean);
+    });
+}
+int hzlb_ensemble_mean(hzlb_ensemble *h, double *mean) {
+    return guarded([&] {
+        need(mean, "mean");
+        auto &e = engine(h);
+        e.member_sum(nullptr, static_cast<double>(e.members()), mean);
+    });
 }
 int hzlb_state_device(hzlb_ensemble *h, void **state) {
     return guarded([&] {

@@ -602,6 +602,13 @@ template <typename R> class EngineT final : public Engine {
         w_valid_ = false;
     }
     const hzlb_config &config() const override { return cfg_; }
+    void mean_device(void *out) override {
+        const long long nr = 2 * static_cast<long long>(compact_);
+        member_mean<R><<<static_cast<unsigned>((nr + 31) / 32), dim3(32, 8), 0, stream_>>>(
+            reinterpret_cast<const R *>(omega_.ptr), nr, M_, static_cast<R *>(out));
+        cuda_check(cudaGetLastError(), "launch ensemble mean");
+        cuda_check(cudaStreamSynchronize(stream_), "ensemble mean");
+    }
     void *state_device() override {
         w_valid_ = false;
         return omega_.ptr;

@@ -103,6 +103,8 @@ class Engine {
     // caller may modify it until its next call on this ensemble
     virtual void *state_device() = 0;
     virtual const hzlb_config &config() const = 0;
+    // member mean of the compact state into `out` (device, compact_size entries, own precision)
+    virtual void mean_device(void *out) = 0;
     virtual size_t compact_size() const = 0;
     virtual int members() const = 0;
     virtual void *stream() const = 0;
@@ -132,7 +134,7 @@ cudaError_t gemm(const tc::GemmArgs &g, int dtype, cudaStream_t s);
 
 // One window of the learned reduced forecast (pod.cu) on an FP32 ensemble.
 int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp *mlp, int q,
-                     double dt, uint64_t steps);
+                     double dt, uint64_t steps, const void *mean_increment);
 
 // Message returned by hzlb_last_error() on this thread.
 void set_last_error(const std::string &message);

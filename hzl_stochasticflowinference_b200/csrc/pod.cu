@@ -209,13 +209,31 @@ __global__ void sum_slices(const float *partial, int slices, int M, int N, float
         C[(i / N) * ldc + i % N] = s;
     }
 }
-// delta = y - x[:, :r] (x row stride ldx), split for 3xTF32.
+// mean[j] = sum_m (y[m][j] - x[m][j]) / rows: the ensemble mean of the coefficient change
+__global__ void delta_mean(const float *y, const float *x, long long ldx, int rows, int r,
+                           float *mean) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= r)
+        return;
+    double s = 0;
+    for (int m = 0; m < rows; ++m)
+        s += static_cast<double>(y[static_cast<long long>(m) * r + j]) - x[m * ldx + j];
+    mean[j] = static_cast<float>(s / rows);
+}
+// x[m][e] += inc[e] for every member
+__global__ void add_to_members(float *x, const float *inc, int rows, long long D) {
+    const long long total = rows * D;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        x[i] += inc[i % D];
+}
+// delta = y - x[:, :r] (x row stride ldx), less center[j] if given, split for 3xTF32.
 __global__ void delta_split(const float *y, const float *x, long long ldx, int rows, int r,
-                            float *hi, float *lo) {
+                            const float *center, float *hi, float *lo) {
     const long long total = static_cast<long long>(rows) * r;
     for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const float d = y[i] - x[(i / r) * ldx + i % r];
+        const float d = y[i] - x[(i / r) * ldx + i % r] - (center ? center[i % r] : 0.0f);
         const float h = tf32_round(d);
         hi[i] = h;
         lo[i] = d - h;
@@ -242,6 +260,35 @@ __global__ void noise_window(uint64_t seed, uint32_t member_base, int members, u
             }
         out[m * ldo + 2 * q] = static_cast<float>(sr);
         out[m * ldo + 2 * q + 1] = static_cast<float>(si);
+    }
+}
+
+// Adds to every member's compact FP32 state the window's noise: on every mode of the noise
+// shell, the sum over steps [first_step, first_step + steps) of the increments the spectral
+// step adds there (same Philox draws, same conjugate handling of the kx = 0 column).  One block
+// per member, one thread per (kx, ky) candidate with 0 <= kx, |ky| <= kmax.
+__global__ void add_window_noise(float2 *x, int C, int LD, int K, uint64_t seed, uint32_t member_base,
+                                 uint64_t first_step, uint64_t steps, double scale, int kmax) {
+    const int m = blockIdx.x;
+    const int side = 2 * kmax + 1;
+    for (int t = threadIdx.x; t < (kmax + 1) * side; t += blockDim.x) {
+        const int kx = t / side, ky = t % side - kmax;
+        const int k2 = kx * kx + ky * ky;
+        if (k2 < 1 || k2 > kmax * kmax || kx >= C || ky > K || -ky > K)
+            continue;
+        const bool rep = kx > 0 || ky > 0;
+        const uint32_t code = mode_code(kx, rep ? ky : -ky);
+        double sr = 0, si = 0;
+        for (uint64_t s = 0; s < steps; ++s) {
+            double xi1, xi2;
+            philox_normal_pair(seed, member_base + m, first_step + s, code, xi1, xi2);
+            sr += scale * xi1;
+            si += rep ? scale * xi2 : -(scale * xi2);
+        }
+        const int j = ky >= 0 ? ky : ky + LD;
+        float2 &v = x[(static_cast<long long>(m) * C + kx) * LD + j];
+        v.x += static_cast<float>(sr);
+        v.y += static_cast<float>(si);
     }
 }
 
@@ -501,16 +548,23 @@ class PodBasis {
         }
     }
     // One window of the learned forecast on an ensemble held by `e`: project, add the window's
-    // noise amplitudes, run the network, add the change of the coefficients back.
+    // noise amplitudes, run the network (which predicts the coefficients without the direct
+    // contribution of the window's noise), add the change of the coefficients back, then add
+    // the window's noise increments themselves on every noise mode.
+    //
+    // With mean_increment (device, D floats: the change of the ensemble mean over the window
+    // from another forecast, e.g. the spectral solver run on the mean), the network only moves
+    // the members about their mean: the members' coefficient changes are centred over the
+    // ensemble and mean_increment is added to every member.
     void learned_window(Engine &e, const hzlb_config &cfg, hzlb_mlp *mlp, int q, double dt,
-                        uint64_t steps) {
+                        uint64_t steps, const float *mean_increment) {
         ensure_fitted();
         const int M = e.members();
         cudaStream_t s = static_cast<cudaStream_t>(e.stream());
         const int in = r + q;
-        io_.ensure(sizeof(float) * (static_cast<size_t>(M) * (in + 3 * r)), "allocate forecast buffers");
+        io_.ensure(sizeof(float) * (static_cast<size_t>(M) * (in + 3 * r) + r), "allocate forecast buffers");
         float *xin = io_.as<float>(), *y = xin + static_cast<size_t>(M) * in, *dhi = y + static_cast<size_t>(M) * r,
-              *dlo = dhi + static_cast<size_t>(M) * r;
+              *dlo = dhi + static_cast<size_t>(M) * r, *dmean = dlo + static_cast<size_t>(M) * r;
         float *state = static_cast<float *>(e.state_device());
         project(state, M, xin, in, s);
         const double scale = cfg.noise_sigma > 0 ? cfg.noise_sigma * std::sqrt(dt) / kSqrt2 : 0.0;
@@ -519,9 +573,22 @@ class PodBasis {
         cuda_check(cudaGetLastError(), "launch noise amplitudes");
         if (int rc = hzlb_mlp_forward(mlp, xin, M, y, s))
             raise(rc, std::string("learned forecast network: ") + hzlb_last_error());
-        delta_split<<<blocks_for(static_cast<long long>(M) * r), 256, 0, s>>>(y, xin, in, M, r, dhi, dlo);
+        if (mean_increment)
+            delta_mean<<<(r + 63) / 64, 64, 0, s>>>(y, xin, in, M, r, dmean);
+        delta_split<<<blocks_for(static_cast<long long>(M) * r), 256, 0, s>>>(
+            y, xin, in, M, r, mean_increment ? dmean : nullptr, dhi, dlo);
         cuda_check(cudaGetLastError(), "launch coefficient change");
         update(state, M, dhi, dlo, s);
+        if (mean_increment) {
+            add_to_members<<<blocks_for(M * D), 256, 0, s>>>(state, mean_increment, M, D);
+            cuda_check(cudaGetLastError(), "launch mean increment");
+        }
+        if (scale > 0) {
+            add_window_noise<<<M, 64, 0, s>>>(reinterpret_cast<float2 *>(state), C, LD, K, cfg.seed,
+                                              cfg.member_base, e.step_index, steps, scale,
+                                              cfg.noise_kmax);
+            cuda_check(cudaGetLastError(), "launch window noise");
+        }
         e.set_time(e.time + static_cast<double>(steps) * dt, e.step_index + steps);
     }
     void modes(float *modes_host, float *mean_host) {
@@ -817,6 +884,27 @@ HZLB_API int hzlb_pod_project(hzlb_pod *h, const void *states, int count, float 
             b.check_status(s);
     });
 }
+HZLB_API int hzlb_add_window_noise(const hzlb_config *config, double dt, uint64_t first_step,
+                                   uint64_t steps, int count, void *state, void *stream) {
+    using namespace hzlb;
+    return guarded_pod([&] {
+        if (!config || !state || count < 1 || !(dt > 0))
+            raise(HZLB_EINVAL, "invalid window noise arguments");
+        const hzlb_config &c = *config;
+        if (c.precision != 4)
+            raise(HZLB_EINVAL, "window noise is added to FP32 states");
+        const int K = (c.n - 1) / 3, C = K + 1, LD = 2 * K + 1;
+        if (!(c.noise_sigma > 0) || c.noise_kmax < 1)
+            return;
+        const double scale = c.noise_sigma * std::sqrt(dt) / kSqrt2;
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        add_window_noise<<<count, 64, 0, s>>>(static_cast<float2 *>(state), C, LD, K, c.seed,
+                                              c.member_base, first_step, steps, scale, c.noise_kmax);
+        cuda_check(cudaGetLastError(), "launch window noise");
+        if (!stream)
+            cuda_check(cudaStreamSynchronize(s), "window noise");
+    });
+}
 HZLB_API int hzlb_noise_amplitudes(const hzlb_config *config, double dt, uint64_t first_step,
                                    uint64_t steps, int count, float *out, long long ldo, void *stream) {
     using namespace hzlb;
@@ -839,7 +927,7 @@ HZLB_API int hzlb_noise_amplitudes(const hzlb_config *config, double dt, uint64_
 namespace hzlb {
 // Defined here so the learned forecast can reach both the engine and the basis.
 int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp *mlp, int q,
-                     double dt, uint64_t steps) {
+                     double dt, uint64_t steps, const void *mean_increment) {
     return guarded_pod([&] {
         if (!mlp || q != 8 || !(dt > 0) || steps == 0)
             raise(HZLB_EINVAL, "learned forecast needs a network with 8 noise inputs, dt > 0, steps > 0");
@@ -854,7 +942,7 @@ int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp 
         if (nr != b.r || nq != q || batch < e.members())
             raise(HZLB_EINVAL, "network shape does not match the POD rank, 8 noise inputs and the "
                                "ensemble size");
-        b.learned_window(e, cfg, mlp, q, dt, steps);
+        b.learned_window(e, cfg, mlp, q, dt, steps, static_cast<const float *>(mean_increment));
         b.check_status(static_cast<cudaStream_t>(e.stream()));
     });
 }

@@ -174,6 +174,12 @@ HZLB_API int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const u
  * until the handle is destroyed; call it again before each modification so the next step
  * does not reuse velocities cached from the old state. */
 HZLB_API int hzlb_state_device(hzlb_ensemble *h, void **state);
+/* Ensemble mean in the compact layout as interleaved doubles (hzlb_compact_size complex
+ * entries), summed in member order as the reference's filters do (filter.cpp:238-243). */
+HZLB_API int hzlb_ensemble_mean(hzlb_ensemble *h, double *mean);
+/* The member mean of the compact state into a device array of hzlb_compact_size complex
+ * entries in the handle's precision (summed in FP64 over member slices). */
+HZLB_API int hzlb_ensemble_mean_device(hzlb_ensemble *h, void *mean);
 
 /* ---- drop-in drivers for the reference's ensemble entry points ---------------------- */
 /* hzl::Parameters (include/hzl/solver.hpp:15-23). */
@@ -340,13 +346,24 @@ HZLB_API int hzlb_pod_project(hzlb_pod *h, const void *states, int count, float 
 HZLB_API int hzlb_noise_amplitudes(const hzlb_config *config, double dt, uint64_t first_step,
                                    uint64_t steps, int count, float *out, long long ldo,
                                    void *stream);
-/* One window of the learned reduced forecast on an FP32 ensemble, in place of `steps` calls'
- * worth of hzlb_step: a = project(state), x = (a, noise amplitudes of the window),
- * state += modes (mlp(x) - a); the part of the state outside the POD space is carried
- * unchanged.  Advances the ensemble's time and step counter by `steps`.  The network must
- * have r = the POD rank, q = 8 and max_batch >= members. */
+/* Adds to `count` compact FP32 states (device) the noise of a window: on every mode of the
+ * noise shell, the sum of the increments hzlb_step adds over steps [first_step, first_step +
+ * steps) (same Philox draws).  stream NULL: waited for. */
+HZLB_API int hzlb_add_window_noise(const hzlb_config *config, double dt, uint64_t first_step,
+                                   uint64_t steps, int count, void *state, void *stream);
+/* One window of the learned reduced forecast on an FP32 ensemble, in place of `steps`
+ * steps of hzlb_step: a = project(state), x = (a, noise amplitudes of the window),
+ * state += modes (mlp(x) - a), then the window's noise increments (hzlb_add_window_noise).
+ * The network predicts the coefficients at the end of the window less the projection of the
+ * window's noise; outside the POD space the state changes by the noise alone.  Advances the
+ * ensemble's time and step counter by `steps`.  The network must have r = the POD rank, q = 8
+ * and max_batch >= members.  mean_increment: NULL, or a device array (compact FP32 field) with
+ * the change of the ensemble mean over the window from another forecast of the mean (the
+ * spectral step of a one-member ensemble holding hzlb_ensemble_mean_device): then the network
+ * moves the members only about their mean (its coefficient changes are centred over the
+ * ensemble) and mean_increment is added to every member. */
 HZLB_API int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
-                                   uint64_t steps);
+                                   uint64_t steps, const void *mean_increment);
 
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */

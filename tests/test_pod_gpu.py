@@ -138,9 +138,9 @@ def test_noise_amplitudes_match_philox(hzlb, oracle):
     assert np.all(got[:, 8:] == 0)
 
 
-def _learned_setup(hzlb, n=32, members=64, rank=8):
+def _learned_setup(hzlb, n=32, members=64, rank=8, noise=0.0):
     import torch
-    cfg = hzlb.Config(n=n, members=members, precision=4, nu=1e-3, noise_sigma=0.05, noise_kmax=4)
+    cfg = hzlb.Config(n=n, members=members, precision=4, nu=1e-3, noise_sigma=noise, noise_kmax=4)
     e = hzlb.Ensemble(cfg)
     full = _full_fields(hzlb, n, members, 12, 9, decay=0.8)
     e.set_state(full)
@@ -184,3 +184,51 @@ def test_learned_forecast_rejects_mismatched_network(hzlb):
     small = hzlb.Mlp(pod.rank, 8, 64, 16)
     with pytest.raises(hzlb.HzlbInvalidArgument):
         e.learned_forecast(pod, small, 5e-4, 20)
+
+
+def test_learned_forecast_adds_the_window_noise(hzlb):
+    """With the network output off, a window adds exactly the window's noise increments, and
+    those equal the sums of the increments the spectral step would add (Philox restated)."""
+    import torch
+    cfg, e, pod, net = _learned_setup(hzlb, noise=0.05)
+    parts = net.unpack(net.params())
+    parts["W3"][:] = 0
+    parts["b3"][:] = 0
+    net.set_params(net.pack(parts))
+    e.set_time(0.0, 100)
+    before = e.get_state_compact()
+    copy = torch.from_numpy(before.view(np.float32).copy()).cuda()
+    hzlb.add_window_noise(cfg, 5e-4, 100, 20, cfg.members, copy.data_ptr())
+    e.learned_forecast(pod, net, 5e-4, 20)
+    after = e.get_state_compact()
+    np.testing.assert_array_equal(after.view(np.float32), copy.cpu().numpy())
+    changed = np.flatnonzero(np.any(after != before, axis=0))
+    k = (cfg.n - 1) // 3
+    ld = 2 * k + 1
+    kx, j = changed // ld, changed % ld
+    ky = np.where(j <= k, j, j - ld)
+    k2 = kx ** 2 + ky ** 2
+    assert len(changed) == 28 and k2.min() >= 1 and k2.max() <= 16
+
+
+def test_window_noise_matches_philox(hzlb, oracle):
+    import torch
+    cfg = hzlb.Config(n=32, members=3, precision=4, noise_sigma=0.05, noise_kmax=4, seed=5,
+                      member_base=7)
+    k = (cfg.n - 1) // 3
+    ld = 2 * k + 1
+    x = torch.zeros((3, 2 * (k + 1) * ld), dtype=torch.float32, device="cuda")
+    hzlb.add_window_noise(cfg, 1e-3, 10, 4, 3, x.data_ptr())
+    got = x.cpu().numpy().view(np.complex64).reshape(3, k + 1, ld)
+    scale = 0.05 * np.sqrt(1e-3) / np.sqrt(2.0)
+    x1, x2 = C.c_double(), C.c_double()
+    for m in range(3):
+        for kx, ky in [(1, -2), (0, 3), (0, -3), (4, 0)]:
+            rep = kx > 0 or ky > 0
+            code = oracle.lib.ho_mode_code(kx, ky if rep else -ky)
+            sr = si = 0.0
+            for s in range(10, 14):
+                oracle.lib.ho_philox_normal_pair(5, 7 + m, s, code, C.byref(x1), C.byref(x2))
+                sr += scale * x1.value
+                si += scale * (x2.value if rep else -x2.value)
+            np.testing.assert_allclose(got[m, kx, ky % ld], sr + 1j * si, rtol=1e-6, atol=1e-9)

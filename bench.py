@@ -14,6 +14,12 @@ Legs:
   cpu_baseline the reference's own CPU solver (oracle/_ref, hzl::ensemble on all host
                threads) on a bounded sample of the same grid size
 
+  learned      (1 GPU) the learned-forecast EnKF twin experiment at 256^2: POD from 2000
+               snapshots (r=64), the 72-512-512-64 BF16 MLP trained on 100,352 solver
+               transitions of 20 steps, 1024-member EnKF observed on 32x32 points (sigma
+               0.1) every 20 steps for 40 cycles; analysis RMSE and wall-clock per cycle of
+               the spectral, learned, hybrid and no-network forecasts (--no-learned skips it)
+
 `--impl reference` times only the reference CPU path (rank 0; other ranks exit 0).
 """
 from __future__ import annotations
@@ -157,6 +163,37 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def learned_experiment() -> dict:
+    """The learned-forecast EnKF twin experiment (hzl_stochasticflowinference_b200.learned) at
+    its full size; wall-clock per cycle (forecast + analysis + fallback) with the GPU
+    synchronised, the first cycle of each filter excluded as set-up."""
+    try:
+        from hzl_stochasticflowinference_b200 import learned as L
+        tc = L.TwinConfig()
+        t0 = time.perf_counter()
+        res = L.run(tc)
+        keep = ("mean_rmse", "final_rmse", "seconds_per_cycle", "fallback_cycles", "speedup",
+                "rmse_ratio")
+        out = {"workload": f"{tc.n}^2 FP32, EnKF {tc.members} members, {len(L.observation_grid(tc)[0])} "
+                           f"point observations (sigma {tc.obs_sd}) every {tc.window} steps of dt "
+                           f"{tc.dt}, {tc.cycles} cycles; POD r={tc.rank} from {tc.snapshots} "
+                           f"snapshots; MLP {tc.rank + 8}-{tc.hidden}-{tc.hidden}-{tc.rank} BF16 "
+                           f"trained on {res['transitions']} transitions; NIS fallback limit "
+                           f"{tc.nis_limit}",
+               "seconds": time.perf_counter() - t0,
+               "pod": {"captured": res["pod"]["captured"], "residual": res["pod"]["residual"],
+                       "seconds": res["pod_seconds"]},
+               "network": {k: res["training"][k] for k in ("val_mse_network",
+                                                           "val_mse_persistence", "val_skill",
+                                                           "train_seconds", "train_steps")},
+               "data_seconds": res["data_seconds"]}
+        for mode in ("spectral", "learned", "hybrid", "persistence", "hybrid_persistence"):
+            out[mode] = {k: res[mode][k] for k in keep if k in res[mode]}
+        return out
+    except Exception as exc:   # report, never lose the main line
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -165,6 +202,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
@@ -278,6 +316,11 @@ def main():
             cpu = {"value": None, "unit": "member-steps/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
 
+    ens.close()
+    learned = None
+    if rank == 0 and world == 1 and not args.no_learned:
+        learned = learned_experiment()
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": world,
@@ -301,9 +344,9 @@ def main():
             "gpu_launches": 8 * args.steps,
             "clocks": clocks.summary(),
             "status": status,
+            "learned": learned,
         }
         print(json.dumps(out), flush=True)
-    ens.close()
     if pg:
         pg.destroy_process_group()
 

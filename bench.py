@@ -21,6 +21,9 @@ Legs:
                the spectral, learned, hybrid and no-network forecasts (--no-learned skips it)
 
 `--impl reference` times only the reference CPU path (rank 0; other ranks exit 0).
+`--case gemm|enkf|learned` times one isolated workload (1 GPU) and prints its own JSON line:
+the tcgen05 GEMM at 4096^3 (TF32 and BF16), one EnKF analysis at 1024 members x 1024
+observations at 256^2, one learned forecast window at 1024 members x 256^2.
 """
 from __future__ import annotations
 
@@ -194,6 +197,74 @@ def learned_experiment() -> dict:
         return {"error": f"{type(exc).__name__}: {exc}"}
 
 
+def run_case(case: str, steps: int, warmup: int) -> None:
+    """Isolated workloads for micro-benchmarks and small profiler captures."""
+    import ctypes as C
+    import torch
+    import hzl_stochasticflowinference_b200 as hz
+    from hzl_stochasticflowinference_b200 import learned as L
+    steps, warmup = max(1, min(steps, 10)), max(1, min(warmup, 3))
+    ev = lambda: torch.cuda.Event(enable_timing=True)   # noqa: E731
+    out = {"case": case}
+    if case == "gemm":
+        lib = hz.library()
+        fn = lib.hzlb_gemm
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_int] * 4 + [C.c_void_p, C.c_longlong, C.c_int, C.c_void_p, C.c_longlong,
+                                       C.c_int, C.c_void_p, C.c_longlong, C.c_float, C.c_float,
+                                       C.c_void_p]
+        n = 4096
+        for name, code, dt in (("tf32", 4, torch.float32), ("bf16", 2, torch.bfloat16)):
+            a = torch.randn(n, n, device="cuda").to(dt)
+            b = torch.randn(n, n, device="cuda").to(dt)
+            c = torch.zeros(n, n, device="cuda")
+            s = torch.cuda.current_stream().cuda_stream
+            run = lambda: fn(n, n, n, code, a.data_ptr(), n, 1, b.data_ptr(), n, 1,  # noqa: E731
+                             c.data_ptr(), n, 1.0, 0.0, s)
+            for _ in range(warmup):
+                assert run() == 0
+            t0, t1 = ev(), ev()
+            t0.record()
+            for _ in range(steps):
+                run()
+            t1.record()
+            torch.cuda.synchronize()
+            ms = t0.elapsed_time(t1) / steps
+            out[name] = {"ms": ms, "tflops": 2 * n ** 3 / ms / 1e9, "shape": [n, n, n]}
+    else:
+        tc = L.TwinConfig()
+        cfg = tc.config(tc.members, 0)
+        e = hz.Ensemble(cfg)
+        e.set_forcing(hz.kolmogorov_forcing(tc.n, tc.forcing_amplitude, tc.forcing_wavenumber))
+        init = np.zeros((tc.members, e.compact_size), np.complex64)
+        g = hz.full_to_compact(hz.grf_spectrum(tc.n, SEED, 0), tc.n)[0]
+        for m in range(tc.members):
+            init[m] = g + L.perturbation(tc, m)
+        e.set_state_compact(init)
+        e.synchronize()
+        xs, ys = L.observation_grid(tc)
+        vals, sd = np.zeros(len(xs)), np.full(len(xs), tc.obs_sd)
+        if case == "enkf":
+            work = lambda i: e.enkf_analysis_nis(xs, ys, vals, sd, None, seed=1, cycle=i)  # noqa: E731
+        else:
+            snaps = L.snapshots(tc, L.spinup(tc))
+            pod = hz.Pod(tc.n, snaps, tc.rank, seed=1)
+            del snaps
+            net = hz.Mlp(tc.rank, 8, tc.hidden, tc.members, seed=1)
+            work = lambda i: e.learned_forecast(pod, net, tc.dt, tc.window)  # noqa: E731
+        for i in range(warmup):
+            work(i)
+        e.synchronize()
+        t = time.perf_counter()
+        for i in range(steps):
+            work(warmup + i)
+        e.synchronize()
+        out["ms"] = (time.perf_counter() - t) * 1e3 / steps
+        out["members"], out["observations"] = tc.members, len(xs)
+        e.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,7 +274,11 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--case", choices=["gemm", "enkf", "learned"])
     args = ap.parse_args()
+    if args.case:
+        run_case(args.case, args.steps, args.warmup)
+        return
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -1,6 +1,11 @@
-// Launchers and C ABI of the tcgen05 GEMM (umma_gemm.cuh).
+// Launchers and C ABI of the tcgen05 GEMM: the TMA-fed kernel (umma_tma.cuh) when both
+// operands are K-contiguous with 16-byte aligned rows, the cp.async kernel (umma_gemm.cuh)
+// otherwise.
 #include "engine.h"
 #include "umma_gemm.cuh"
+#include "umma_tma.cuh"
+
+#include <mutex>
 
 namespace hzlb {
 namespace {
@@ -21,7 +26,79 @@ template <typename TIn, int BN> cudaError_t launch(const tc::GemmArgs &g, cudaSt
     tc::umma_gemm_kernel<TIn, BN><<<grid, 128, smem, s>>>(g);
     return cudaGetLastError();
 }
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                 const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                 const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encoder() {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+// Tensor map of a K-contiguous operand (rows x K, row stride ld elements): boxes of
+// box_rows x 128 bytes, 128-byte swizzle, zero fill out of range.
+template <typename TIn>
+bool make_map(CUtensorMap *map, const void *ptr, int rows, int K, long long ld, int box_rows) {
+    EncodeTiled fn = encoder();
+    if (!fn || (reinterpret_cast<uintptr_t>(ptr) & 15) || (ld * sizeof(TIn)) % 16)
+        return false;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * sizeof(TIn))};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(tc::SLAB / sizeof(TIn)),
+                               static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUtensorMapDataType dt =
+        sizeof(TIn) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    return fn(map, dt, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+template <typename TIn, int BN, int ST> cudaError_t launch_tma(const tc::GemmArgs &g, cudaStream_t s,
+                                                               bool &used) {
+    used = false;
+    CUtensorMap ma, mb;
+    if (!make_map<TIn>(&ma, g.A, g.M, g.K, g.lda, tc::BM) ||
+        !make_map<TIn>(&mb, g.B, g.N, g.K, g.ldb, BN))
+        return cudaSuccess;
+    constexpr size_t smem = tc::tma_smem<BN, ST>();
+    static bool configured[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 64 && !configured[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(tc::umma_tma_kernel<TIn, BN, ST>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        if (e != cudaSuccess)
+            return e;
+        configured[dev] = true;
+    }
+    const dim3 grid((g.N + BN - 1) / BN, (g.M + tc::BM - 1) / tc::BM, g.splits > 1 ? g.splits : 1);
+    tc::umma_tma_kernel<TIn, BN, ST><<<grid, 128, smem, s>>>(ma, mb, g);
+    used = true;
+    return cudaGetLastError();
+}
 template <typename TIn> cudaError_t launch_any(const tc::GemmArgs &g, cudaStream_t s) {
+    if (g.a_kcontig && g.b_kcontig) {
+        bool used = false;
+        cudaError_t e;
+        if (g.N >= 128)
+            e = launch_tma<TIn, 128, 3>(g, s, used);
+        else if (g.N > 32)
+            e = launch_tma<TIn, 64, 4>(g, s, used);
+        else
+            e = launch_tma<TIn, 32, 4>(g, s, used);
+        if (e != cudaSuccess || used)
+            return e;
+    }
     if (g.N >= 128)
         return launch<TIn, 128>(g, s);
     if (g.N > 32)

@@ -108,6 +108,38 @@ double cholesky_host(std::vector<double> &b, size_t k) {
     }
     return smallest;
 }
+// Orthonormalise the k columns of the m x k row-major matrix y in place (two Gram-Schmidt
+// passes per column); a column that loses almost all of its norm is replaced by a random one.
+void gram_schmidt_host(std::vector<double> &y, size_t m, size_t k, std::mt19937_64 &rng) {
+    std::normal_distribution<double> nd;
+    auto col_norm = [&](size_t j) {
+        double s = 0;
+        for (size_t i = 0; i < m; ++i)
+            s += y[i * k + j] * y[i * k + j];
+        return std::sqrt(s);
+    };
+    for (size_t j = 0; j < k; ++j) {
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            const double before = col_norm(j);
+            for (int pass = 0; pass < 2; ++pass)
+                for (size_t l = 0; l < j; ++l) {
+                    double d = 0;
+                    for (size_t i = 0; i < m; ++i)
+                        d += y[i * k + l] * y[i * k + j];
+                    for (size_t i = 0; i < m; ++i)
+                        y[i * k + j] -= d * y[i * k + l];
+                }
+            const double after = col_norm(j);
+            if (after > 1e-10 * before && after > 0) {
+                for (size_t i = 0; i < m; ++i)
+                    y[i * k + j] /= after;
+                break;
+            }
+            for (size_t i = 0; i < m; ++i)
+                y[i * k + j] = nd(rng);
+        }
+    }
+}
 // Inverse of a lower-triangular k x k matrix.
 std::vector<double> lower_inverse(const std::vector<double> &L, size_t k) {
     std::vector<double> X(k * k, 0.0);
@@ -654,8 +686,18 @@ class PodBasis {
                 for (int i = 0; i < k; ++i)
                     for (int j = 0; j < k; ++j)
                         b[static_cast<size_t>(i) * k + j] *= dsc[i] * dsc[j];
-                if (!(cholesky_host(b, k) > 1e-7))
-                    raise(HZLB_ERUNTIME, "subspace iteration lost rank; reduce oversampling");
+                if (!(cholesky_host(b, k) > 1e-7)) {
+                    // (numerically) dependent columns: Gram-Schmidt on the host, replacing
+                    // each dependent column by a fresh random direction
+                    std::vector<double> y = download(src, static_cast<size_t>(m) * k, s);
+                    gram_schmidt_host(y, m, k, rng);
+                    upload(rd, y, s);
+                    cuda_check(cudaMemcpyAsync(Q, rd.ptr, sizeof(double) * m * k, cudaMemcpyDeviceToDevice, s),
+                               "copy subspace basis");
+                    cuda_check(cudaMemcpyAsync(Y, rd.ptr, sizeof(double) * m * k, cudaMemcpyDeviceToDevice, s),
+                               "copy subspace basis");
+                    return;
+                }
                 const std::vector<double> li = lower_inverse(b, k);
                 // Q = Y D L^{-T}:  rhs[l][j] = dsc[l] li[j][l]
                 std::vector<double> rhs(static_cast<size_t>(k) * k);

@@ -185,6 +185,75 @@ __device__ __forceinline__ float gelu(float x) {
     return 0.5f * x * (1.0f + tanhf(k0 * (x + k1 * x * x * x)));
 }
 
+// Epilogue of a 128 x BN accumulator tile: each warp copies its 32 TMEM lanes (rows) to the
+// shared-memory tile `stage` (row stride BN + 1 floats, conflict-free), then writes its rows
+// back with lanes along the columns, so every global read and write is a contiguous 128-byte
+// row segment.  `stage` must hold 128 x (BN + 1) floats and be free (all copies landed, all
+// MMAs complete).
+template <int BN>
+__device__ __forceinline__ void store_tile(const GemmArgs &g, uint32_t tmem, float *stage, int m0,
+                                           int n0) {
+    constexpr int TS = BN + 1;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    float *mine = stage + warp * 32 * TS;
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            mine[lane * TS + c0 + i] = v[i];
+    }
+    __syncwarp();
+    static_assert(BN % 32 == 0, "store_tile: BN multiple of 32");
+    constexpr int CPL = BN / 32;   // columns per lane
+    constexpr int RB = 8;          // rows per batch: their C reads are all issued first
+    const bool split = g.splits > 1;
+    const bool read_c = !split && g.beta != 0.0f && g.C;
+    for (int r0 = 0; r0 < 32; r0 += RB) {
+        float cin[RB][CPL];
+#pragma unroll
+        for (int rr = 0; rr < RB; ++rr)
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) {
+                const int row = m0 + warp * 32 + r0 + rr, col = n0 + lane + 32 * j;
+                cin[rr][j] = (read_c && row < g.M && col < g.N)
+                                 ? g.C[static_cast<long long>(row) * g.ldc + col]
+                                 : 0.0f;
+            }
+#pragma unroll
+        for (int rr = 0; rr < RB; ++rr) {
+            const int row = m0 + warp * 32 + r0 + rr;
+            if (row >= g.M)
+                break;
+#pragma unroll
+            for (int j = 0; j < CPL; ++j) {
+                const int c = lane + 32 * j, col = n0 + c;
+                if (col >= g.N)
+                    continue;
+                float x = g.alpha * mine[(r0 + rr) * TS + c];
+                if (split) {
+                    g.partial[(static_cast<long long>(blockIdx.z) * g.M + row) * g.N + col] = x;
+                    continue;
+                }
+                const long long at = static_cast<long long>(row) * g.ldc + col;
+                if (read_c)
+                    x += g.beta * cin[rr][j];
+                if (g.epilogue >= EPI_BIAS)
+                    x += g.bias[col];
+                if (g.epilogue == EPI_BIAS_GELU) {
+                    if (g.pre)
+                        g.pre[at] = x;
+                    x = gelu(x);
+                }
+                if (g.C)
+                    g.C[at] = x;
+                if (g.Cbf)
+                    g.Cbf[at] = __float2bfloat16(x);
+            }
+        }
+    }
+}
+
 template <typename TIn, int BN>
 __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
     static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M = 128");
@@ -283,39 +352,7 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
     ok = ok_sh != 0;
     if (ok) {
         tc_fence_after();
-        // epilogue: warp w reads rows 32w..32w+31 (TMEM lanes), 16 columns at a time
-        const int row = m0 + warp * 32 + (threadIdx.x % 32);
-        for (int c0 = 0; c0 < BN; c0 += 16) {
-            float v[16];
-            tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
-            if (row < g.M) {
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int col = n0 + c0 + i;
-                    if (col >= g.N)
-                        continue;
-                    float x = g.alpha * v[i];
-                    if (g.splits > 1) {
-                        g.partial[(static_cast<long long>(blockIdx.z) * g.M + row) * g.N + col] = x;
-                        continue;
-                    }
-                    const long long at = static_cast<long long>(row) * g.ldc + col;
-                    if (g.beta != 0.0f && g.C)
-                        x += g.beta * g.C[at];
-                    if (g.epilogue >= EPI_BIAS)
-                        x += g.bias[col];
-                    if (g.epilogue == EPI_BIAS_GELU) {
-                        if (g.pre)
-                            g.pre[at] = x;
-                        x = gelu(x);
-                    }
-                    if (g.C)
-                        g.C[at] = x;
-                    if (g.Cbf)
-                        g.Cbf[at] = __float2bfloat16(x);
-                }
-            }
-        }
+        store_tile<BN>(g, tmem, reinterpret_cast<float *>(smem), m0, n0);
     } else if (threadIdx.x == 0 && g.status) {
         atomicOr(g.status, STATUS_TIMEOUT);
     }
@@ -326,7 +363,9 @@ __global__ void __launch_bounds__(128) umma_gemm_kernel(const GemmArgs g) {
 }
 
 template <typename TIn, int BN> constexpr size_t gemm_smem() {
-    return STAGES * (BM * SLAB + BN * SLAB);
+    // the ring, which the epilogue reuses for the 128 x (BN + 1) float tile
+    return STAGES * (BM * SLAB + BN * SLAB) > BM * (BN + 1) * 4 ? STAGES * (BM * SLAB + BN * SLAB)
+                                                                : BM * (BN + 1) * 4;
 }
 
 } // namespace tc

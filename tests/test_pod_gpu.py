@@ -89,11 +89,13 @@ def _numpy_pod(x, n, rank):
     return ev[order], modes_w / w, np.trace(G)
 
 
-@pytest.mark.parametrize("m,rank", [(120, 8), (600, 16)])
-def test_compact_pod_matches_numpy(hzlb, m, rank):
+@pytest.mark.parametrize("m,rank,data_rank", [(120, 8, 24), (600, 16, 24), (400, 8, 10)])
+def test_compact_pod_matches_numpy(hzlb, m, rank, data_rank):
+    """(400, 8, 10): the data span fewer directions than the 32 iteration vectors, so the
+    orthonormalisation meets dependent columns and must replace them."""
     import torch
     n = 32
-    full = _full_fields(hzlb, n, m, 24, 5, decay=0.8)
+    full = _full_fields(hzlb, n, m, data_rank, 5, decay=0.8)
     x = hzlb.full_to_compact(full, n).astype(np.complex64).view(np.float32)
     pod = hzlb.Pod(n, torch.from_numpy(x).cuda(), rank, oversample=24, iterations=80, seed=1)
     info = pod.info()

@@ -13,6 +13,11 @@ Legs:
   roofline     dominant kernel: algorithmic bytes per launch / mean launch duration
   cpu_baseline the reference's own CPU solver (oracle/_ref, hzl::ensemble on all host
                threads) on a bounded sample of the same grid size
+  gpu_reference the reference's own GPU path (src/cuda_solver.cu: cuFFT Z2Z, FP64, one solver
+               instance per member launched in sequence, host OU forcing), built for sm_100a by
+               oracle/Makefile, through its hzl-cuda-ensemble-benchmark driver at 256^2
+  fp64         this path's FP64 variant at 256^2 (512 members), device-timed, for a like-for-like
+               precision comparison with gpu_reference
 
   learned      (1 GPU) the learned-forecast EnKF twin experiment at 256^2: POD from 2000
                snapshots (r=64), the 72-512-512-64 BF16 MLP trained on 100,352 solver
@@ -164,6 +169,56 @@ def run_reference(args, rank, world):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
+
+
+def reference_gpu_sample(n: int, steps: int = 20, members: int = 64) -> dict:
+    """The reference's own cuFFT ensemble benchmark (oracle/_ref/hzl-cuda-ensemble-benchmark):
+    its GPU member-steps/s at n^2 (its parameters: nu 0.01, friction 0.1, OU shell forcing,
+    FP64, sequential launches per member)."""
+    exe = ROOT / "oracle" / "_ref" / "hzl-cuda-ensemble-benchmark"
+    if not exe.exists():
+        return {"value": None, "unit": "member-steps/s",
+                "sample": "unavailable: oracle/_ref/hzl-cuda-ensemble-benchmark not built"}
+    workers = os.cpu_count() or 1
+    cmd = [str(exe), str(n), str(steps), "0.00025", str(members), str(workers)]
+    try:
+        proc = subprocess.run(cmd, capture_output=True, text=True, timeout=600, check=True)
+        res = json.loads(proc.stdout.strip().splitlines()[-1])
+    except Exception as exc:   # report, never lose the main line
+        return {"value": None, "unit": "member-steps/s", "sample": f"unavailable: {exc}"}
+    return {"value": res["gpu_member_steps_per_second"], "unit": "member-steps/s",
+            "kind": "reference cuFFT build (FP64)",
+            "sample": f"{' '.join(['hzl-cuda-ensemble-benchmark'] + cmd[1:])}: {members} members x "
+                      f"{steps} steps at {n}^2, its own CUDA path (cuFFT Z2Z FP64, one solver per "
+                      f"member, sequential launches, host OU forcing upload per step); its CPU/GPU "
+                      f"energy agreement {res['maximum_relative_energy_error']:.1e}",
+            "evolution_seconds": res["gpu_evolution_seconds"]}
+
+
+def fp64_sample(hz, torch, n: int, members: int = 512, steps: int = 10) -> dict:
+    """This path in FP64 at n^2: device-timed member-steps/s."""
+    cfg = hz.Config(n=n, members=members, precision=8, nu=NU, alpha=0.0, forcing_kmax=0,
+                    noise_sigma=SIGMA, noise_kmax=4, seed=SEED)
+    e = hz.Ensemble(cfg)
+    init = np.zeros((members, e.compact_size), np.complex128)
+    for m in range(members):
+        init[m] = hz.full_to_compact(hz.grf_spectrum(n, SEED, m), n)[0]
+    e.set_state_compact(init)
+    e.set_forcing(hz.kolmogorov_forcing(n)[None])
+    stream = torch.cuda.ExternalStream(e.stream)
+    for _ in range(3):
+        e.step(DT, 1)
+    e.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(steps):
+        e.step(DT, 1)
+    t1.record(stream)
+    e.synchronize()
+    ms = t0.elapsed_time(t1)
+    e.close()
+    return {"value": members * steps / (ms / 1e3), "unit": "member-steps/s", "members": members,
+            "steps": steps, "dtype": "f64"}
 
 
 def learned_experiment() -> dict:
@@ -392,9 +447,13 @@ def main():
                    "sample": f"unavailable: {exc}"}
 
     ens.close()
-    learned = None
-    if rank == 0 and world == 1 and not args.no_learned:
-        learned = learned_experiment()
+    learned = gpu_ref = fp64 = None
+    if rank == 0 and world == 1:
+        fp64 = fp64_sample(hz, torch, N)
+        if not args.no_cpu_baseline:
+            gpu_ref = reference_gpu_sample(N)
+        if not args.no_learned:
+            learned = learned_experiment()
 
     if rank == 0:
         out = {
@@ -414,6 +473,8 @@ def main():
                          "row_kernel": {"ms": row_ms, "gbs": row_gbs},
                          "column_kernel": {"ms": col_ms, "gbs": col_gbs}},
             "cpu_baseline": cpu,
+            "gpu_reference": gpu_ref,
+            "fp64": fp64,
             "e2e": {"value": e2e_value, "unit": "member-steps/s",
                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
             "gpu_launches": 8 * args.steps,

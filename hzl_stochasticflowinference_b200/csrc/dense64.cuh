@@ -1,6 +1,6 @@
 // FP64 dense linear algebra for the EnKF innovation system (p x p, p up to a few thousand):
 // a tiled SIMT GEMM with arbitrary operand strides, a blocked right-looking Cholesky whose
-// diagonal blocks are factored and inverted in shared memory, and blocked forward/backward
+// diagonal blocks are factored and inverted in shared memory, and blocked forward
 // substitution for many right-hand sides built from the same GEMM.  FP64 stays here on
 // purpose: the innovation Cholesky and solve are the one place the analysis needs it.
 #pragma once
@@ -29,34 +29,54 @@ struct GemmArgs {
 
 // LOWER: skip tiles strictly above the diagonal (only C[m][n], n <= m, is wanted).  A block
 // reads all of its A rows before it writes C, so C may alias the A rows of its own tile when
-// N <= BN (one tile column).
+// N <= BN (one tile column).  The k-tiles are double-buffered: the next tile is loaded into
+// registers while the current one is multiplied from shared memory.
 template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const GemmArgs g) {
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     if (LOWER && n0 > m0 + BM - 1)
         return;
-    __shared__ double As[BK][BM + 1], Bs[BK][BN + 1];
+    __shared__ double As[2][BK][BM + 1], Bs[2][BK][BN + 1];
     const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
     double acc[4][4] = {};
     const bool a_k = g.sak == 1, b_k = g.sbk == 1;
-    for (int k0 = 0; k0 < g.K; k0 += BK) {
+    double ra[4], rb[4];
+    auto fetch = [&](int k0) {
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const int q = tid + 256 * r;
             const int mk_m = a_k ? q / BK : q % BM, mk_k = a_k ? q % BK : q / BM;
             const int gm = m0 + mk_m, gk = k0 + mk_k;
-            As[mk_k][mk_m] = (gm < g.M && gk < g.K) ? g.A[gm * g.sam + gk * g.sak] : 0.0;
+            ra[r] = (gm < g.M && gk < g.K) ? g.A[gm * g.sam + gk * g.sak] : 0.0;
             const int kn_n = b_k ? q / BK : q % BN, kn_k = b_k ? q % BK : q / BN;
             const int gn = n0 + kn_n, gk2 = k0 + kn_k;
-            Bs[kn_k][kn_n] = (gn < g.N && gk2 < g.K) ? g.B[gk2 * g.sbk + gn * g.sbn] : 0.0;
+            rb[r] = (gn < g.N && gk2 < g.K) ? g.B[gk2 * g.sbk + gn * g.sbn] : 0.0;
         }
-        __syncthreads();
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = tid + 256 * r;
+            const int mk_m = a_k ? q / BK : q % BM, mk_k = a_k ? q % BK : q / BM;
+            As[buf][mk_k][mk_m] = ra[r];
+            const int kn_n = b_k ? q / BK : q % BN, kn_k = b_k ? q % BK : q / BN;
+            Bs[buf][kn_k][kn_n] = rb[r];
+        }
+    };
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    int buf = 0;
+    for (int k0 = 0; k0 < g.K; k0 += BK) {
+        const bool more = k0 + BK < g.K;
+        if (more)
+            fetch(k0 + BK);   // global loads in flight during the products below
 #pragma unroll
         for (int k = 0; k < BK; ++k) {
             double a[4], b[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                a[i] = As[k][ty + 16 * i];
-                b[i] = Bs[k][tx + 16 * i];
+                a[i] = As[buf][k][ty + 16 * i];
+                b[i] = Bs[buf][k][tx + 16 * i];
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i)
@@ -64,7 +84,11 @@ template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const G
                 for (int j = 0; j < 4; ++j)
                     acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
-        __syncthreads();
+        if (more) {
+            stash(buf ^ 1);
+            __syncthreads();
+            buf ^= 1;
+        }
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
@@ -186,12 +210,12 @@ inline cudaError_t cholesky(double *S, int p, double *inv, int *info, cudaStream
     return cudaGetLastError();
 }
 
-// Solve (L L^T) z = d for each of `rows` right-hand sides stored as the rows of D (rows x p,
-// row-major); the solutions replace D.  Y is rows x p workspace.
-inline cudaError_t cholesky_solve_rows(const double *L, int p, const double *inv, double *D,
-                                       double *Y, int rows, cudaStream_t s) {
+// Forward substitution L y = d for each of `rows` right-hand sides stored as the rows of D
+// (rows x p, row-major): the solutions go to Y (rows x p); D is overwritten on the way.
+inline cudaError_t forward_rows(const double *L, int p, const double *inv, double *D, double *Y,
+                                int rows, cudaStream_t s) {
     const int nblk = (p + NB - 1) / NB;
-    // forward: Y_k = (D_k - sum_{j<k} Y_j L_kj^T) L_kk^{-T}, right-looking on D
+    // Y_k = (D_k - sum_{j<k} Y_j L_kj^T) L_kk^{-T}, right-looking on D
     for (int b = 0; b < nblk; ++b) {
         const int k0 = b * NB, nb = p - k0 < NB ? p - k0 : NB, pr = p - k0 - nb;
         const double *ib = inv + static_cast<long long>(b) * NB * NB;
@@ -202,22 +226,6 @@ inline cudaError_t cholesky_solve_rows(const double *L, int p, const double *inv
         if (pr > 0) {
             GemmArgs u{rows, pr, nb, -1.0, 1.0, Y + k0, p, 1,
                        L + static_cast<long long>(k0 + nb) * p + k0, 1, p, D + k0 + nb, p};
-            e = gemm(u, s);
-            if (e != cudaSuccess)
-                return e;
-        }
-    }
-    // backward: Z_k = (Y_k - sum_{j>k} Z_j L_jk) L_kk^{-1}, right-looking on Y; Z into D
-    for (int b = nblk - 1; b >= 0; --b) {
-        const int k0 = b * NB, nb = p - k0 < NB ? p - k0 : NB;
-        const double *ib = inv + static_cast<long long>(b) * NB * NB;
-        GemmArgs g{rows, nb, nb, 1.0, 0.0, Y + k0, p, 1, ib, NB, 1, D + k0, p};
-        cudaError_t e = gemm(g, s);
-        if (e != cudaSuccess)
-            return e;
-        if (k0 > 0) {
-            GemmArgs u{rows, k0, nb, -1.0, 1.0, D + k0, p, 1, L + static_cast<long long>(k0) * p, p,
-                       1, Y, p};
             e = gemm(u, s);
             if (e != cudaSuccess)
                 return e;

@@ -629,12 +629,13 @@ template <typename R> class EngineT final : public Engine {
         const size_t mp = static_cast<size_t>(M_) * p, m1p = mp + p;
         const size_t nblk = (p + d64::NB - 1) / d64::NB;
         const size_t eps_n = q.perturbations ? mp : 0;
-        const size_t doubles = 3 * p + eps_n + mp + 2 * m1p + p * p + nblk * d64::NB * d64::NB +
-                               static_cast<size_t>(M_) * M_ + 1;
+        // ha (M rows) and d (M + 1 rows) are adjacent: one forward substitution covers both
+        const size_t doubles = 3 * p + eps_n + mp + m1p + (mp + m1p) + p * p +
+                               nblk * d64::NB * d64::NB + static_cast<size_t>(M_) * M_ + 1;
         enkf_.ensure(sizeof(double) * doubles + 64, "allocate EnKF workspace");
         double *ybuf = enkf_.as<double>(), *sdbuf = ybuf + p, *hmean = sdbuf + p,
                *eps_d = hmean + p, *ha = eps_d + eps_n, *d = ha + mp, *yw = d + m1p,
-               *P = yw + m1p, *inv = P + p * p, *W = inv + nblk * d64::NB * d64::NB,
+               *P = yw + mp + m1p, *inv = P + p * p, *W = inv + nblk * d64::NB * d64::NB,
                *nis_d = W + static_cast<size_t>(M_) * M_;
         int *info = reinterpret_cast<int *>(nis_d + 1);
         cuda_check(cudaMemcpyAsync(ybuf, q.values, sizeof(double) * p, cudaMemcpyHostToDevice,
@@ -660,10 +661,13 @@ template <typename R> class EngineT final : public Engine {
                    "launch innovation covariance");
         add_obs_variance<<<(pi + 127) / 128, 128, 0, stream_>>>(P, sdbuf, pi);
         cuda_check(d64::cholesky(P, pi, inv, info, stream_), "launch innovation Cholesky");
-        // Z = S^{-1} D for the M perturbed innovations and the mean innovation
-        cuda_check(d64::cholesky_solve_rows(P, pi, inv, d, yw, M_ + 1, stream_),
+        // L^{-1} applied to the anomalies HA, the M perturbed innovations and the mean
+        // innovation at once (rows of [HA; D], written to yw): with S = L L^T,
+        // W = (L^{-1} HA)^T-rows . (L^{-1} D)-rows / (M-1) and NIS = |L^{-1} dbar|^2 / p
+        cuda_check(d64::forward_rows(P, pi, inv, ha, yw, 2 * M_ + 1, stream_),
                    "launch innovation solve");
-        innovation_statistic<<<1, 256, 0, stream_>>>(ybuf, hmean, d + mp, pi, nis_d);
+        const double *yha = yw, *yd = yw + mp;
+        innovation_statistic<<<1, 256, 0, stream_>>>(yd + mp, pi, nis_d);
         cuda_check(cudaGetLastError(), "launch innovation statistic");
         double nis = 0;
         int host_info = 0;
@@ -676,8 +680,8 @@ template <typename R> class EngineT final : public Engine {
             raise(HZLB_ERUNTIME, "EnKF innovation covariance is not positive definite");
         if (q.nis_limit > 0 && !(nis <= q.nis_limit))
             return EnkfResult{nis, 0};
-        // W[a][m] = sum_o HA[a][o] Z[m][o] / (M-1)
-        cuda_check(d64::gemm(d64::GemmArgs{M_, M_, pi, 1.0 / (M_ - 1), 0.0, ha, pi, 1, d, 1, pi,
+        // W[a][m] = sum_o (L^{-1} HA)[a][o] (L^{-1} D)[m][o] / (M-1)
+        cuda_check(d64::gemm(d64::GemmArgs{M_, M_, pi, 1.0 / (M_ - 1), 0.0, yha, pi, 1, yd, 1, pi,
                                            W, M_},
                              stream_),
                    "launch ensemble weights");

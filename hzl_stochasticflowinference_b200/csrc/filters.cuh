@@ -118,14 +118,13 @@ __global__ void add_obs_variance(double *P, const double *sd, int p) {
     if (a < p)
         P[static_cast<size_t>(a) * p + a] += sd[a] * sd[a];
 }
-// Normalised innovation statistic dbar^T S^{-1} dbar / p with dbar = y - mean, given
-// z = S^{-1} dbar (one block).
-__global__ void innovation_statistic(const double *y, const double *mean, const double *z, int p,
-                                     double *out) {
+// Normalised innovation statistic dbar^T S^{-1} dbar / p = |L^{-1} dbar|^2 / p, given
+// w = L^{-1} dbar with S = L L^T (one block).
+__global__ void innovation_statistic(const double *w, int p, double *out) {
     __shared__ double part[32];
     double s = 0;
     for (int o = threadIdx.x; o < p; o += blockDim.x)
-        s += (y[o] - mean[o]) * z[o];
+        s += w[o] * w[o];
     for (int k = 16; k > 0; k >>= 1)
         s += __shfl_xor_sync(0xffffffffu, s, k);
     if ((threadIdx.x & 31) == 0)

@@ -178,25 +178,28 @@ __device__ __forceinline__ float tf32_round(float x) {
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
 }
-// Weight of real entry e of a compact member: sqrt(2) on the columns kx > 0.
+// Weight of real entry e of a compact member: sqrt(2) on the columns kx > 0, i.e. from
+// complex index ld on.
 __device__ __forceinline__ double column_weight(long long e, int ld) {
-    return (e >> 1) / ld > 0 ? kSqrt2 : 1.0;
+    return (e >> 1) >= ld ? kSqrt2 : 1.0;
 }
 // c = w (x - mean) for rows x D reals of the compact layout; FP64 copy (optional) and 3xTF32
-// split into hi / lo.
-__global__ void center_weight(const float *x, const float *mean, long long rows, long long D, int ld,
+// split into hi / lo.  Grid: x over the entries of a row, y over rows.
+__global__ void center_weight(const float *x, const float *mean, int rows, int D, int ld,
                               double *xd, float *hi, float *lo) {
-    const long long total = rows * D;
-    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long e = i % D;
-        const double c = column_weight(e, ld) * (static_cast<double>(x[i]) - static_cast<double>(mean[e]));
-        if (xd)
-            xd[i] = c;
-        const float f = static_cast<float>(c), h = tf32_round(f);
-        hi[i] = h;
-        lo[i] = f - h;
-    }
+    for (int row = blockIdx.y; row < rows; row += gridDim.y)
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < D; e += gridDim.x * blockDim.x) {
+            const long long i = static_cast<long long>(row) * D + e;
+            const double c = column_weight(e, ld) * (static_cast<double>(x[i]) - static_cast<double>(mean[e]));
+            if (xd)
+                xd[i] = c;
+            const float f = static_cast<float>(c), h = tf32_round(f);
+            hi[i] = h;
+            lo[i] = f - h;
+        }
+}
+dim3 center_grid(int rows, long long D) {
+    return dim3(static_cast<unsigned>((D + 255) / 256), static_cast<unsigned>(std::min(rows, 65535)));
 }
 __global__ void center_double(const double *x, const double *mean, long long rows, long long D,
                               double *out) {
@@ -214,9 +217,11 @@ __global__ void symmetric_to_double(const float *g, int m, double *out) {
     }
 }
 // From the weighted orthonormal modes U (r x D, FP64): the 3xTF32 split of U (projection),
-// the unweighted modes U / w as FP32 (r x D) and their split transposed, [e][j] (update).
+// the unweighted modes U / w as FP32 (r x D), and for the update the transposed unweighted
+// modes with the three split terms side by side along K: ut3[e] = (hi[0..r), lo[0..r),
+// hi[0..r)), so one product with K = 3r sums hi*hi + hi*lo + lo*hi.
 __global__ void mode_tables(const double *U, int r, long long D, int ld, float *uw_hi, float *uw_lo,
-                            float *modes, float *ut_hi, float *ut_lo) {
+                            float *modes, float *ut3) {
     const long long total = static_cast<long long>(r) * D;
     for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
@@ -226,8 +231,9 @@ __global__ void mode_tables(const double *U, int r, long long D, int ld, float *
         uw_lo[i] = f - h;
         const float u = static_cast<float>(U[i] / column_weight(e, ld)), uh = tf32_round(u);
         modes[i] = u;
-        ut_hi[e * r + j] = uh;
-        ut_lo[e * r + j] = u - uh;
+        ut3[e * 3 * r + j] = uh;
+        ut3[e * 3 * r + r + j] = u - uh;
+        ut3[e * 3 * r + 2 * r + j] = uh;
     }
 }
 // C[i][j] (leading dimension ldc) = sum over slices z of partial[z][i][j]
@@ -259,16 +265,20 @@ __global__ void add_to_members(float *x, const float *inc, int rows, long long D
          i += static_cast<long long>(gridDim.x) * blockDim.x)
         x[i] += inc[i % D];
 }
-// delta = y - x[:, :r] (x row stride ldx), less center[j] if given, split for 3xTF32.
+// delta = y - x[:, :r] (x row stride ldx), less center[j] if given, split for 3xTF32 into
+// d3[m] = (hi[0..r), hi[0..r), lo[0..r)) to pair with ut3 of mode_tables.
 __global__ void delta_split(const float *y, const float *x, long long ldx, int rows, int r,
-                            const float *center, float *hi, float *lo) {
+                            const float *center, float *d3) {
     const long long total = static_cast<long long>(rows) * r;
     for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const float d = y[i] - x[(i / r) * ldx + i % r] - (center ? center[i % r] : 0.0f);
+        const long long m = i / r;
+        const int j = static_cast<int>(i % r);
+        const float d = y[i] - x[m * ldx + j] - (center ? center[j] : 0.0f);
         const float h = tf32_round(d);
-        hi[i] = h;
-        lo[i] = d - h;
+        d3[m * 3 * r + j] = h;
+        d3[m * 3 * r + r + j] = h;
+        d3[m * 3 * r + 2 * r + j] = d - h;
     }
 }
 // Noise-mode amplitudes of a forecast window: for the four lowest modes (kx, ky) = (1,0),
@@ -412,8 +422,8 @@ class PodBasis {
         xd.ensure(sizeof(double) * m * D, "allocate centred snapshots");
         hl.ensure(sizeof(float) * 2 * m * D, "allocate snapshot split");
         float *hi = hl.as<float>(), *lo = hi + static_cast<long long>(m) * D;
-        center_weight<<<blocks_for(m * D), 256, 0, s>>>(snaps, mean_.as<float>(), m, D, LD,
-                                                         xd.as<double>(), hi, lo);
+        center_weight<<<center_grid(m, D), 256, 0, s>>>(snaps, mean_.as<float>(), m, static_cast<int>(D),
+                                                         LD, xd.as<double>(), hi, lo);
         cuda_check(cudaGetLastError(), "launch snapshot centring");
         // Gram matrix on the tensor cores: hi hi^T + hi lo^T + lo hi^T
         gram32.ensure(sizeof(float) * m * m, "allocate snapshot Gram");
@@ -508,10 +518,10 @@ class PodBasis {
         for (double v : norms)
             if (v < 1e-8)
                 raise(HZLB_ERUNTIME, "numerically degenerate POD mode");
-        tables_.ensure(sizeof(float) * 5 * r * D, "allocate mode tables");
+        tables_.ensure(sizeof(float) * 6 * r * D, "allocate mode tables");
         float *t = tables_.as<float>();
         mode_tables<<<blocks_for(r * D), 256, 0, s>>>(ud.as<double>(), r, D, LD, t, t + r * D,
-                                                       t + 2 * r * D, t + 3 * r * D, t + 4 * r * D);
+                                                       t + 2 * r * D, t + 3 * r * D);
         cuda_check(cudaGetLastError(), "launch mode tables");
         check_status(s);
     }
@@ -522,7 +532,8 @@ class PodBasis {
         const long long cd = static_cast<long long>(count) * D;
         work_.ensure(sizeof(float) * 2 * cd, "allocate projection workspace");
         float *hi = work_.as<float>(), *lo = hi + cd;
-        center_weight<<<blocks_for(cd), 256, 0, s>>>(x, mean_.as<float>(), count, D, LD, nullptr, hi, lo);
+        center_weight<<<center_grid(count, D), 256, 0, s>>>(x, mean_.as<float>(), count,
+                                                             static_cast<int>(D), LD, nullptr, hi, lo);
         cuda_check(cudaGetLastError(), "launch state centring");
         // split-K: each of the three products over K = D in chunks of kchunk
         const int eps = tc::SLAB / 4;
@@ -554,30 +565,27 @@ class PodBasis {
         sum_slices<<<blocks_for(slice), 256, 0, s>>>(partial_.as<float>(), 3 * splits, count, r, a, ldc);
         cuda_check(cudaGetLastError(), "launch split-K sum");
     }
-    // x[count][D] += delta[count][r] (unweighted) modes, delta given split as hi / lo
-    void update(float *x, int count, const float *d_hi, const float *d_lo, cudaStream_t s) {
+    // x[count][D] += delta[count][r] (unweighted) modes: one 3xTF32 product with the split
+    // terms side by side along K (d3 from delta_split, ut3 from mode_tables), so the ensemble
+    // state is read and written once
+    void update(float *x, int count, const float *d3, cudaStream_t s) {
         ensure_fitted();
-        const float *t = tables_.as<float>();
-        const float *ut_hi = t + 3 * r * D, *ut_lo = t + 4 * r * D;
-        const float *pa[3] = {d_hi, d_hi, d_lo}, *pb[3] = {ut_hi, ut_lo, ut_hi};
-        for (int i = 0; i < 3; ++i) {
-            tc::GemmArgs g{};
-            g.M = count;
-            g.N = static_cast<int>(D);
-            g.K = r;
-            g.A = pa[i];
-            g.lda = r;
-            g.a_kcontig = 1;
-            g.B = pb[i];
-            g.ldb = r;
-            g.b_kcontig = 1;
-            g.C = x;
-            g.ldc = D;
-            g.alpha = 1.0f;
-            g.beta = 1.0f;
-            g.status = status_ptr();
-            cuda_check(gemm(g, 4, s), "launch mode update");
-        }
+        tc::GemmArgs g{};
+        g.M = count;
+        g.N = static_cast<int>(D);
+        g.K = 3 * r;
+        g.A = d3;
+        g.lda = 3 * r;
+        g.a_kcontig = 1;
+        g.B = tables_.as<float>() + 3 * r * D;
+        g.ldb = 3 * r;
+        g.b_kcontig = 1;
+        g.C = x;
+        g.ldc = D;
+        g.alpha = 1.0f;
+        g.beta = 1.0f;
+        g.status = status_ptr();
+        cuda_check(gemm(g, 4, s), "launch mode update");
     }
     // One window of the learned forecast on an ensemble held by `e`: project, add the window's
     // noise amplitudes, run the network (which predicts the coefficients without the direct
@@ -594,9 +602,9 @@ class PodBasis {
         const int M = e.members();
         cudaStream_t s = static_cast<cudaStream_t>(e.stream());
         const int in = r + q;
-        io_.ensure(sizeof(float) * (static_cast<size_t>(M) * (in + 3 * r) + r), "allocate forecast buffers");
-        float *xin = io_.as<float>(), *y = xin + static_cast<size_t>(M) * in, *dhi = y + static_cast<size_t>(M) * r,
-              *dlo = dhi + static_cast<size_t>(M) * r, *dmean = dlo + static_cast<size_t>(M) * r;
+        io_.ensure(sizeof(float) * (static_cast<size_t>(M) * (in + 4 * r) + r), "allocate forecast buffers");
+        float *xin = io_.as<float>(), *y = xin + static_cast<size_t>(M) * in, *d3 = y + static_cast<size_t>(M) * r,
+              *dmean = d3 + static_cast<size_t>(M) * 3 * r;
         float *state = static_cast<float *>(e.state_device());
         project(state, M, xin, in, s);
         const double scale = cfg.noise_sigma > 0 ? cfg.noise_sigma * std::sqrt(dt) / kSqrt2 : 0.0;
@@ -608,9 +616,9 @@ class PodBasis {
         if (mean_increment)
             delta_mean<<<(r + 63) / 64, 64, 0, s>>>(y, xin, in, M, r, dmean);
         delta_split<<<blocks_for(static_cast<long long>(M) * r), 256, 0, s>>>(
-            y, xin, in, M, r, mean_increment ? dmean : nullptr, dhi, dlo);
+            y, xin, in, M, r, mean_increment ? dmean : nullptr, d3);
         cuda_check(cudaGetLastError(), "launch coefficient change");
-        update(state, M, dhi, dlo, s);
+        update(state, M, d3, s);
         if (mean_increment) {
             add_to_members<<<blocks_for(M * D), 256, 0, s>>>(state, mean_increment, M, D);
             cuda_check(cudaGetLastError(), "launch mean increment");

@@ -19,6 +19,10 @@ Legs:
   fp64         this path's FP64 variant at 256^2 (512 members), device-timed, for a like-for-like
                precision comparison with gpu_reference
 
+  filters      (1 GPU) the 128^2 filtering twin experiment: EnKF 512 members (inflation 1.05) and
+               bootstrap PF 2048 particles, 16x16 observations (sigma 0.1) every 50 steps, 40
+               cycles; analysis RMSE and wall-clock per cycle, beside the reference CPU filters'
+               forecast cost extrapolated from a measured single-thread member-step
   learned      (1 GPU) the learned-forecast EnKF twin experiment at 256^2: POD from 2000
                snapshots (r=64), the 72-512-512-64 BF16 MLP trained on 100,352 solver
                transitions of 20 steps, 1024-member EnKF observed on 32x32 points (sigma
@@ -151,6 +155,52 @@ def cpu_reference_sample(n: int, seconds_target: float = 15.0):
               f"steps on {threads} threads, {el:.1f} s, includes the reference's per-step "
               f"validate_step diagnostics")
     return value, threads, sample
+
+
+def cpu_filter_extrapolation(tc) -> dict:
+    """Per-cycle cost of the reference's filters at the config-2 size, extrapolated from a
+    measured single-thread member-step of its CPU solver at tc.n^2 (its filters advance the
+    members one after another on one thread, src/filter.cpp:38-126, 204-356; the analysis is
+    not included, so these are lower bounds)."""
+    from oracle.oracle import Reference, params6
+    ref = Reference()
+    p = params6(tc.nu, 0.1, 0.2, 0.5, 2, 3)
+    t0 = time.perf_counter()
+    ref.ensemble(tc.n, p, tc.dt, 20, 1, 1, SEED)
+    per_step = (time.perf_counter() - t0) / 20
+    return {"member_step_seconds": per_step,
+            "enkf_cycle_seconds": per_step * tc.enkf_members * tc.obs_every,
+            "pf_cycle_seconds": per_step * tc.particles * tc.obs_every,
+            "sample": f"hzl::ensemble on 1 thread, 1 member x 20 steps at {tc.n}^2, "
+                      f"extrapolated to the forecast of one cycle (analysis not included)"}
+
+
+def filter_experiment(cpu: bool) -> dict:
+    """The 128^2 filtering twin experiment (hzl_stochasticflowinference_b200.twin)."""
+    try:
+        from hzl_stochasticflowinference_b200 import twin as T
+        tc = T.FilterTwinConfig()
+        t0 = time.perf_counter()
+        res = T.run(tc)
+        keep = ("initial_rmse", "mean_rmse", "final_rmse", "seconds_per_cycle")
+        out = {"workload": f"{tc.n}^2 FP32 forecast, {len(T.observation_grid(tc)[0])} point "
+                           f"observations (sigma {tc.obs_sd}) every {tc.obs_every} steps of dt "
+                           f"{tc.dt}, {tc.cycles} cycles; EnKF {tc.enkf_members} members, "
+                           f"inflation {tc.inflation}; bootstrap PF {tc.particles} particles, "
+                           f"resampling when ESS < {tc.resample_fraction} x particles",
+               "seconds": time.perf_counter() - t0,
+               "enkf": {k: res["enkf"][k] for k in keep},
+               "pf": {k: res["pf"][k] for k in keep}}
+        out["pf"]["resampling_events"] = res["pf"]["resampling_events"]
+        out["pf"]["min_ess"] = min(res["pf"]["ess"])
+        if cpu:
+            try:
+                out["reference_cpu_extrapolated"] = cpu_filter_extrapolation(tc)
+            except Exception as exc:
+                out["reference_cpu_extrapolated"] = {"sample": f"unavailable: {exc}"}
+        return out
+    except Exception as exc:   # report, never lose the main line
+        return {"error": f"{type(exc).__name__}: {exc}"}
 
 
 def run_reference(args, rank, world):
@@ -447,13 +497,14 @@ def main():
                    "sample": f"unavailable: {exc}"}
 
     ens.close()
-    learned = gpu_ref = fp64 = None
+    learned = gpu_ref = fp64 = filters = None
     if rank == 0 and world == 1:
         fp64 = fp64_sample(hz, torch, N)
         if not args.no_cpu_baseline:
             gpu_ref = reference_gpu_sample(N)
         if not args.no_learned:
             learned = learned_experiment()
+            filters = filter_experiment(not args.no_cpu_baseline)
 
     if rank == 0:
         out = {
@@ -481,6 +532,7 @@ def main():
             "clocks": clocks.summary(),
             "status": status,
             "learned": learned,
+            "filters": filters,
         }
         print(json.dumps(out), flush=True)
     if pg:

@@ -137,6 +137,7 @@ def library() -> C.CDLL:
                                              C.POINTER(C.c_int)]),
         "hzlb_state_device": (C.c_int, [vp, C.POINTER(vp)]),
         "hzlb_ensemble_mean": (C.c_int, [vp, _dp]),
+        "hzlb_weighted_mean": (C.c_int, [vp, _dp, _dp]),
         "hzlb_grf_spectrum": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, _dp]),
         "hzlb_run_ensemble": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), C.c_double,
                                         C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_int,
@@ -410,6 +411,13 @@ class Ensemble:
     def mean_device(self, out) -> None:
         """Member mean of the compact state into out (CUDA tensor of the state's precision)."""
         _check(self._lib.hzlb_ensemble_mean_device(self._h, C.c_void_p(out.data_ptr())))
+
+    def weighted_mean_compact(self, weights) -> np.ndarray:
+        """sum_m w[m] x_m, compact layout, complex128."""
+        w = _f64(weights)
+        out = np.zeros(self.compact_size, np.complex128)
+        _check(self._lib.hzlb_weighted_mean(self._h, _p(w), out.view(np.float64).ctypes.data_as(_dp)))
+        return out
 
     def mean_compact(self) -> np.ndarray:
         """Ensemble mean, compact layout, complex128."""

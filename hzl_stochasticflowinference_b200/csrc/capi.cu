@@ -258,6 +258,13 @@ int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double
     });
     return outer != HZLB_OK ? outer : rc;
 }
+int hzlb_weighted_mean(hzlb_ensemble *h, const double *weights, double *mean) {
+    return guarded([&] {
+        need(weights, "weights");
+        need(mean, "mean");
+        engine(h).member_sum(weights, 0.0, mean);
+    });
+}
 int hzlb_ensemble_mean_device(hzlb_ensemble *h, void *mean) {
     return guarded([&] {
         need(mean, "mean");

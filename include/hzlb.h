@@ -177,6 +177,9 @@ HZLB_API int hzlb_state_device(hzlb_ensemble *h, void **state);
 /* Ensemble mean in the compact layout as interleaved doubles (hzlb_compact_size complex
  * entries), summed in member order as the reference's filters do (filter.cpp:238-243). */
 HZLB_API int hzlb_ensemble_mean(hzlb_ensemble *h, double *mean);
+/* Weighted member sum sum_m w[m] x_m in the compact layout as interleaved doubles, in member
+ * order (the bootstrap filter's weighted mean, filter.cpp:113-120); w: members doubles. */
+HZLB_API int hzlb_weighted_mean(hzlb_ensemble *h, const double *weights, double *mean);
 /* The member mean of the compact state into a device array of hzlb_compact_size complex
  * entries in the handle's precision (summed in FP64 over member slices). */
 HZLB_API int hzlb_ensemble_mean_device(hzlb_ensemble *h, void *mean);

@@ -23,6 +23,9 @@ Legs:
                bootstrap PF 2048 particles, 16x16 observations (sigma 0.1) every 50 steps, 40
                cycles; analysis RMSE and wall-clock per cycle, beside the reference CPU filters'
                forecast cost extrapolated from a measured single-thread member-step
+  mixed        (1 GPU) the uneven batch: 4096 x 64^2, 1024 x 128^2, 128 x 256^2, 8 x 512^2 FP32
+               members in one CUDA graph per batch of steps, 500 steps, serial schedule and the
+               autotuner's schedule
   learned      (1 GPU) the learned-forecast EnKF twin experiment at 256^2: POD from 2000
                snapshots (r=64), the 72-512-512-64 BF16 MLP trained on 100,352 solver
                transitions of 20 steps, 1024-member EnKF observed on 32x32 points (sigma
@@ -271,6 +274,20 @@ def fp64_sample(hz, torch, n: int, members: int = 512, steps: int = 10) -> dict:
             "steps": steps, "dtype": "f64"}
 
 
+def mixed_experiment() -> dict:
+    try:
+        from hzl_stochasticflowinference_b200 import batch
+        t0 = time.perf_counter()
+        res = batch.run()
+        res["seconds"] = time.perf_counter() - t0
+        peak, kind = peaks()
+        res["tuned"]["frac_of_hbm"] = res["tuned"]["algorithmic_gbs"] / peak
+        res["peak_kind"] = kind
+        return res
+    except Exception as exc:   # report, never lose the main line
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def learned_experiment() -> dict:
     """The learned-forecast EnKF twin experiment (hzl_stochasticflowinference_b200.learned) at
     its full size; wall-clock per cycle (forecast + analysis + fallback) with the GPU
@@ -497,7 +514,7 @@ def main():
                    "sample": f"unavailable: {exc}"}
 
     ens.close()
-    learned = gpu_ref = fp64 = filters = None
+    learned = gpu_ref = fp64 = filters = mixed = None
     if rank == 0 and world == 1:
         fp64 = fp64_sample(hz, torch, N)
         if not args.no_cpu_baseline:
@@ -505,6 +522,7 @@ def main():
         if not args.no_learned:
             learned = learned_experiment()
             filters = filter_experiment(not args.no_cpu_baseline)
+            mixed = mixed_experiment()
 
     if rank == 0:
         out = {
@@ -533,6 +551,7 @@ def main():
             "status": status,
             "learned": learned,
             "filters": filters,
+            "mixed": mixed,
         }
         print(json.dumps(out), flush=True)
     if pg:

@@ -176,6 +176,15 @@ def library() -> C.CDLL:
                                             C.c_uint64, C.c_int, vp, C.c_longlong, vp]),
         "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, vp]),
         "hzlb_ensemble_mean_device": (C.c_int, [vp, vp]),
+        "hzlb_mixed_create": (C.c_int, [C.POINTER(hzlb_config), C.c_int, C.POINTER(vp)]),
+        "hzlb_mixed_destroy": (None, [vp]),
+        "hzlb_mixed_group": (vp, [vp, C.c_int]),
+        "hzlb_mixed_step": (C.c_int, [vp, _dp, C.c_uint64]),
+        "hzlb_mixed_tune": (C.c_int, [vp, _dp, C.c_int, _dp]),
+        "hzlb_mixed_schedule": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int)]),
+        "hzlb_mixed_set_schedule": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int),
+                                              C.POINTER(C.c_int)]),
         "hzlb_add_window_noise": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
                                             C.c_uint64, C.c_int, vp, vp]),
     }
@@ -253,7 +262,22 @@ class Ensemble:
         _check(self._lib.hzlb_ensemble_create(C.byref(cfg), C.byref(self._h)))
         self.compact_size = int(self._lib.hzlb_compact_size(self._h))
 
+    @classmethod
+    def borrow(cls, handle: int, config: Config, owner) -> "Ensemble":
+        """Wraps a handle owned by another object (a mixed batch); never destroys it."""
+        e = cls.__new__(cls)
+        e.config = config
+        e.n, e.members = config.n, config.members
+        e._lib = library()
+        e._h = C.c_void_p(handle)
+        e._borrowed = owner
+        e.compact_size = int(e._lib.hzlb_compact_size(e._h))
+        return e
+
     def close(self):
+        if getattr(self, "_borrowed", None) is not None:
+            self._h = None
+            return
         if getattr(self, "_h", None):
             self._lib.hzlb_ensemble_destroy(self._h)
             self._h = None
@@ -745,3 +769,49 @@ def add_window_noise(config: Config, dt: float, first_step: int, steps: int, cou
     _torch_ready()
     _check(library().hzlb_add_window_noise(C.byref(cfg), dt, first_step, steps, count,
                                            C.c_void_p(ptr), None))
+
+
+class Mixed:
+    """Mixed-resolution ensembles advanced by one graph per batch of steps (hzlb_mixed_*)."""
+
+    def __init__(self, configs: list):
+        self._lib = library()
+        arr = (hzlb_config * len(configs))(*[c.to_c() for c in configs])
+        self._h = C.c_void_p()
+        _check(self._lib.hzlb_mixed_create(arr, len(configs), C.byref(self._h)))
+        self.configs = list(configs)
+        self.groups = [Ensemble.borrow(self._lib.hzlb_mixed_group(self._h, g), c, self)
+                       for g, c in enumerate(configs)]
+
+    def close(self):
+        for g in getattr(self, "groups", []):
+            g.close()
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.hzlb_mixed_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        self.close()
+
+    def step(self, dts, steps: int) -> None:
+        d = _f64(dts)
+        _check(self._lib.hzlb_mixed_step(self._h, _p(d), steps))
+
+    def tune(self, dts, repeats: int = 2) -> float:
+        d = _f64(dts)
+        ms = C.c_double()
+        _check(self._lib.hzlb_mixed_tune(self._h, _p(d), repeats, C.byref(ms)))
+        return ms.value
+
+    def schedule(self) -> dict:
+        k = len(self.configs)
+        serial = C.c_int()
+        col, row = (C.c_int * k)(), (C.c_int * k)()
+        _check(self._lib.hzlb_mixed_schedule(self._h, C.byref(serial), col, row))
+        return dict(serial=bool(serial.value), column_caps=list(col), row_caps=list(row))
+
+    def set_schedule(self, serial: bool, column_caps=None, row_caps=None) -> None:
+        k = len(self.configs)
+        col = (C.c_int * k)(*column_caps) if column_caps is not None else None
+        row = (C.c_int * k)(*row_caps) if row_caps is not None else None
+        _check(self._lib.hzlb_mixed_set_schedule(self._h, int(serial), col, row))

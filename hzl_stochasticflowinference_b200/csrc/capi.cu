@@ -6,9 +6,6 @@
 #include <string>
 #include <vector>
 
-struct hzlb_ensemble {
-    std::unique_ptr<hzlb::Engine> engine;
-};
 
 namespace {
 thread_local std::string last_error;

@@ -372,6 +372,33 @@ template <typename R> class EngineT final : public Engine {
         graphs_.push_back({dt, steps, exec});
         return exec;
     }
+    void prepare_steps(double dt) override {
+        const int largest = (n_ - 1) / 3;
+        if (!std::isfinite(dt) || dt <= 0 ||
+            dt * (2 * cfg_.nu * largest * largest + cfg_.alpha) > 2.5)
+            raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");
+        if (!w_valid_) {
+            launch_start();
+            cuda_check(cudaStreamSynchronize(stream_), "start pass");
+            w_valid_ = true;
+        }
+    }
+    void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap) override {
+        ColumnArgs<R> a = column_args(dt);
+        RowArgs<R> r = row_args();
+        for (int i = 0; i < steps; ++i)
+            for (int st = 1; st <= 4; ++st) {
+                r.cfl_scale = st == 1 ? dt * n_ / (2 * kPi) : 0.0;
+                cuda_check(launch_row<R>(n_, r, s, row_cap), "launch row pass");
+                a.stage = st;
+                cuda_check(launch_column<R>(n_, a, s, col_cap), "launch column pass");
+            }
+    }
+    void finish_steps(double dt, uint64_t nsteps) override {
+        w_valid_ = true;
+        time += dt * static_cast<double>(nsteps);
+        step_index += nsteps;
+    }
     void step(double dt, uint64_t nsteps) override {
         const int largest = (n_ - 1) / 3;
         if (!std::isfinite(dt) || dt <= 0 ||

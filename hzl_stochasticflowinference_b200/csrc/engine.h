@@ -103,6 +103,14 @@ class Engine {
     // caller may modify it until its next call on this ensemble
     virtual void *state_device() = 0;
     virtual const hzlb_config &config() const = 0;
+    // ---- stepping inside a caller's graph (mixed-resolution batches, mixed.cu) ------------
+    // validate dt and run the start pass if the velocity columns are stale (waits for it)
+    virtual void prepare_steps(double dt) = 0;
+    // enqueue `steps` RK4 steps on stream s, persistent grids capped at col_cap / row_cap
+    // blocks (0: every resident block); allowed during stream capture
+    virtual void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap) = 0;
+    // account for nsteps steps enqueued that way (clock, step counter, cached velocities)
+    virtual void finish_steps(double dt, uint64_t nsteps) = 0;
     // member mean of the compact state into `out` (device, compact_size entries, own precision)
     virtual void mean_device(void *out) = 0;
     virtual size_t compact_size() const = 0;
@@ -125,6 +133,14 @@ class Engine {
 };
 
 std::unique_ptr<Engine> make_engine(const hzlb_config &c);
+} // namespace hzlb
+
+// The opaque handle of include/hzlb.h.
+struct hzlb_ensemble {
+    std::unique_ptr<hzlb::Engine> engine;
+};
+
+namespace hzlb {
 
 // Tensor-core GEMM launcher (gemm.cu); dtype 2 = BF16 operands, 4 = FP32 read as TF32.
 namespace tc {

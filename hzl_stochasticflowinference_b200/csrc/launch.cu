@@ -51,15 +51,17 @@ template <typename R, int N> struct L {
     }
     static dim3 col_grid(int members) { return dim3(members, (G::C + G::LPB - 1) / G::LPB); }
     static dim3 row_grid(int members) { return dim3(members, N / G::TY); }
-    static cudaError_t column(const ColumnArgs<R> &a, cudaStream_t s) {
+    static cudaError_t column(const ColumnArgs<R> &a, cudaStream_t s, int cap) {
         const int items = a.members * G::NCG;
-        const int grid = std::min(items, resident(col_resident));
+        const int res = resident(col_resident);
+        const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
         column_kernel<R, N><<<grid, G::COL_THREADS, col_smem, s>>>(a, items);
         return cudaGetLastError();
     }
-    static cudaError_t row(const RowArgs<R> &a, cudaStream_t s) {
+    static cudaError_t row(const RowArgs<R> &a, cudaStream_t s, int cap) {
         const int items = a.members * (N / G::TY);
-        const int grid = std::min(items, resident(row_resident));
+        const int res = resident(row_resident);
+        const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
         row_kernel<R, N><<<grid, G::ROW_THREADS, row_smem, s>>>(a, items);
         return cudaGetLastError();
     }
@@ -104,10 +106,21 @@ template <typename R, int N> struct DoPrepare {
     static cudaError_t run() { return L<R, N>::prepare(); }
 };
 template <typename R, int N> struct DoColumn {
-    static cudaError_t run(const ColumnArgs<R> &a, cudaStream_t s) { return L<R, N>::column(a, s); }
+    static cudaError_t run(const ColumnArgs<R> &a, cudaStream_t s, int cap) {
+        return L<R, N>::column(a, s, cap);
+    }
 };
 template <typename R, int N> struct DoRow {
-    static cudaError_t run(const RowArgs<R> &a, cudaStream_t s) { return L<R, N>::row(a, s); }
+    static cudaError_t run(const RowArgs<R> &a, cudaStream_t s, int cap) {
+        return L<R, N>::row(a, s, cap);
+    }
+};
+template <typename R, int N> struct DoResident {
+    static cudaError_t run(int *c, int *r) {
+        *c = L<R, N>::resident(L<R, N>::col_resident);
+        *r = L<R, N>::resident(L<R, N>::row_resident);
+        return cudaSuccess;
+    }
 };
 template <typename R, int N> struct DoPhysical {
     static cudaError_t run(const cx<R> *f, long long st, cx<R> *c, R *p, const cx<R> *tw, int m,
@@ -130,11 +143,15 @@ template <typename R, int N> struct DoShape {
 } // namespace
 
 template <typename R> cudaError_t prepare_kernels(int n) { return dispatch<R, DoPrepare>(n); }
-template <typename R> cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s) {
-    return dispatch<R, DoColumn>(n, a, s);
+template <typename R>
+cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s, int cap) {
+    return dispatch<R, DoColumn>(n, a, s, cap);
 }
-template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s) {
-    return dispatch<R, DoRow>(n, a, s);
+template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s, int cap) {
+    return dispatch<R, DoRow>(n, a, s, cap);
+}
+template <typename R> cudaError_t resident_blocks(int n, int *column, int *row) {
+    return dispatch<R, DoResident>(n, column, row);
 }
 template <typename R>
 cudaError_t launch_physical(int n, const cx<R> *field, long long stride, cx<R> *cols, R *phys,
@@ -170,8 +187,9 @@ template <typename R> KernelShape kernel_shape(int n) {
 
 #define HZLB_INSTANTIATE(R)                                                                        \
     template cudaError_t prepare_kernels<R>(int);                                                  \
-    template cudaError_t launch_column<R>(int, const ColumnArgs<R> &, cudaStream_t);               \
-    template cudaError_t launch_row<R>(int, const RowArgs<R> &, cudaStream_t);                     \
+    template cudaError_t launch_column<R>(int, const ColumnArgs<R> &, cudaStream_t, int);          \
+    template cudaError_t launch_row<R>(int, const RowArgs<R> &, cudaStream_t, int);                \
+    template cudaError_t resident_blocks<R>(int, int *, int *);                                    \
     template cudaError_t launch_physical<R>(int, const cx<R> *, long long, cx<R> *, R *,          \
                                             const cx<R> *, int, cudaStream_t);                     \
     template cudaError_t launch_velocity_max<R>(int, const cx<R> *, unsigned long long *,         \

@@ -12,8 +12,12 @@ struct KernelShape {
 };
 
 template <typename R> cudaError_t prepare_kernels(int n);
-template <typename R> cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s);
-template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s);
+// cap > 0 limits the persistent grid to cap blocks (default: all resident blocks of the device)
+template <typename R>
+cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s, int cap = 0);
+template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s, int cap = 0);
+// resident blocks of the column and row kernels on the current device (after prepare_kernels)
+template <typename R> cudaError_t resident_blocks(int n, int *column, int *row);
 template <typename R>
 cudaError_t launch_physical(int n, const cx<R> *field, long long stride, cx<R> *cols, R *phys,
                             const cx<R> *tw, int members, cudaStream_t s);

@@ -1,0 +1,333 @@
+// Mixed-resolution ensembles advanced together: one CUDA graph per batch of steps holds every
+// resolution's RK4 launches.  In the concurrent schedule the graph forks one branch per
+// resolution (each branch on its own stream during capture, so the kernels of different
+// resolutions share the SMs), and joins at the end; in the serial schedule the resolutions
+// follow each other on one stream, each with the whole device.  The persistent row/column
+// kernels of each resolution take a cap on their grid (blocks), so concurrent branches can be
+// given shares of the GPU.
+//
+// The autotuner (hzlb_mixed_tune) measures the batch step time of candidate schedules on the
+// actual ensembles — the serial schedule, and the concurrent schedule with each resolution's
+// grid cap chosen by coordinate descent over fractions of its resident block count (largest
+// work first, two passes) — and keeps the fastest.  Each candidate is captured as a graph and
+// timed with CUDA events after a warm-up launch.  The ensembles' states and clocks are saved
+// on the device before tuning and restored after it, so tuning leaves them as they were.
+//
+// No counterpart in the reference (it steps one solver at a time).
+#include "engine.h"
+#include "launch.h"
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace hzlb {
+
+struct GroupCaps {
+    int col = 0, row = 0;   // 0: every resident block
+};
+
+class Mixed {
+  public:
+    Mixed(const hzlb_config *cfgs, int count) {
+        if (!cfgs || count < 1 || count > 16)
+            raise(HZLB_EINVAL, "mixed batch needs 1..16 ensemble configurations");
+        device_ = cfgs[0].device;
+        for (int g = 0; g < count; ++g) {
+            if (cfgs[g].device != device_)
+                raise(HZLB_EINVAL, "all resolutions of a mixed batch must be on one device");
+            auto h = std::make_unique<hzlb_ensemble>();
+            h->engine = make_engine(cfgs[g]);
+            groups_.push_back(std::move(h));
+        }
+        cuda_check(cudaSetDevice(device_), "select CUDA device");
+        cuda_check(cudaStreamCreateWithFlags(&main_, cudaStreamNonBlocking), "create stream");
+        branch_.resize(count);
+        join_.resize(count);
+        for (int g = 0; g < count; ++g) {
+            cuda_check(cudaStreamCreateWithFlags(&branch_[g], cudaStreamNonBlocking), "create stream");
+            cuda_check(cudaEventCreateWithFlags(&join_[g], cudaEventDisableTiming), "create event");
+        }
+        cuda_check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "create event");
+        caps_.assign(count, GroupCaps{});
+        resident_.resize(count);
+        for (int g = 0; g < count; ++g) {
+            const hzlb_config &c = cfgs[g];
+            cudaError_t e = c.precision == 4
+                                ? resident_blocks<float>(c.n, &resident_[g].col, &resident_[g].row)
+                                : resident_blocks<double>(c.n, &resident_[g].col, &resident_[g].row);
+            cuda_check(e, "query resident blocks");
+        }
+    }
+    ~Mixed() {
+        drop();
+        for (auto s : branch_)
+            if (s)
+                cudaStreamDestroy(s);
+        for (auto e : join_)
+            if (e)
+                cudaEventDestroy(e);
+        if (fork_)
+            cudaEventDestroy(fork_);
+        if (main_)
+            cudaStreamDestroy(main_);
+    }
+    int count() const { return static_cast<int>(groups_.size()); }
+    hzlb_ensemble *group(int g) { return g >= 0 && g < count() ? groups_[g].get() : nullptr; }
+
+    void step(const double *dt, uint64_t nsteps) {
+        check_dt(dt);
+        for (int g = 0; g < count(); ++g)
+            groups_[g]->engine->prepare_steps(dt[g]);
+        constexpr int kBatch = 8;
+        uint64_t left = nsteps;
+        while (left >= kBatch) {
+            cuda_check(cudaGraphLaunch(graph_for(dt, kBatch), main_), "launch mixed graph");
+            left -= kBatch;
+        }
+        if (left)
+            cuda_check(cudaGraphLaunch(graph_for(dt, static_cast<int>(left)), main_),
+                       "launch mixed graph");
+        cuda_check(cudaStreamSynchronize(main_), "mixed step");
+        for (int g = 0; g < count(); ++g)
+            groups_[g]->engine->finish_steps(dt[g], nsteps);
+    }
+
+    // Returns the best step time (ms per step); the chosen schedule stays in effect.
+    double tune(const double *dt, int repeats) {
+        check_dt(dt);
+        repeats = std::max(1, repeats);
+        // save every group's state and clock (restored below)
+        std::vector<DeviceBuffer> saved(count());
+        std::vector<std::pair<double, uint64_t>> clocks(count());
+        for (int g = 0; g < count(); ++g) {
+            Engine &e = *groups_[g]->engine;
+            const hzlb_config &c = e.config();
+            saved[g].ensure(e.compact_size() * 2 * c.precision * static_cast<size_t>(e.members()),
+                            "allocate tuning snapshot");
+            e.get_state_compact(saved[g].ptr, 0, e.members());
+            clocks[g] = {e.time, e.step_index};
+        }
+        for (int g = 0; g < count(); ++g)
+            groups_[g]->engine->prepare_steps(dt[g]);
+        // serial schedule
+        set_schedule(true, std::vector<GroupCaps>(count()));
+        const double serial = measure(dt, repeats);
+        // concurrent schedule: coordinate descent over grid-cap fractions
+        std::vector<GroupCaps> best(count());
+        set_schedule(false, best);
+        double best_ms = measure(dt, repeats);
+        std::vector<int> order(count());
+        for (int g = 0; g < count(); ++g)
+            order[g] = g;
+        std::sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+        const double fracs[] = {1.0, 0.75, 0.5, 0.25, 0.125};
+        for (int pass = 0; pass < 2; ++pass)
+            for (int g : order)
+                for (double f : fracs) {
+                    std::vector<GroupCaps> trial = best;
+                    trial[g].col = std::max(1, static_cast<int>(std::lround(resident_[g].col * f)));
+                    trial[g].row = std::max(1, static_cast<int>(std::lround(resident_[g].row * f)));
+                    set_schedule(false, trial);
+                    const double ms = measure(dt, repeats);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = trial;
+                    }
+                }
+        if (serial <= best_ms) {
+            set_schedule(true, std::vector<GroupCaps>(count()));
+            best_ms = serial;
+        } else {
+            set_schedule(false, best);
+        }
+        tuned_serial_ms_ = serial;
+        for (int g = 0; g < count(); ++g) {
+            Engine &e = *groups_[g]->engine;
+            e.set_state_compact(saved[g].ptr, 0, e.members());
+            e.set_time(clocks[g].first, clocks[g].second);
+            e.synchronize();
+            e.status();   // clears status bits raised while tuning
+        }
+        return best_ms;
+    }
+    void schedule(int *serial, int *col_caps, int *row_caps) const {
+        if (serial)
+            *serial = serial_ ? 1 : 0;
+        for (int g = 0; g < count(); ++g) {
+            if (col_caps)
+                col_caps[g] = caps_[g].col ? caps_[g].col : resident_[g].col;
+            if (row_caps)
+                row_caps[g] = caps_[g].row ? caps_[g].row : resident_[g].row;
+        }
+    }
+    void set_schedule(bool serial, const std::vector<GroupCaps> &caps) {
+        serial_ = serial;
+        caps_ = caps;
+        drop();
+    }
+
+  private:
+    struct Graph {
+        std::vector<double> dt;
+        int steps;
+        cudaGraphExec_t exec;
+    };
+    void check_dt(const double *dt) const {
+        if (!dt)
+            raise(HZLB_EINVAL, "null time steps");
+        for (int g = 0; g < count(); ++g)
+            if (!std::isfinite(dt[g]) || dt[g] <= 0)
+                raise(HZLB_EINVAL, "time steps must be positive and finite");
+    }
+    // bytes moved per step by a resolution (members x compact size), for the tuning order
+    double work(int g) const {
+        const hzlb_config &c = groups_[g]->engine->config();
+        const int K = (c.n - 1) / 3;
+        return static_cast<double>(c.members) * c.n * (K + 1) * c.precision;
+    }
+    void drop() {
+        for (auto &g : graphs_)
+            if (g.exec)
+                cudaGraphExecDestroy(g.exec);
+        graphs_.clear();
+    }
+    cudaGraphExec_t graph_for(const double *dt, int steps) {
+        for (auto &g : graphs_)
+            if (g.steps == steps && std::equal(g.dt.begin(), g.dt.end(), dt))
+                return g.exec;
+        // graphs are kept for the current time steps only (an adaptive caller changes them)
+        if (!graphs_.empty() && !std::equal(graphs_.front().dt.begin(), graphs_.front().dt.end(), dt))
+            drop();
+        cudaGraph_t graph = nullptr;
+        cuda_check(cudaStreamBeginCapture(main_, cudaStreamCaptureModeThreadLocal),
+                   "begin mixed capture");
+        try {
+            if (serial_) {
+                for (int g = 0; g < count(); ++g)
+                    groups_[g]->engine->enqueue_steps_on(dt[g], steps, main_, 0, 0);
+            } else {
+                cuda_check(cudaEventRecord(fork_, main_), "fork");
+                for (int g = 0; g < count(); ++g) {
+                    cuda_check(cudaStreamWaitEvent(branch_[g], fork_, 0), "branch wait");
+                    groups_[g]->engine->enqueue_steps_on(dt[g], steps, branch_[g], caps_[g].col,
+                                                         caps_[g].row);
+                    cuda_check(cudaEventRecord(join_[g], branch_[g]), "join record");
+                    cuda_check(cudaStreamWaitEvent(main_, join_[g], 0), "join wait");
+                }
+            }
+        } catch (...) {
+            cudaStreamEndCapture(main_, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            throw;
+        }
+        cuda_check(cudaStreamEndCapture(main_, &graph), "end mixed capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "instantiate mixed graph");
+        graphs_.push_back({std::vector<double>(dt, dt + count()), steps, exec});
+        return exec;
+    }
+    double measure(const double *dt, int repeats) {
+        constexpr int kSteps = 8;
+        cudaGraphExec_t exec = graph_for(dt, kSteps);
+        cuda_check(cudaGraphLaunch(exec, main_), "warm-up mixed graph");
+        cudaEvent_t a, b;
+        cuda_check(cudaEventCreate(&a), "create event");
+        cuda_check(cudaEventCreate(&b), "create event");
+        cuda_check(cudaEventRecord(a, main_), "record");
+        for (int i = 0; i < repeats; ++i)
+            cuda_check(cudaGraphLaunch(exec, main_), "launch mixed graph");
+        cuda_check(cudaEventRecord(b, main_), "record");
+        cuda_check(cudaEventSynchronize(b), "time mixed graph");
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        for (int g = 0; g < count(); ++g)
+            groups_[g]->engine->finish_steps(dt[g], static_cast<uint64_t>(kSteps) * (repeats + 1));
+        return ms / (static_cast<double>(repeats) * kSteps);
+    }
+
+    int device_ = 0;
+    std::vector<std::unique_ptr<hzlb_ensemble>> groups_;
+    cudaStream_t main_ = nullptr;
+    std::vector<cudaStream_t> branch_;
+    std::vector<cudaEvent_t> join_;
+    cudaEvent_t fork_ = nullptr;
+    std::vector<GroupCaps> caps_, resident_;
+    bool serial_ = false;
+    double tuned_serial_ms_ = 0;
+    std::vector<Graph> graphs_;
+};
+
+} // namespace hzlb
+
+struct hzlb_mixed {
+    std::unique_ptr<hzlb::Mixed> mixed;
+};
+
+namespace {
+template <class F> int guarded_mixed(F &&f) {
+    try {
+        f();
+        return HZLB_OK;
+    } catch (const hzlb::Error &e) {
+        hzlb::set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception &e) {
+        hzlb::set_last_error(e.what());
+        return HZLB_ERUNTIME;
+    }
+}
+hzlb::Mixed &mixed(hzlb_mixed *h) {
+    if (!h || !h->mixed)
+        hzlb::raise(HZLB_EINVAL, "null mixed handle");
+    return *h->mixed;
+}
+} // namespace
+
+extern "C" {
+HZLB_API int hzlb_mixed_create(const hzlb_config *configs, int count, hzlb_mixed **out) {
+    return guarded_mixed([&] {
+        if (!out)
+            hzlb::raise(HZLB_EINVAL, "null output");
+        auto h = std::make_unique<hzlb_mixed>();
+        h->mixed = std::make_unique<hzlb::Mixed>(configs, count);
+        *out = h.release();
+    });
+}
+HZLB_API void hzlb_mixed_destroy(hzlb_mixed *h) { delete h; }
+HZLB_API hzlb_ensemble *hzlb_mixed_group(hzlb_mixed *h, int group) {
+    return h && h->mixed ? h->mixed->group(group) : nullptr;
+}
+HZLB_API int hzlb_mixed_step(hzlb_mixed *h, const double *dt, uint64_t nsteps) {
+    return guarded_mixed([&] { mixed(h).step(dt, nsteps); });
+}
+HZLB_API int hzlb_mixed_tune(hzlb_mixed *h, const double *dt, int repeats, double *ms_per_step) {
+    return guarded_mixed([&] {
+        const double ms = mixed(h).tune(dt, repeats);
+        if (ms_per_step)
+            *ms_per_step = ms;
+    });
+}
+HZLB_API int hzlb_mixed_schedule(hzlb_mixed *h, int *serial, int *col_caps, int *row_caps) {
+    return guarded_mixed([&] { mixed(h).schedule(serial, col_caps, row_caps); });
+}
+HZLB_API int hzlb_mixed_set_schedule(hzlb_mixed *h, int serial, const int *col_caps,
+                                     const int *row_caps) {
+    return guarded_mixed([&] {
+        auto &m = mixed(h);
+        std::vector<hzlb::GroupCaps> caps(m.count());
+        for (int g = 0; g < m.count(); ++g) {
+            caps[g].col = col_caps ? std::max(0, col_caps[g]) : 0;
+            caps[g].row = row_caps ? std::max(0, row_caps[g]) : 0;
+        }
+        m.set_schedule(serial != 0, caps);
+    });
+}
+} // extern "C"

@@ -368,6 +368,28 @@ HZLB_API int hzlb_add_window_noise(const hzlb_config *config, double dt, uint64_
 HZLB_API int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
                                    uint64_t steps, const void *mean_increment);
 
+/* ---- mixed-resolution batches (no counterpart in the reference) -----------------------
+ * Ensembles of different grid sizes (and precisions) on one device advanced together: one CUDA
+ * graph per batch of steps holds every resolution's launches, either as concurrent branches
+ * (each resolution's persistent kernels capped to a share of the GPU) or one after another.
+ * hzlb_mixed_group returns the handle of resolution `group` (owned by the batch: set states,
+ * forcing, read diagnostics through it; do not destroy it).  dt: one time step per group. */
+typedef struct hzlb_mixed hzlb_mixed;
+HZLB_API int hzlb_mixed_create(const hzlb_config *configs, int count, hzlb_mixed **out);
+HZLB_API void hzlb_mixed_destroy(hzlb_mixed *h);
+HZLB_API hzlb_ensemble *hzlb_mixed_group(hzlb_mixed *h, int group);
+HZLB_API int hzlb_mixed_step(hzlb_mixed *h, const double *dt, uint64_t nsteps);
+/* Autotuner: times the serial schedule and the concurrent one with each group's grid cap
+ * chosen by coordinate descent over fractions of its resident blocks (`repeats` graph
+ * launches of 8 steps per candidate) and keeps the fastest; *ms_per_step = its step time.
+ * The ensembles' states, clocks and status are restored afterwards. */
+HZLB_API int hzlb_mixed_tune(hzlb_mixed *h, const double *dt, int repeats, double *ms_per_step);
+/* The schedule in effect: serial flag and per-group grid caps (blocks) of the column and row
+ * kernels; set_schedule overrides it (caps 0 or NULL: every resident block). */
+HZLB_API int hzlb_mixed_schedule(hzlb_mixed *h, int *serial, int *col_caps, int *row_caps);
+HZLB_API int hzlb_mixed_set_schedule(hzlb_mixed *h, int serial, const int *col_caps,
+                                     const int *row_caps);
+
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */
 /* Gaussian random vorticity spectrum, E(k) ~ k^4 exp(-(k/6)^2), unit enstrophy, retained modes

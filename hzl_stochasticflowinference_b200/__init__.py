@@ -137,6 +137,8 @@ def library() -> C.CDLL:
                                              C.POINTER(C.c_int)]),
         "hzlb_state_device": (C.c_int, [vp, C.POINTER(vp)]),
         "hzlb_ensemble_mean": (C.c_int, [vp, _dp]),
+        "hzlb_enable_ou": (C.c_int, [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
+        "hzlb_get_forcing_compact": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
         "hzlb_weighted_mean": (C.c_int, [vp, _dp, _dp]),
         "hzlb_grf_spectrum": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, _dp]),
         "hzlb_run_ensemble": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), C.c_double,
@@ -435,6 +437,20 @@ class Ensemble:
     def mean_device(self, out) -> None:
         """Member mean of the compact state into out (CUDA tensor of the state's precision)."""
         _check(self._lib.hzlb_ensemble_mean_device(self._h, C.c_void_p(out.data_ptr())))
+
+    def enable_ou(self, sigma: float, tau: float, kmin: int, kmax: int, initialize: bool = True):
+        """Device OU shell forcing (hzlb_enable_ou)."""
+        _check(self._lib.hzlb_enable_ou(self._h, sigma, tau, kmin, kmax, int(initialize)))
+
+    def forcing_compact(self, first: int = 0, count: int | None = None) -> np.ndarray:
+        """Per-member forcing, compact forcing layout, complex128 [count][cols * (2K+1)]."""
+        count = self.members - first if count is None else count
+        k = retained_k(self.n)
+        cols = min(self.config.forcing_kmax + 1, k + 1)
+        out = np.zeros((count, cols * (2 * k + 1)), np.complex128)
+        _check(self._lib.hzlb_get_forcing_compact(self._h, out.view(np.float64).ctypes.data_as(_dp),
+                                                  first, count))
+        return out
 
     def weighted_mean_compact(self, weights) -> np.ndarray:
         """sum_m w[m] x_m, compact layout, complex128."""

@@ -275,6 +275,16 @@ int hzlb_ensemble_mean(hzlb_ensemble *h, double *mean) {
         e.member_sum(nullptr, static_cast<double>(e.members()), mean);
     });
 }
+int hzlb_enable_ou(hzlb_ensemble *h, double sigma, double tau, int kmin, int kmax,
+                   int initialize) {
+    return guarded([&] { engine(h).enable_ou(sigma, tau, kmin, kmax, initialize != 0); });
+}
+int hzlb_get_forcing_compact(hzlb_ensemble *h, double *out, int first, int count) {
+    return guarded([&] {
+        need(out, "out");
+        engine(h).get_forcing_compact(out, first, count);
+    });
+}
 int hzlb_state_device(hzlb_ensemble *h, void **state) {
     return guarded([&] {
         need(state, "state");

@@ -2,6 +2,7 @@
 #include "engine.h"
 #include "dense64.cuh"
 #include "filters.cuh"
+#include "ou.cuh"
 #include "umma_gemm.cuh"
 
 #include <algorithm>
@@ -332,14 +333,53 @@ template <typename R> class EngineT final : public Engine {
     }
     // The eight launches of one RK4 step; the final column pass also emits the derivative
     // columns of the new state, so consecutive steps chain without a separate start pass.
-    void enqueue_step(double dt) {
-        ColumnArgs<R> a = column_args(dt);
-        RowArgs<R> r = row_args();
-        for (int s = 1; s <= 4; ++s) {
-            r.cfl_scale = s == 1 ? dt * n_ / (2 * kPi) : 0.0;
-            cuda_check(launch_row<R>(n_, r, stream_), "launch row pass");
-            a.stage = s;
-            cuda_check(launch_column<R>(n_, a, stream_), "launch column pass");
+    void enqueue_step(double dt) { enqueue_steps_on(dt, 1, stream_, 0, 0); }
+    // the OU half-step transition (ou.cuh) before (half 0) or after (half 1) a step's stages
+    void enqueue_ou(double dt, int half, cudaStream_t s) {
+        const double h = dt / 2;
+        const double decay = std::exp(-h / ou_tau_);
+        const double scale = ou_sigma_ * std::sqrt(-ou_tau_ * std::expm1(-2 * h / ou_tau_) / 4);
+        ou_transition<R><<<M_, 64, 0, s>>>(forcing_.as<cx<R>>(), fcols_, LD_, K_, ou_kmin_ * ou_kmin_,
+                                           ou_kmax_, decay, scale, cfg_.seed, cfg_.member_base,
+                                           ctl_.as<StepControl>(), half, 0);
+        cuda_check(cudaGetLastError(), "launch OU transition");
+    }
+    void enable_ou(double sigma, double tau, int kmin, int kmax, bool initialize) override {
+        if (!cfg_.forcing_per_member || fcount_ == 0)
+            raise(HZLB_EINVAL, "device OU forcing needs per-member forcing storage");
+        if (!std::isfinite(sigma) || sigma < 0 || !std::isfinite(tau) || tau <= 0 || kmin < 1 ||
+            kmax < kmin || 3 * kmax >= n_)
+            raise(HZLB_EINVAL, "invalid OU forcing parameters");
+        if (kmax >= fcols_)
+            raise(HZLB_EINVAL, "forcing storage must cover the OU shell (forcing_kmax >= kmax)");
+        ou_ = true;
+        ou_sigma_ = sigma;
+        ou_tau_ = tau;
+        ou_kmin_ = kmin;
+        ou_kmax_ = kmax;
+        drop_graphs();
+        if (initialize) {
+            ou_transition<R><<<M_, 64, 0, stream_>>>(forcing_.as<cx<R>>(), fcols_, LD_, K_, kmin * kmin,
+                                                     kmax, 0.0, sigma * std::sqrt(tau / 4), cfg_.seed,
+                                                     cfg_.member_base, ctl_.as<StepControl>(), 0, 1);
+            cuda_check(cudaGetLastError(), "launch OU initialisation");
+            cuda_check(cudaStreamSynchronize(stream_), "OU initialisation");
+        }
+    }
+    void get_forcing_compact(double *out, int first, int count) override {
+        if (fcount_ == 0)
+            raise(HZLB_EINVAL, "this ensemble holds no forcing");
+        if (first < 0 || count < 0 || first + count > fcount_)
+            raise(HZLB_EINVAL, "forcing range out of bounds");
+        const size_t block = static_cast<size_t>(fcols_) * LD_;
+        std::vector<cx<R>> tmp(block * count);
+        cuda_check(cudaMemcpyAsync(tmp.data(), forcing_.as<cx<R>>() + first * block,
+                                   sizeof(cx<R>) * tmp.size(), cudaMemcpyDeviceToHost, stream_),
+                   "download forcing");
+        cuda_check(cudaStreamSynchronize(stream_), "download forcing");
+        for (size_t i = 0; i < tmp.size(); ++i) {
+            out[2 * i] = static_cast<double>(tmp[i].x);
+            out[2 * i + 1] = static_cast<double>(tmp[i].y);
         }
     }
     void drop_graphs() {
@@ -386,13 +426,18 @@ template <typename R> class EngineT final : public Engine {
     void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap) override {
         ColumnArgs<R> a = column_args(dt);
         RowArgs<R> r = row_args();
-        for (int i = 0; i < steps; ++i)
+        for (int i = 0; i < steps; ++i) {
+            if (ou_)
+                enqueue_ou(dt, 0, s);
             for (int st = 1; st <= 4; ++st) {
                 r.cfl_scale = st == 1 ? dt * n_ / (2 * kPi) : 0.0;
                 cuda_check(launch_row<R>(n_, r, s, row_cap), "launch row pass");
                 a.stage = st;
                 cuda_check(launch_column<R>(n_, a, s, col_cap), "launch column pass");
             }
+            if (ou_)
+                enqueue_ou(dt, 1, s);
+        }
     }
     void finish_steps(double dt, uint64_t nsteps) override {
         w_valid_ = true;
@@ -426,6 +471,9 @@ template <typename R> class EngineT final : public Engine {
             dt * (2 * cfg_.nu * largest * largest + cfg_.alpha) > 2.5)
             raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");
         *row_ms = *col_ms = 0;
+        if (ou_)
+            raise(HZLB_EINVAL, "profiled stepping times the spectral kernels only; it does not "
+                               "advance device OU forcing");
         if (nsteps == 0)
             return;
         if (!w_valid_)
@@ -778,6 +826,9 @@ template <typename R> class EngineT final : public Engine {
     };
     hzlb_config cfg_;
     int n_ = 0, M_ = 0, K_ = 0, C_ = 0, LD_ = 0, fcols_ = 0, fcount_ = 0;
+    bool ou_ = false;
+    double ou_sigma_ = 0, ou_tau_ = 1;
+    int ou_kmin_ = 0, ou_kmax_ = 0;
     size_t compact_ = 0;
     cudaStream_t stream_ = nullptr;
     DeviceBuffer omega_, ystage_, acc_, w_, nl_, forcing_, ctl_, tw_, phys_, scratch_d_, vbits_,

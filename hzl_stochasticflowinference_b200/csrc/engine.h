@@ -103,6 +103,9 @@ class Engine {
     // caller may modify it until its next call on this ensemble
     virtual void *state_device() = 0;
     virtual const hzlb_config &config() const = 0;
+    // OU shell forcing on the device (ou.cuh): per-member forcing, transitions inside the step
+    virtual void enable_ou(double sigma, double tau, int kmin, int kmax, bool initialize) = 0;
+    virtual void get_forcing_compact(double *out, int first, int count) = 0;
     // ---- stepping inside a caller's graph (mixed-resolution batches, mixed.cu) ------------
     // validate dt and run the start pass if the velocity columns are stale (waits for it)
     virtual void prepare_steps(double dt) = 0;

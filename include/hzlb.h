@@ -101,6 +101,20 @@ HZLB_API size_t hzlb_compact_size(const hzlb_ensemble *h); /* complex entries pe
  * columns |kx| <= forcing_kmax (HZLB_EINVAL otherwise). */
 HZLB_API int hzlb_set_forcing(hzlb_ensemble *h, const double *spectra, int first, int count);
 
+/* Ornstein-Uhlenbeck shell forcing on the device (the reference's ShellForcing,
+ * solver.cpp:67-119, with Philox draws instead of its host mt19937_64 streams: parity is
+ * statistical).  Needs forcing_per_member = 1 and forcing_kmax >= kmax.  Every later step is
+ * the reference's midpoint scheme: a transition of dt/2, the RK4 stages with that forcing, a
+ * transition of dt/2; the modes kmin^2 <= |k|^2 <= kmax^2 of the forcing are owned by the
+ * process (others keep what hzlb_set_forcing put there).  initialize != 0 draws the stationary
+ * start sigma sqrt(tau/4) (xi1 + i xi2) (initialize_ou, solver.cpp:84-92).  No counterpart
+ * entry point in the reference. */
+HZLB_API int hzlb_enable_ou(hzlb_ensemble *h, double sigma, double tau, int kmin, int kmax,
+                            int initialize);
+/* Forcing of members [first, first+count) in the compact forcing layout (forcing_kmax + 1
+ * columns of 2K+1 entries) as interleaved doubles. */
+HZLB_API int hzlb_get_forcing_compact(hzlb_ensemble *h, double *out, int first, int count);
+
 /* Advance every member by nsteps RK4 steps of size dt (asynchronous on the handle's stream).
  * HZLB_EINVAL for a nonpositive/nonfinite dt or dt * (2 nu K^2 + alpha) > 2.5
  * (cuda_solver.cu:205-208). */

@@ -63,7 +63,7 @@ METRIC = "ensemble member-steps/s at 256^2"
 # DRAM bytes (read + write) per member per launch, from one ncu capture of 256 members at
 # 256^2 FP32 (profiles/row_kernel_256sq_fp32.md, profiles/column_kernel_256sq_fp32.md); the
 # traffic grows in proportion to the members processed, so a full launch is this x members.
-NCU_TRAFFIC_PER_MEMBER = {"row_kernel": 527182.0, "column_kernel": 846284.0}
+NCU_TRAFFIC_PER_MEMBER = {"row_kernel": 516570.0, "column_kernel": 854213.0}
 
 
 def peaks():

@@ -137,6 +137,12 @@ def library() -> C.CDLL:
                                              C.POINTER(C.c_int)]),
         "hzlb_state_device": (C.c_int, [vp, C.POINTER(vp)]),
         "hzlb_ensemble_mean": (C.c_int, [vp, _dp]),
+        "hzlb_galerkin_create": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), _dp, _dp,
+                                           C.c_size_t, C.c_int, C.POINTER(vp)]),
+        "hzlb_galerkin_destroy": (None, [vp]),
+        "hzlb_galerkin_coefficients": (C.c_int, [vp, _dp, _dp, _dp]),
+        "hzlb_galerkin_rhs": (C.c_int, [vp, _dp, C.c_size_t, _dp]),
+        "hzlb_galerkin_step": (C.c_int, [vp, _dp, C.c_size_t, C.c_double, C.c_uint64]),
         "hzlb_enable_ou": (C.c_int, [vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
         "hzlb_get_forcing_compact": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
         "hzlb_weighted_mean": (C.c_int, [vp, _dp, _dp]),
@@ -831,3 +837,40 @@ class Mixed:
         col = (C.c_int * k)(*column_caps) if column_caps is not None else None
         row = (C.c_int * k)(*row_caps) if row_caps is not None else None
         _check(self._lib.hzlb_mixed_set_schedule(self._h, int(serial), col, row))
+
+
+class GalerkinModel:
+    """hzl::GalerkinModel (src/reduced.cpp:137-209) with its drifts evaluated on the GPU."""
+
+    def __init__(self, n: int, p: "Parameters", mean, modes, device: int = 0):
+        self._lib = library()
+        m = _c128(mean).reshape(n * n)
+        u = _c128(modes).reshape(-1, n * n)
+        self.rank = len(u)
+        self._h = C.c_void_p()
+        pc = p.to_c()
+        _check(self._lib.hzlb_galerkin_create(n, C.byref(pc), m.view(np.float64).ctypes.data_as(_dp),
+                                              u.view(np.float64).ctypes.data_as(_dp), self.rank,
+                                              device, C.byref(self._h)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.hzlb_galerkin_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def coefficients(self):
+        r = self.rank
+        c, A, Q = np.zeros(r), np.zeros((r, r)), np.zeros((r, r, r))
+        _check(self._lib.hzlb_galerkin_coefficients(self._h, _p(c), _p(A), _p(Q)))
+        return c, A, Q
+
+    def rhs(self, a) -> np.ndarray:
+        a = _f64(a).reshape(-1, self.rank)
+        out = np.zeros_like(a)
+        _check(self._lib.hzlb_galerkin_rhs(self._h, _p(a), len(a), _p(out)))
+        return out
+
+    def step(self, a, dt: float, steps: int = 1) -> np.ndarray:
+        a = _f64(a).reshape(-1, self.rank).copy()
+        _check(self._lib.hzlb_galerkin_step(self._h, _p(a), len(a), dt, steps))
+        return a

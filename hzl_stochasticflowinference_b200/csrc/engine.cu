@@ -366,6 +366,22 @@ template <typename R> class EngineT final : public Engine {
             cuda_check(cudaStreamSynchronize(stream_), "OU initialisation");
         }
     }
+    void drift(void *out) override {
+        if (!w_valid_)
+            launch_start();
+        w_valid_ = true;   // the stage-1 column pass below does not emit velocities
+        RowArgs<R> r = row_args();
+        r.cfl_scale = 0.0;
+        cuda_check(launch_row<R>(n_, r, stream_), "launch row pass");
+        ColumnArgs<R> a = column_args(1.0);
+        a.stage = 1;
+        a.emit = 0;
+        cuda_check(launch_column<R>(n_, a, stream_), "launch column pass");
+        cuda_check(cudaMemcpyAsync(out, acc_.ptr, sizeof(cx<R>) * compact_ * M_, cudaMemcpyDefault,
+                                   stream_),
+                   "copy drift");
+        cuda_check(cudaStreamSynchronize(stream_), "drift");
+    }
     void get_forcing_compact(double *out, int first, int count) override {
         if (fcount_ == 0)
             raise(HZLB_EINVAL, "this ensemble holds no forcing");

@@ -106,6 +106,10 @@ class Engine {
     // OU shell forcing on the device (ou.cuh): per-member forcing, transitions inside the step
     virtual void enable_ou(double sigma, double tau, int kmin, int kmax, bool initialize) = 0;
     virtual void get_forcing_compact(double *out, int first, int count) = 0;
+    // drift of every member's state, -N - (nu k^2 + alpha) w + f (the RK stage-1 derivative),
+    // into `out` (device or host, members x compact_size entries of the handle's precision);
+    // the state is unchanged
+    virtual void drift(void *out) = 0;
     // ---- stepping inside a caller's graph (mixed-resolution batches, mixed.cu) ------------
     // validate dt and run the start pass if the velocity columns are stale (waits for it)
     virtual void prepare_steps(double dt) = 0;

@@ -332,6 +332,27 @@ HZLB_API int hzlb_fit_pod(size_t m, size_t dimension, const double *snapshots, s
                           double fraction, int device, size_t *rank, double *mean, double *modes,
                           double *singular_values, double *captured);
 
+/* GalerkinModel(PODBasis, Solver&) (reduced.hpp:19-30, reduced.cpp:137-209): the quadratic
+ * reduced model da/dt = c + A a + Q(a,a) of the deterministic drift in the coefficients of a
+ * POD basis (mean and `rank` modes in the reference layout, e.g. from hzlb_fit_pod).  The
+ * drifts it needs are evaluated by the batched FP64 spectral kernels in one launch sequence.
+ * HZLB_EINVAL for forcing_sigma != 0, as the reference. */
+typedef struct hzlb_galerkin hzlb_galerkin;
+HZLB_API int hzlb_galerkin_create(int n, const hzlb_parameters *p, const double *mean,
+                                  const double *modes, size_t rank, int device,
+                                  hzlb_galerkin **out);
+HZLB_API void hzlb_galerkin_destroy(hzlb_galerkin *h);
+/* c (rank), A (rank x rank, [i][j]), Q (rank^3, [i][j][k]); any may be NULL */
+HZLB_API int hzlb_galerkin_coefficients(hzlb_galerkin *h, double *constant, double *linear,
+                                        double *quadratic);
+/* GalerkinModel::rhs for `count` coefficient vectors (host arrays, count x rank) */
+HZLB_API int hzlb_galerkin_rhs(hzlb_galerkin *h, const double *coefficients, size_t count,
+                               double *out);
+/* GalerkinModel::step: nsteps RK4 steps of dt for `count` coefficient vectors in place;
+ * HZLB_ERUNTIME "unstable Galerkin trajectory" on a nonfinite result */
+HZLB_API int hzlb_galerkin_step(hzlb_galerkin *h, double *coefficients, size_t count, double dt,
+                                uint64_t nsteps);
+
 /* No counterpart in the reference (its fit is capped at 512 snapshots).  POD of `snapshots`
  * FP32 fields of an n x n ensemble in the compact layout (device pointer, snapshots x
  * hzlb_compact_size complex floats), with the reference's inner product (spectral_inner over

@@ -262,6 +262,8 @@ class Reference:
                                  _u32p, _dp, _dp, _dp, _u64, _u64, C.c_double, C.c_double, _u64,
                                  _u64, _u64, u64p, _dp, _dp]
         lib.ref_fit_pod.argtypes = [_u64, _u64, _dp, _u64, C.c_double, u64p, _dp, _dp, _dp, _dp]
+        lib.ref_galerkin.argtypes = [C.c_int, _dp, _u64, _dp, _dp, _u64, _dp, _dp, _dp, C.c_double,
+                                     _u64]
 
     def check(self, rc: int):
         if rc != 0:
@@ -347,6 +349,18 @@ class Reference:
                                      _ptr(rec), _ptr(means)))
         r = records.value
         return dict(records=rec[:r].copy(), means=means[:r].copy())
+
+    def galerkin(self, n: int, p6, mean, modes, a, dt: float, steps: int):
+        """hzl::GalerkinModel: (rhs at a, state after `steps` RK4 steps of dt from a)."""
+        p = np.ascontiguousarray(p6, dtype=np.float64)
+        m = np.ascontiguousarray(mean, dtype=np.complex128).reshape(-1)
+        u = np.ascontiguousarray(modes, dtype=np.complex128).reshape(len(modes), -1)
+        a = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, len(u))
+        rhs, stepped = np.zeros_like(a), np.zeros_like(a)
+        self.check(self.lib.ref_galerkin(n, _ptr(p), len(u), _ptr(m.view(np.float64)),
+                                         _ptr(u.view(np.float64)), len(a), _ptr(a), _ptr(rhs),
+                                         _ptr(stepped), dt, steps))
+        return rhs, stepped
 
     def fit_pod(self, snapshots: np.ndarray, max_rank: int, fraction: float = 0.9999):
         s = np.ascontiguousarray(snapshots.reshape(len(snapshots), -1), dtype=np.complex128)

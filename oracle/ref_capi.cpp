@@ -292,4 +292,28 @@ int ref_fit_pod(unsigned long long m, unsigned long long dimension, const double
         *captured = b.captured_variance;
     });
 }
+// hzl::GalerkinModel over a POD basis given as mean + modes (reference layout): its rhs at
+// `count` coefficient vectors, and `steps` RK4 steps of dt from them (in place).
+int ref_galerkin(int n, const double *p6, unsigned long long rank, const double *mean,
+                 const double *modes, unsigned long long count, const double *a, double *rhs,
+                 double *stepped, double dt, unsigned long long steps) {
+    return guarded([&] {
+        const std::size_t dim = static_cast<std::size_t>(n) * n;
+        hzl::PODBasis basis;
+        basis.mean = to_field(mean, dim);
+        for (std::size_t j = 0; j < rank; ++j)
+            basis.modes.push_back(to_field(modes + 2 * j * dim, dim));
+        basis.singular_values.assign(rank, 1.0);
+        hzl::Solver solver(static_cast<std::size_t>(n), params(p6), 0);
+        hzl::GalerkinModel model(basis, solver);
+        for (std::size_t s = 0; s < count; ++s) {
+            hzl::Vector v(a + s * rank, a + (s + 1) * rank);
+            const auto r = model.rhs(v);
+            std::copy(r.begin(), r.end(), rhs + s * rank);
+            for (std::size_t t = 0; t < steps; ++t)
+                model.step(v, dt);
+            std::copy(v.begin(), v.end(), stepped + s * rank);
+        }
+    });
+}
 } // extern "C"

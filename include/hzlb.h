@@ -20,6 +20,10 @@
  *     (filter.hpp:17-18, filter.cpp:66-120)            hzlb_gather_members
  *   ensemble_kalman_filter analysis                    hzlb_enkf_analysis
  *     (filter.hpp:52-54, filter.cpp:237-321)
+ *   fit_pod / PODBasis                                 hzlb_fit_pod
+ *     (reduced.hpp:6-17, reduced.cpp:8-136)
+ *   GalerkinModel (rhs, step)                          hzlb_galerkin_create / _rhs / _step
+ *     (reduced.hpp:19-30, reduced.cpp:137-209)
  *
  * Conventions.  Every function returns HZLB_OK (0) or a negative HZLB_E* code; the message
  * of the last failure on the calling thread is hzlb_last_error().  HZLB_EINVAL corresponds

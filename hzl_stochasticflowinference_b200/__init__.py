@@ -155,6 +155,9 @@ def library() -> C.CDLL:
                                             _dp, C.POINTER(C.c_uint64),
                                             C.POINTER(hzlb_filter_record), C.c_size_t,
                                             C.POINTER(C.c_size_t), _dp]),
+        "hzlb_particle_log_likelihood": (C.c_int, [C.POINTER(hzlb_dataset), _dp, C.c_uint64,
+                                                   C.c_uint64, C.c_uint64, C.c_int, C.c_int,
+                                                   C.c_int, _dp]),
         "hzlb_ensemble_kalman_filter": (C.c_int, [C.POINTER(hzlb_dataset),
                                                   C.POINTER(hzlb_parameters), C.c_uint64,
                                                   C.c_uint64, C.POINTER(hzlb_enkf_options),
@@ -589,6 +592,32 @@ def bootstrap_filter(ds: dict, p: Parameters, particles: int, seed: int,
                      recs[i].effective_particles, recs[i].maximum_weight] for i in range(k)])
     return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec.reshape(-1, 4),
                 means=means[:k].copy())
+
+
+def particle_log_likelihood(ds: dict, log_parameters, particles: int, seed: int,
+                            precision: int = 8, device: int = 0) -> float:
+    """hzl::particle_log_likelihood (src/filter.cpp:141-149)."""
+    return _particle_ll(ds, log_parameters, particles, 0, seed, 0, precision, device)
+
+
+def averaged_particle_log_likelihood(ds: dict, log_parameters, particles: int, replicates: int,
+                                     seed: int, precision: int = 8, device: int = 0) -> float:
+    """hzl::averaged_particle_log_likelihood (src/filter.cpp:150-165): all replicates advance
+    as one batched ensemble of replicates x particles members."""
+    return _particle_ll(ds, log_parameters, particles, replicates, seed, 1, precision, device)
+
+
+def _particle_ll(ds, log_parameters, particles, replicates, seed, averaged, precision, device):
+    q = np.ascontiguousarray(log_parameters, dtype=np.float64)
+    if q.shape != (4,):
+        raise HzlbInvalidArgument(HZLB_EINVAL, "stochastic inference expects log(nu), "
+                                  "log(alpha), log(sigma), log(tau)")
+    dc, keep = _dataset_c(ds)
+    out = C.c_double()
+    _check(library().hzlb_particle_log_likelihood(C.byref(dc), _p(q), particles, replicates,
+                                                  seed, averaged, precision, device,
+                                                  C.byref(out)))
+    return out.value
 
 
 def ensemble_kalman_filter(ds: dict, p: Parameters, members: int, seed: int,

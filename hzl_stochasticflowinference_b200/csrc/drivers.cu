@@ -74,7 +74,17 @@ void validate_params(int n, const Params &p) {
 // kmin^2 <= |k|^2 <= kmax^2 in the reference's enumeration order (y outer, x inner).
 class OuBank {
   public:
-    OuBank(int n, const Params &p, int members, uint64_t seed) : n_(n), p_(p), M_(members) {
+    OuBank(int n, const Params &p, int members, uint64_t seed)
+        : OuBank(n, p, member_seeds(members, seed)) {}
+    // member m draws from NormalStream(stream_seeds[m])
+    static std::vector<uint64_t> member_seeds(int members, uint64_t seed) {
+        std::vector<uint64_t> v(members);
+        for (int m = 0; m < members; ++m)
+            v[m] = stream_seed(seed, static_cast<uint64_t>(m));
+        return v;
+    }
+    OuBank(int n, const Params &p, const std::vector<uint64_t> &stream_seeds)
+        : n_(n), p_(p), M_(static_cast<int>(stream_seeds.size())) {
         for (int y = 0; y < n; ++y)
             for (int x = 0; x < n; ++x) {
                 const int a = wave(x, n), b = wave(y, n);
@@ -92,7 +102,7 @@ class OuBank {
         streams_.reserve(M_);
         const double scale = p.sigma * std::sqrt(p.tau / 4);   // stationary draw
         for (int m = 0; m < M_; ++m) {
-            streams_.emplace_back(stream_seed(seed, m));
+            streams_.emplace_back(stream_seeds[m]);
             for (size_t k = 0; k < P; ++k) {
                 const double re = streams_[m](), im = streams_[m]();
                 value_[m * P + k] = scale * cd(re, im);
@@ -286,7 +296,11 @@ struct RefEnsemble {
     int precision_;
     std::vector<double> fbuf;
     RefEnsemble(int n_, const Params &p_, int members, uint64_t seed, int precision, int device)
-        : n(n_), M(members), p(p_), bank(n_, p_, members, seed), precision_(precision) {
+        : RefEnsemble(n_, p_, OuBank::member_seeds(members, seed), precision, device) {}
+    RefEnsemble(int n_, const Params &p_, const std::vector<uint64_t> &stream_seeds, int precision,
+                int device)
+        : n(n_), M(static_cast<int>(stream_seeds.size())), p(p_), bank(n_, p_, stream_seeds),
+          precision_(precision) {
         hzlb_config c{};
         c.n = n;
         c.members = M;
@@ -503,6 +517,167 @@ HZLB_API int hzlb_bootstrap_filter(const hzlb_dataset *data, const hzlb_paramete
         *log_likelihood = ll;
         *resampling_events = events;
         *nrecords = std::min(nrec, capacity);
+    });
+}
+
+// particle_log_likelihood / averaged_particle_log_likelihood (filter.cpp:141-165): the prior
+// (stochastic_log_prior, :127-140) and stability checks, then `replicates` bootstrap filters
+// (one for the plain likelihood) run as one batched ensemble: replicate r is the reference's
+// bootstrap_filter(data, decode(q), particles, seed_r) with seed_r = stream_seed(seed, r) for
+// the averaged likelihood (seed itself for the plain one) — its members draw their OU forcing
+// from stream_seed(seed_r, j), its resampling uniforms from mt19937_64(stream_seed(seed_r,
+// 2^64-1)) and its clones are reseeded with stream_seed(seed_r, (g+1) particles + j) — while
+// every step and observation of all replicates' members is one launch sequence.
+HZLB_API int hzlb_particle_log_likelihood(const hzlb_dataset *data, const double *log_parameters,
+                                          uint64_t particles, uint64_t replicates, uint64_t seed,
+                                          int averaged, int precision, int device, double *out) {
+    return guarded_driver([&] {
+        if (!data || !log_parameters || !out)
+            raise(HZLB_EINVAL, "null argument");
+        if (averaged && replicates == 0)
+            raise(HZLB_EINVAL, "averaged particle likelihood needs at least one replicate");
+        const double ninf = -std::numeric_limits<double>::infinity();
+        // stochastic_log_prior: only its finiteness matters here
+        for (int i = 0; i < 4; ++i) {
+            const double q = log_parameters[i];
+            if (!std::isfinite(q) || q < -10 || q > (i < 2 ? 0 : 2)) {
+                *out = ninf;
+                return;
+            }
+        }
+        // decode, then the explicit diffusion bound, both before the dataset is validated
+        Params p{std::exp(log_parameters[0]), std::exp(log_parameters[1]),
+                 std::exp(log_parameters[2]), std::exp(log_parameters[3]), data->forcing_min,
+                 data->forcing_max};
+        if (data->n < 0)
+            raise(HZLB_EINVAL, "invalid observation dataset");
+        const double largest = static_cast<double>((static_cast<uint64_t>(data->n) - 1) / 3);
+        if (data->dt * (2 * p.nu * largest * largest + p.alpha) > 2.5) {
+            *out = ninf;
+            return;
+        }
+        const Dataset ds = load_dataset(data);
+        validate_params(ds.n, p);
+        if (particles < 2)
+            raise(HZLB_EINVAL, "particle filter needs at least two particles");
+        if (particles > (1u << 20) || (averaged && replicates > (1u << 16)) ||
+            (averaged ? replicates : 1) * particles > (1u << 22))
+            raise(HZLB_EINVAL, "particle count times replicates exceeds the batch limit");
+        const int R = averaged ? static_cast<int>(replicates) : 1;
+        const int P = static_cast<int>(particles), M = R * P, n = ds.n;
+        std::vector<uint64_t> rseed(R), member_seed(M);
+        for (int r = 0; r < R; ++r) {
+            rseed[r] = averaged ? stream_seed(seed, static_cast<uint64_t>(r)) : seed;
+            for (int j = 0; j < P; ++j)
+                member_seed[r * P + j] = stream_seed(rseed[r], static_cast<uint64_t>(j));
+        }
+        RefEnsemble e(n, p, member_seed, precision, device);
+        e.set_initial("multimode");
+        std::vector<double> weights(M, 1 / static_cast<double>(P)), ll(R, 0.0), logs(P), w(P);
+        std::vector<char> done(R, 0);
+        std::vector<std::mt19937_64> resampling;
+        for (int r = 0; r < R; ++r)
+            resampling.emplace_back(stream_seed(rseed[r], std::numeric_limits<uint64_t>::max()));
+        size_t current = 0, begin = 0, group = 0;
+        while (begin < ds.obs.size()) {
+            const uint64_t target = ds.obs[begin].step;
+            size_t end = begin;
+            while (end < ds.obs.size() && ds.obs[end].step == target)
+                ++end;
+            for (uint64_t s = current; s < target; ++s)
+                e.step(ds.dt);
+            e.check_status();
+            const size_t pc = end - begin;
+            std::vector<uint32_t> xs(pc), ys(pc);
+            for (size_t o = 0; o < pc; ++o) {
+                xs[o] = ds.obs[begin + o].x;
+                ys[o] = ds.obs[begin + o].y;
+            }
+            std::vector<double> field(static_cast<size_t>(M) * pc);
+            e.engine->observe(xs.data(), ys.data(), pc, field.data());
+            const double half_log_two_pi = 0.5 * std::log(2 * kPi);
+            std::vector<uint32_t> anc(M);
+            for (int i = 0; i < M; ++i)
+                anc[i] = static_cast<uint32_t>(i);
+            bool any_resampled = false;
+            std::vector<int> resampled_replicates, retired;
+            for (int r = 0; r < R; ++r) {
+                if (done[r])
+                    continue;
+                const double *wr = weights.data() + static_cast<size_t>(r) * P;
+                for (int j = 0; j < P; ++j) {
+                    double value = wr[j] > 0 ? std::log(wr[j]) : ninf;
+                    for (size_t o = 0; o < pc; ++o) {
+                        const auto &ob = ds.obs[begin + o];
+                        const double residual =
+                            (field[static_cast<size_t>(r * P + j) * pc + o] - ob.value) / ob.standard_deviation;
+                        value -= 0.5 * residual * residual + std::log(ob.standard_deviation) + half_log_two_pi;
+                    }
+                    logs[j] = value;
+                }
+                double maximum = logs[0];
+                for (int j = 1; j < P; ++j)
+                    if (maximum < logs[j])
+                        maximum = logs[j];
+                if (!std::isfinite(maximum)) {
+                    ll[r] = ninf;
+                    done[r] = 1;
+                    retired.push_back(r);
+                    continue;
+                }
+                double inc = 0, ess = 0, mw = 0;
+                pf_weights_host(logs.data(), P, w.data(), &inc, &ess, &mw);
+                std::copy(w.begin(), w.end(), weights.begin() + static_cast<size_t>(r) * P);
+                ll[r] += inc;
+                if (ess < static_cast<double>(P) / 2 && end < ds.obs.size()) {
+                    const double u = static_cast<double>(resampling[r]() >> 11) * 0x1.0p-53;
+                    std::vector<uint32_t> local(P);
+                    systematic_resample_host(w.data(), P, u, local.data());
+                    for (int j = 0; j < P; ++j)
+                        anc[r * P + j] = static_cast<uint32_t>(r * P) + local[j];
+                    std::fill(weights.begin() + static_cast<size_t>(r) * P,
+                              weights.begin() + static_cast<size_t>(r + 1) * P, 1 / static_cast<double>(P));
+                    resampled_replicates.push_back(r);
+                    any_resampled = true;
+                }
+            }
+            const auto live = std::find(done.begin(), done.end(), 0);
+            if (live == done.end())
+                break;
+            // a replicate that has ended stops being weighted; its members are overwritten by
+            // a copy of a live member so that they stay finite while the others advance
+            if (!retired.empty()) {
+                const uint32_t source = static_cast<uint32_t>((live - done.begin()) * P);
+                for (int r : retired)
+                    for (int j = 0; j < P; ++j)
+                        anc[r * P + j] = source;
+                any_resampled = true;
+            }
+            if (any_resampled) {
+                e.engine->gather(anc.data());
+                e.bank.gather(anc);
+                for (int r : resampled_replicates)
+                    for (int j = 0; j < P; ++j)
+                        e.bank.reseed(r * P + j,
+                                      stream_seed(rseed[r], (group + 1) * particles + static_cast<uint64_t>(j)));
+            }
+            current = target;
+            begin = end;
+            ++group;
+        }
+        if (!averaged) {
+            *out = ll[0];
+            return;
+        }
+        const double maximum = *std::max_element(ll.begin(), ll.end());
+        if (!std::isfinite(maximum)) {
+            *out = ninf;
+            return;
+        }
+        double total = 0;
+        for (double v : ll)
+            total += std::exp(v - maximum);
+        *out = maximum + std::log(total / static_cast<double>(R));
     });
 }
 

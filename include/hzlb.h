@@ -16,6 +16,8 @@
  *     (solver.hpp:86, solver.cpp:398-402)
  *   hzl::ensemble(n, p, dt, steps, count, ...)         hzlb_ensemble_create + hzlb_step +
  *     (inference.hpp:85-86, inference.cpp:555-590)     hzlb_diagnostics
+ *   (averaged_)particle_log_likelihood                hzlb_particle_log_likelihood
+ *     (filter.hpp:19-24, filter.cpp:141-165)
  *   bootstrap_filter weights / resampling             hzlb_pf_weights, hzlb_systematic_resample,
  *     (filter.hpp:17-18, filter.cpp:66-120)            hzlb_gather_members
  *   ensemble_kalman_filter analysis                    hzlb_enkf_analysis
@@ -254,6 +256,17 @@ HZLB_API int hzlb_bootstrap_filter(const hzlb_dataset *data, const hzlb_paramete
                                    int precision, int device, double *log_likelihood,
                                    uint64_t *resampling_events, hzlb_filter_record *records,
                                    size_t capacity, size_t *nrecords, double *mean_vorticity);
+/* hzl::particle_log_likelihood(data, q, particles, seed) (averaged = 0) and
+ * hzl::averaged_particle_log_likelihood(data, q, particles, replicates, seed) (averaged = 1)
+ * (include/hzl/filter.hpp:19-24, src/filter.cpp:141-165).  log_parameters = {log nu, log alpha,
+ * log sigma, log tau}; *out = -inf outside the prior's support or past the explicit diffusion
+ * bound, else the (log-mean-exp over replicates of the) bootstrap filter log-likelihood.  All
+ * replicates x particles members advance as one ensemble; replicate r reproduces
+ * bootstrap_filter(data, decode(q), particles, stream_seed(seed, r)) (seed itself when
+ * averaged = 0).  replicates is ignored when averaged = 0. */
+HZLB_API int hzlb_particle_log_likelihood(const hzlb_dataset *data, const double *log_parameters,
+                                          uint64_t particles, uint64_t replicates, uint64_t seed,
+                                          int averaged, int precision, int device, double *out);
 /* hzl::ensemble_kalman_filter(data, p, members, seed, options) (include/hzl/filter.hpp:52-54,
  * src/filter.cpp:204-356): serial perturbed-observation updates of the joint (vorticity,
  * forcing) state.  mean_vorticity (optional): capacity x n*n complex per record. */

@@ -258,6 +258,9 @@ class Reference:
         lib.ref_bootstrap_filter.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
                                              u64p, _u32p, _u32p, _dp, _dp, _dp, _u64, _u64, C.c_int,
                                              _dp, u64p, _u64, u64p, _dp, _dp]
+        lib.ref_particle_log_likelihood.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                                    _u64, u64p, _u32p, _u32p, _dp, _dp, _dp, _u64,
+                                                    _u64, _u64, C.c_int, _dp]
         lib.ref_enkf.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64, u64p, _u32p,
                                  _u32p, _dp, _dp, _dp, _u64, _u64, C.c_double, C.c_double, _u64,
                                  _u64, _u64, u64p, _dp, _dp]
@@ -334,6 +337,17 @@ class Reference:
         g = groups.value
         return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec[:g].copy(),
                     means=means[:g].copy())
+
+    def particle_log_likelihood(self, ds, q, particles, seed, replicates=None):
+        """particle_log_likelihood, or averaged_particle_log_likelihood when replicates is
+        given (filter.cpp:141-165)."""
+        args, keep = self._ds_args(ds)
+        qa = np.ascontiguousarray(q, dtype=np.float64)
+        out = C.c_double()
+        self.check(self.lib.ref_particle_log_likelihood(
+            *args, _ptr(qa), particles, replicates or 0, seed, int(replicates is not None),
+            C.byref(out)))
+        return out.value
 
     def enkf(self, ds, p6, members, seed, inflation=1.0, localization=0.0, forecast_steps=0,
              forecast_every=1):

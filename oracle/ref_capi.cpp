@@ -247,6 +247,22 @@ int ref_bootstrap_filter(int n, double dt, int stochastic, int fmin, int fmax,
     });
 }
 
+// particle_log_likelihood (averaged = 0) / averaged_particle_log_likelihood (averaged = 1)
+int ref_particle_log_likelihood(int n, double dt, int stochastic, int fmin, int fmax,
+                                unsigned long long nobs, const unsigned long long *steps,
+                                const unsigned *xs, const unsigned *ys, const double *values,
+                                const double *sds, const double *q4, unsigned long long particles,
+                                unsigned long long replicates, unsigned long long seed,
+                                int averaged, double *out) {
+    return guarded([&] {
+        const auto d = dataset(static_cast<std::size_t>(n), dt, stochastic, fmin, fmax, nobs, steps,
+                               xs, ys, values, sds);
+        const hzl::Vector q(q4, q4 + 4);
+        *out = averaged ? hzl::averaged_particle_log_likelihood(d, q, particles, replicates, seed)
+                        : hzl::particle_log_likelihood(d, q, particles, seed);
+    });
+}
+
 int ref_enkf(int n, double dt, int stochastic, int fmin, int fmax, unsigned long long nobs,
              const unsigned long long *steps, const unsigned *xs, const unsigned *ys,
              const double *values, const double *sds, const double *p6, unsigned long long members,

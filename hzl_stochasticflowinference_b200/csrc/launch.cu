@@ -18,10 +18,15 @@ template <typename R, int N> struct L {
 
     // persistent grids: resident blocks per SM x SMs, per device
     static inline int col_resident[64] = {}, row_resident[64] = {};
+    // one column kernel per RK stage
+    static constexpr void (*col_kernels[5])(const ColumnArgs<R>, int) = {
+        column_kernel<R, N, 0>, column_kernel<R, N, 1>, column_kernel<R, N, 2>,
+        column_kernel<R, N, 3>, column_kernel<R, N, 4>};
     static cudaError_t prepare() {
-        cudaError_t e = cudaFuncSetAttribute(column_kernel<R, N>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             static_cast<int>(col_smem));
+        cudaError_t e = cudaSuccess;
+        for (int st = 0; st < 5 && e == cudaSuccess; ++st)
+            e = cudaFuncSetAttribute(col_kernels[st], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(col_smem));
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(row_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(row_smem));
@@ -30,9 +35,14 @@ template <typename R, int N> struct L {
             e = cudaGetDevice(&dev);
         if (e == cudaSuccess)
             e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cb, column_kernel<R, N>,
-                                                              G::COL_THREADS, col_smem);
+        // persistent grid of the column pass: the fewest resident blocks over the stages
+        cb = 1 << 30;
+        for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
+            int b = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, col_kernels[st], G::COL_THREADS,
+                                                              col_smem);
+            cb = std::min(cb, b);
+        }
         if (e == cudaSuccess)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rb, row_kernel<R, N>,
                                                               G::ROW_THREADS, row_smem);
@@ -55,7 +65,9 @@ template <typename R, int N> struct L {
         const int items = a.members * G::NCG;
         const int res = resident(col_resident);
         const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
-        column_kernel<R, N><<<grid, G::COL_THREADS, col_smem, s>>>(a, items);
+        if (a.stage < 0 || a.stage > 4)
+            return cudaErrorInvalidValue;
+        col_kernels[a.stage]<<<grid, G::COL_THREADS, col_smem, s>>>(a, items);
         return cudaGetLastError();
     }
     static cudaError_t row(const RowArgs<R> &a, cudaStream_t s, int cap) {

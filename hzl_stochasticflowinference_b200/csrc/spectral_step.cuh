@@ -50,7 +50,10 @@ template <typename R, int N> struct Cfg {
     // up to whole 16-byte chunks
     static constexpr int PER16 = 16 / (2 * static_cast<int>(sizeof(R)));
     static constexpr int ST_STRIDE = (LPB * LD + PER16 + PER16 - 1) / PER16 * PER16;
-    static constexpr int ST_WORDS = 3 * ST_STRIDE > 2 * LPB * N ? 3 * ST_STRIDE : 2 * LPB * N;
+    // per-line stride of the product buffer and of the inverse-transform exchange area: a
+    // padded FFT line buffer rounded up to whole 16-byte chunks
+    static constexpr int LS = (BUF + PER16 - 1) / PER16 * PER16;
+    static constexpr int ST_WORDS = 3 * ST_STRIDE > LPB * (LS + N) ? 3 * ST_STRIDE : LPB * (LS + N);
     // row kernel: TY rows per block, one row per group of T threads, 128 threads at least
     static constexpr int TY_RAW = 128 / T;
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
@@ -151,24 +154,27 @@ __device__ __forceinline__ bool block_wait(uint64_t *bar, uint32_t parity, volat
     return ok;
 }
 
-template <typename R, int N>
+// S is the RK stage (0: velocity of the initial state only, 1..3 intermediate, 4 final), a
+// compile-time constant so that each stage's epilogue is straight-line code.
+template <typename R, int N, int S>
 __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     column_kernel(const ColumnArgs<R> a, int items) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD, K = G::K, LPB = G::LPB;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // product input [2][LPB][N]; state window [3][ST_STRIDE], reused as the staging of the
-    // velocity rows [N][2][LPB] once the epilogue has consumed it
+    // product input [2][LPB][LS]: each line's two input columns, padded, double as the
+    // exchange buffers of its forward transforms once read; state window [3][ST_STRIDE],
+    // reused once the epilogue has consumed it as the exchange buffers [LPB][LS] of the
+    // inverse transforms followed by the staging rows [N][LPB] of one output field
     cx<R> *nlbuf = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *stbuf = nlbuf + 2 * LPB * N;
-    cx<R> *lines = stbuf + G::ST_WORDS;                            // [LPB][BUF]
-    cx<R> *tw = lines + LPB * G::BUF;                              // [TWE] per-pass twiddles
+    cx<R> *stbuf = nlbuf + 2 * LPB * G::LS;
+    cx<R> *tw = stbuf + G::ST_WORDS;                               // [TWE] per-pass twiddles
     __shared__ __align__(8) uint64_t bars[3];                      // nl, (unused), state
     __shared__ int flags[2];
     __shared__ unsigned long long step_sh;
 
-    const bool forward = a.stage > 0;
-    const int nst = a.stage <= 1 ? 1 : 3;   // state arrays read: w_n (and stage input, acc)
+    constexpr bool forward = S > 0;
+    constexpr int nst = S <= 1 ? 1 : 3;   // state arrays read: w_n (and stage input, acc)
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -179,14 +185,22 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     load_pass_twiddles<N, E, R>(tw, a.tw);
     __syncthreads();
 
+    // one bulk copy per product column, issued by the lanes of warp 0 once lane 0 has armed
+    // the barrier (every lane of warp 0 calls this)
     auto issue_nl = [&](int it) {
         const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
         const int nl = min(LPB, C - kx0);
-        const uint32_t bytes = static_cast<uint32_t>(nl * N * sizeof(cx<R>));
-        mbar_arrive_expect(&bars[0], 2 * bytes);
-        for (int f = 0; f < 2; ++f)
-            bulk_copy_g2s(nlbuf + f * LPB * N,
-                          a.nl + ((static_cast<size_t>(m) * 2 + f) * C + kx0) * N, bytes, &bars[0]);
+        constexpr uint32_t bytes = static_cast<uint32_t>(N * sizeof(cx<R>));
+        const int lane = threadIdx.x & 31;
+        if (lane == 0)
+            mbar_arrive_expect(&bars[0], 2 * nl * bytes);
+        __syncwarp();
+        for (int c = lane; c < 2 * nl; c += 32) {
+            const int f = c / nl, l = c % nl;
+            bulk_copy_g2s(nlbuf + (f * LPB + l) * G::LS,
+                          a.nl + ((static_cast<size_t>(m) * 2 + f) * C + kx0 + l) * N, bytes,
+                          &bars[0]);
+        }
     };
     // state window of a column group: starts `shift` entries early so that the copy is
     // 16-byte aligned, and covers whole 16-byte chunks
@@ -205,15 +219,14 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         const size_t base = window(it, shift, bytes);
         mbar_arrive_expect(&bars[2], nst * bytes);
         bulk_copy_g2s(stbuf, a.omega + base, bytes, &bars[2]);
-        if (nst == 3) {
+        if constexpr (nst == 3) {
             bulk_copy_g2s(stbuf + G::ST_STRIDE, a.ystage + base, bytes, &bars[2]);
             bulk_copy_g2s(stbuf + 2 * G::ST_STRIDE, a.acc + base, bytes, &bars[2]);
         }
     };
 
     const int line = threadIdx.x / T, t = threadIdx.x % T;
-    cx<R> *sm = lines + line * G::BUF;
-    if (threadIdx.x == 0 && forward && static_cast<int>(blockIdx.x) < items)
+    if (threadIdx.x < 32 && forward && static_cast<int>(blockIdx.x) < items)
         issue_nl(blockIdx.x);
     bool timed_out = false;
     int k = 0;
@@ -236,7 +249,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
 
         cx<R> y[E];   // next stage input at this thread's positions (zero outside the band)
         cx<R> v[E];
-        if (!forward) {
+        if constexpr (!forward) {
             if (!block_wait(&bars[2], k & 1, &flags[1])) {
                 timed_out = true;
                 break;
@@ -252,29 +265,31 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 break;
             }
             // forward column FFTs of the product spectra (unnormalised; 1/N^2 below):
-            // A^ = -kx ky P^ - (kx^2 - ky^2) Q^ with P = v^2 - u^2, Q = u v
-            const cx<R> *srcP = nlbuf + line * N;
-            const cx<R> *srcQ = srcP + LPB * N;
+            // A^ = -kx ky P^ - (kx^2 - ky^2) Q^ with P = v^2 - u^2, Q = u v.  One loop body for
+            // both fields keeps a single copy of the transform in the kernel.
             cx<R> adv[E];
+#pragma unroll 1
+            for (int f = 0; f < 2; ++f) {
+                cx<R> *src = nlbuf + (f * LPB + line) * G::LS;
 #pragma unroll
-            for (int r = 0; r < E; ++r)
-                v[r] = srcP[t + r * T];
-            fft_line<N, E, -1, R>(v, sm, tw, t);
-            static_for<0, E>([&](auto rc) {
-                constexpr int r = decltype(rc)::value;
-                const int p = t + r * T;
-                const int ky = Band<N, T, r>::low ? p : (Band<N, T, r>::high ? p - N : (p <= K ? p : p - N));
-                adv[r] = scale(static_cast<R>(-kxc * ky), v[r]);
-            });
-#pragma unroll
-            for (int r = 0; r < E; ++r)
-                v[r] = srcQ[t + r * T];
-            // every line has its product inputs in registers: stream the next item's in
+                for (int r = 0; r < E; ++r)
+                    v[r] = src[t + r * T];
+                __syncwarp();   // the line's lanes have read the column it exchanges in
+                fft_line<N, E, -1, R>(v, src, tw, t);
+                if (f == 0) {
+                    static_for<0, E>([&](auto rc) {
+                        constexpr int r = decltype(rc)::value;
+                        const int p = t + r * T;
+                        const int ky = Band<N, T, r>::low ? p : (Band<N, T, r>::high ? p - N : (p <= K ? p : p - N));
+                        adv[r] = scale(static_cast<R>(-kxc * ky), v[r]);
+                    });
+                }
+            }
+            // every line is done with the product buffer: stream the next item's in
             fence_proxy_async_shared();
             __syncthreads();
-            if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items)
+            if (threadIdx.x < 32 && it + static_cast<int>(gridDim.x) < items)
                 issue_nl(it + gridDim.x);
-            fft_line<N, E, -1, R>(v, sm, tw, t);
             if (!block_wait(&bars[2], k & 1, &flags[1])) {
                 timed_out = true;
                 break;
@@ -291,7 +306,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                     const int ky = j <= K ? j : j - LD;
                     const R k2 = static_cast<R>(kxc * kxc + ky * ky);
                     const cx<R> wn = s_w[j];
-                    const cx<R> ys = a.stage == 1 ? wn : s_y[j];
+                    const cx<R> ys = S == 1 ? wn : s_y[j];
                     // rhs: active ? -A^ - (nu k^2 + alpha) w + f : 0   (solver.cpp:197-202)
                     cx<R> kk = mk<R>(0, 0);
                     if (!(kxc == 0 && j == 0)) {
@@ -304,15 +319,15 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                                                 static_cast<size_t>(kxc) * LD + j];
                     }
                     const size_t idx = cbase + j;
-                    if (a.stage == 1) {
+                    if constexpr (S == 1) {
                         a.acc[idx] = kk;
                         y[r] = wn + scale(dt / 2, kk);
                         a.ystage[idx] = y[r];
-                    } else if (a.stage == 2) {
+                    } else if constexpr (S == 2) {
                         a.acc[idx] = s_a[j] + scale(static_cast<R>(2.0), kk);
                         y[r] = wn + scale(dt / 2, kk);
                         a.ystage[idx] = y[r];
-                    } else if (a.stage == 3) {
+                    } else if constexpr (S == 3) {
                         a.acc[idx] = s_a[j] + scale(static_cast<R>(2.0), kk);
                         y[r] = wn + scale(dt, kk);
                         a.ystage[idx] = y[r];
@@ -341,11 +356,12 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
 
         if (a.emit) {
             // velocity of the next stage input (solver.cpp:177-185): u^ = i ky psi^,
-            // v^ = -i kx psi^ with psi^ = w^/k^2; inverse column FFTs, staged in shared memory
-            // (reusing the state window) as rows [y][field][line]
+            // v^ = -i kx psi^ with psi^ = w^/k^2; inverse column FFTs exchanging in the state
+            // window, each field staged there as rows [y][line] (swizzled) and written to the
+            // rows [y][field][kx] of W in 32-byte runs
             fence_proxy_async_shared();
             __syncthreads();   // every line is done with the state window
-            cx<R> *wst = stbuf;
+            cx<R> *xb = stbuf + line * G::LS;
             // psi^ = w^ / k^2 once per mode (k = 0 gives 0), then u^ and v^ from it
             static_for<0, E>([&](auto rc) {
                 constexpr int r = decltype(rc)::value;
@@ -361,6 +377,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 }
                 y[r] = psi;
             });
+            cx<R> *wst = stbuf + LPB * G::LS;   // one field's rows [N][LPB]
+            const int nl = min(LPB, C - kx0);
+            cx<R> *dst = a.w + static_cast<size_t>(m) * N * 2 * C + kx0;
 #pragma unroll 1
             for (int f = 0; f < 2; ++f) {
                 static_for<0, E>([&](auto rc) {
@@ -371,22 +390,20 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                     const cx<R> psi = y[r];
                     v[r] = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
                 });
-                fft_line<N, E, +1, R>(v, sm, tw, t);
+                fft_line<N, E, +1, R>(v, xb, tw, t);
+                if (f == 1)
+                    __syncthreads();   // field 0 is out of the staging rows
 #pragma unroll
                 for (int r = 0; r < E; ++r) {
                     const int yy = t + r * T;
-                    wst[yy * 2 * LPB + ((f * LPB + line) ^ swz<2 * LPB>(yy))] = v[r];
+                    wst[yy * LPB + (line ^ swz<LPB>(yy))] = v[r];
                 }
-            }
-            __syncthreads();
-            const int nl = min(LPB, C - kx0);
-            cx<R> *dst = a.w + static_cast<size_t>(m) * N * 2 * C + kx0;
-            for (int i = threadIdx.x; i < N * 2 * LPB; i += blockDim.x) {
-                const int l = i % LPB, yf = i / LPB;
-                const int yy = yf >> 1;
-                if (l < nl)
-                    dst[static_cast<size_t>(yf) * C + l] =
-                        wst[yy * 2 * LPB + (((yf & 1) * LPB + l) ^ swz<2 * LPB>(yy))];
+                __syncthreads();
+                for (int i = threadIdx.x; i < N * LPB; i += blockDim.x) {
+                    const int l = i % LPB, yy = i / LPB;
+                    if (l < nl)
+                        dst[(static_cast<size_t>(yy) * 2 + f) * C + l] = wst[yy * LPB + (l ^ swz<LPB>(yy))];
+                }
             }
         }
         fence_proxy_async_shared();   // this thread's shared-memory accesses precede the next bulk copies
@@ -398,7 +415,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         return;   // uniform across the block
     }
 
-    if (a.stage == 4) {
+    if constexpr (S == 4) {
         // the last block to finish advances the device step counter (every block read it
         // before arriving, so no block sees the new value)
         if (threadIdx.x == 0) {
@@ -414,14 +431,12 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     }
 }
 
-// Inverse row transform of two real fields packed as a + i b.  A and B hold the x-spectra of
-// the row for kx = 0..K (column-pass output); negative kx follow from the fields being real
-// (A(-kx) = conj A(kx)), and the kx = 0 entries are real (imaginary roundoff dropped, as the
-// reference keeps only the real part of its inverse transforms).  On exit z = a + i b at
-// the thread's x positions.
+// Packs the x-spectra of two real fields as a + i b for the inverse row transform.  A and B
+// hold kx = 0..K of the row (column-pass output); negative kx follow from the fields being
+// real (A(-kx) = conj A(kx)), and the kx = 0 entries are real (imaginary roundoff dropped, as
+// the reference keeps only the real part of its inverse transforms).
 template <int N, int E, typename R>
-__device__ __forceinline__ void packed_row_inverse(cx<R> (&z)[E], const cx<R> *A, const cx<R> *B,
-                                                   cx<R> *sm, const cx<R> *tw, int t) {
+__device__ __forceinline__ void pack_row(cx<R> (&z)[E], const cx<R> *A, const cx<R> *B, int t) {
     constexpr int T = N / E, K = (N - 1) / 3;
     static_for<0, E>([&](auto rc) {
         constexpr int r = decltype(rc)::value;
@@ -453,40 +468,46 @@ __device__ __forceinline__ void packed_row_inverse(cx<R> (&z)[E], const cx<R> *A
         }
         z[r] = mk<R>(za.x - zb.y, za.y + zb.x);
     });
-    fft_line<N, E, +1, R>(z, sm, tw, t);
 }
+
+// Number of a thread's positions p = t + r T that can hold a retained kx (0 <= p <= K).
+template <int N, int E> struct LowSlots {
+    static constexpr int T = N / E, K = (N - 1) / 3;
+    static constexpr int value = K / T + 1 < E ? K / T + 1 : E;
+};
 
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowArgs<R> a, int items) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // input tiles [2][TY][2][C]; once a tile is packed into registers its buffer holds the
-    // product spectra [2C][TY] (swizzled rows) until they are stored
-    cx<R> *tiles = reinterpret_cast<cx<R> *>(smem_raw);
-    cx<R> *lines = tiles + 2 * G::TILE;                    // [GROUPS][BUF]
-    cx<R> *tw = lines + G::GROUPS * G::BUF;                // [TWE] per-pass twiddles
-    __shared__ __align__(8) uint64_t bars[2];
+    // input tile [TY][2][C], refilled with the next item's tile as soon as every row has read
+    // its entries; FFT line buffers [GROUPS][BUF], reused once every row has finished its
+    // transforms as the staging of the product spectra [2C][TY] (swizzled rows)
+    cx<R> *tile = reinterpret_cast<cx<R> *>(smem_raw);
+    cx<R> *lines = tile + G::TILE;
+    cx<R> *tw = lines + G::GROUPS * G::BUF;
+    static_assert(2 * C * TY <= G::GROUPS * G::BUF, "product staging fits in the line buffers");
+    __shared__ __align__(8) uint64_t bar;
     __shared__ int flag;
     constexpr int tiles_per_member = N / TY;
     constexpr uint32_t tile_bytes = G::TILE * sizeof(cx<R>);
     static_assert(tile_bytes % 16 == 0, "bulk copies move 16-byte multiples");
+    constexpr int RL = LowSlots<N, E>::value;
 
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        mbar_init(&bar, 1);
         mbar_init_fence();
     }
     load_pass_twiddles<N, E, R>(tw, a.tw);
     __syncthreads();
-    auto issue = [&](int it, int b) {
+    auto issue = [&](int it) {
         const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
-        mbar_arrive_expect(&bars[b], tile_bytes);
-        bulk_copy_g2s(tiles + b * G::TILE, a.w + (static_cast<size_t>(m) * N + y0) * 2 * C,
-                      tile_bytes, &bars[b]);
+        mbar_arrive_expect(&bar, tile_bytes);
+        bulk_copy_g2s(tile, a.w + (static_cast<size_t>(m) * N + y0) * 2 * C, tile_bytes, &bar);
     };
     if (threadIdx.x == 0 && static_cast<int>(blockIdx.x) < items)
-        issue(blockIdx.x, 0);
+        issue(blockIdx.x);
 
     const int g = threadIdx.x / T, t = threadIdx.x % T;
     const bool active = g < TY;
@@ -494,20 +515,21 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
     cx<R> *sm = lines + g * G::BUF;
     int k = 0;
     for (int it = blockIdx.x; it < items; it += gridDim.x, ++k) {
-        const int b = k & 1;
         const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
-        if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items) {
-            fence_proxy_async_shared();
-            issue(it + gridDim.x, b ^ 1);
-        }
-        if (!block_wait(&bars[b], (k >> 1) & 1, &flag)) {
+        if (!block_wait(&bar, k & 1, &flag)) {
             if (threadIdx.x == 0)
                 atomicOr(&a.ctl->status, STATUS_TIMEOUT);
             return;   // uniform across the block
         }
-        const cx<R> *row = tiles + b * G::TILE + ty * 2 * C;
+        const cx<R> *row = tile + ty * 2 * C;
         cx<R> z[E];
-        packed_row_inverse<N, E, R>(z, row, row + C, sm, tw, t);
+        pack_row<N, E, R>(z, row, row + C, t);
+        // every row holds its inputs in registers: stream the next item's tile in
+        fence_proxy_async_shared();
+        __syncthreads();
+        if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items)
+            issue(it + gridDim.x);
+        fft_line<N, E, +1, R>(z, sm, tw, t);
         R vmax = 0;
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -523,23 +545,32 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
                 atomicOr(&a.ctl->status, STATUS_CFL);
         }
         fft_line<N, E, -1, R>(z, sm, tw, t);
-#pragma unroll
-        for (int r = 0; r < E; ++r)
-            sm[pad<E>(t + r * T)] = z[r];
-        __syncthreads();   // every group has packed its row: the tile buffer takes the products
-        cx<R> *nlt = tiles + b * G::TILE;
+        // separate P^ and Q^ at kx = p from z(p) and conj z(N - p); only the partners of
+        // retained kx are stored
+        static_for<0, E>([&](auto rc) {
+            constexpr int r = decltype(rc)::value;
+            if constexpr (!Band<N, T, r>::zero)
+                sm[pad<E>(t + r * T)] = z[r];
+        });
+        __syncwarp();
+        cx<R> ph[RL], qh[RL];
+        static_for<0, RL>([&](auto rc) {
+            constexpr int r = decltype(rc)::value;
+            const int p = t + r * T;
+            const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
+            const cx<R> sa = zk + zc, sb = zk - zc;
+            ph[r] = mk<R>(sa.x / 2, sa.y / 2);
+            qh[r] = mk<R>(sb.y / 2, -sb.x / 2);
+        });
+        __syncthreads();   // every row is done with its line buffer: stage the products there
+        cx<R> *nlt = lines;
         if (active) {
-            static_for<0, E>([&](auto rc) {
+            static_for<0, RL>([&](auto rc) {
                 constexpr int r = decltype(rc)::value;
-                using Bd = Band<N, T, r>;
-                if constexpr (Bd::low || Bd::mixed) {
-                    const int p = t + r * T;
-                    if (Bd::low || p <= K) {
-                        const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
-                        const cx<R> sa = zk + zc, sb = zk - zc;
-                        nlt[p * TY + (ty ^ swz<TY>(p))] = mk<R>(sa.x / 2, sa.y / 2);          // P^
-                        nlt[(C + p) * TY + (ty ^ swz<TY>(C + p))] = mk<R>(sb.y / 2, -sb.x / 2);   // Q^
-                    }
+                const int p = t + r * T;
+                if (Band<N, T, r>::low || p <= K) {
+                    nlt[p * TY + (ty ^ swz<TY>(p))] = ph[r];                 // P^
+                    nlt[(C + p) * TY + (ty ^ swz<TY>(C + p))] = qh[r];       // Q^
                 }
             });
         }
@@ -549,18 +580,18 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
             const int t2 = i % TY, fk = i / TY;
             dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * TY + (t2 ^ swz<TY>(fk))];
         }
-        fence_proxy_async_shared();
-        __syncthreads();
+        // the next item's transforms write the line buffers only after its tile barrier and
+        // the block barrier that follows it
     }
 }
 
 template <typename R, int N> constexpr size_t column_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (2 * G::LPB * N + G::ST_WORDS + G::LPB * G::BUF + G::TWE);
+    return sizeof(cx<R>) * (2 * G::LPB * G::LS + G::ST_WORDS + G::TWE);
 }
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
-    return sizeof(cx<R>) * (2 * G::TILE + G::GROUPS * G::BUF + G::TWE);
+    return sizeof(cx<R>) * (G::TILE + G::GROUPS * G::BUF + G::TWE);
 }
 
 } // namespace hzlb

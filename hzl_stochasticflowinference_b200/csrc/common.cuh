@@ -12,7 +12,9 @@
 
 namespace hzlb {
 
-template <typename R> struct cx {
+// Interleaved complex value, aligned to its size (as float2 / double2) so that one load or
+// store moves both parts; device buffers of cx<R> must be aligned to sizeof(cx<R>).
+template <typename R> struct alignas(2 * sizeof(R)) cx {
     R x, y;
 };
 template <typename R> __host__ __device__ __forceinline__ cx<R> mk(R a, R b) {

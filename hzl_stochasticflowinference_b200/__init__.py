@@ -155,6 +155,11 @@ def library() -> C.CDLL:
                                             _dp, C.POINTER(C.c_uint64),
                                             C.POINTER(hzlb_filter_record), C.c_size_t,
                                             C.POINTER(C.c_size_t), _dp]),
+        "hzlb_dataset_save": (C.c_int, [C.POINTER(hzlb_dataset), C.c_char_p]),
+        "hzlb_dataset_validate": (C.c_int, [C.POINTER(hzlb_dataset)]),
+        "hzlb_dataset_load": (C.c_int, [C.c_char_p, C.POINTER(hzlb_dataset),
+                                        C.POINTER(hzlb_observation), C.c_size_t,
+                                        C.POINTER(C.c_size_t)]),
         "hzlb_particle_log_likelihood": (C.c_int, [C.POINTER(hzlb_dataset), _dp, C.c_uint64,
                                                    C.c_uint64, C.c_uint64, C.c_int, C.c_int,
                                                    C.c_int, _dp]),
@@ -592,6 +597,37 @@ def bootstrap_filter(ds: dict, p: Parameters, particles: int, seed: int,
                      recs[i].effective_particles, recs[i].maximum_weight] for i in range(k)])
     return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec.reshape(-1, 4),
                 means=means[:k].copy())
+
+
+def save_dataset(ds: dict, path) -> None:
+    """hzl::Dataset::save (src/inference.cpp:214-226): HZL_OBSERVATIONS_V2 text."""
+    dc, keep = _dataset_c(ds)
+    _check(library().hzlb_dataset_save(C.byref(dc), str(path).encode()))
+
+
+def validate_dataset(ds: dict) -> None:
+    """hzl::Dataset::validate (src/inference.cpp:197-213)."""
+    dc, keep = _dataset_c(ds)
+    _check(library().hzlb_dataset_validate(C.byref(dc)))
+
+
+def load_dataset(path) -> dict:
+    """hzl::Dataset::load (src/inference.cpp:227-257): V1 or V2 files, as the dataset dict the
+    drivers take (n, dt, stochastic, forcing_min, forcing_max, steps, x, y, value, sd)."""
+    lib = library()
+    header, count = hzlb_dataset(), C.c_size_t()
+    _check(lib.hzlb_dataset_load(str(path).encode(), C.byref(header), None, 0, C.byref(count)))
+    obs = (hzlb_observation * max(count.value, 1))()
+    _check(lib.hzlb_dataset_load(str(path).encode(), C.byref(header), obs, count.value,
+                                 C.byref(count)))
+    k = count.value
+    return dict(n=header.n, dt=header.dt, stochastic=header.stochastic,
+                forcing_min=header.forcing_min, forcing_max=header.forcing_max,
+                steps=np.array([obs[i].step for i in range(k)], np.uint64),
+                x=np.array([obs[i].x for i in range(k)], np.uint32),
+                y=np.array([obs[i].y for i in range(k)], np.uint32),
+                value=np.array([obs[i].value for i in range(k)]),
+                sd=np.array([obs[i].standard_deviation for i in range(k)]))
 
 
 def particle_log_likelihood(ds: dict, log_parameters, particles: int, seed: int,

@@ -224,6 +224,19 @@ typedef struct {
     size_t count;
     const hzlb_observation *observations;
 } hzlb_dataset;
+/* Dataset files.  hzlb_dataset_save writes HZL_OBSERVATIONS_V2 text, byte for byte as
+ * hzl::Dataset::save (include/hzl/inference.hpp:43-45, src/inference.cpp:214-226);
+ * hzlb_dataset_load reads V1 or V2 files as hzl::Dataset::load (src/inference.cpp:227-257).
+ * Both validate as hzl::Dataset::validate (src/inference.cpp:197-213): HZLB_EINVAL for an
+ * invalid dataset, HZLB_ERUNTIME for a malformed or unwritable file.  load: *count receives
+ * the number of observations; with observations NULL only the header is filled (a first call
+ * to size the buffer), else capacity must hold *count entries and header->observations points
+ * at them. */
+HZLB_API int hzlb_dataset_save(const hzlb_dataset *data, const char *path);
+HZLB_API int hzlb_dataset_load(const char *path, hzlb_dataset *header,
+                               hzlb_observation *observations, size_t capacity, size_t *count);
+/* hzl::Dataset::validate (src/inference.cpp:197-213) alone. */
+HZLB_API int hzlb_dataset_validate(const hzlb_dataset *data);
 /* hzl::FilterRecord without the field (include/hzl/filter.hpp:5-9). */
 typedef struct {
     uint64_t step;

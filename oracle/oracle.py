@@ -258,6 +258,11 @@ class Reference:
         lib.ref_bootstrap_filter.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
                                              u64p, _u32p, _u32p, _dp, _dp, _dp, _u64, _u64, C.c_int,
                                              _dp, u64p, _u64, u64p, _dp, _dp]
+        lib.ref_dataset_save.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
+                                         u64p, _u32p, _u32p, _dp, _dp, C.c_char_p]
+        ip = C.POINTER(C.c_int)
+        lib.ref_dataset_load.argtypes = [C.c_char_p, _u64, ip, _dp, ip, ip, ip, u64p, u64p,
+                                         _u32p, _u32p, _dp, _dp]
         lib.ref_particle_log_likelihood.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
                                                     _u64, u64p, _u32p, _u32p, _dp, _dp, _dp, _u64,
                                                     _u64, _u64, C.c_int, _dp]
@@ -337,6 +342,29 @@ class Reference:
         g = groups.value
         return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec[:g].copy(),
                     means=means[:g].copy())
+
+    def dataset_save(self, ds, path):
+        """Dataset::save (src/inference.cpp:214-226)."""
+        args, keep = self._ds_args(ds)
+        self.check(self.lib.ref_dataset_save(*args, str(path).encode()))
+
+    def dataset_load(self, path, capacity=100000):
+        """Dataset::load (src/inference.cpp:227-257)."""
+        n, stochastic, fmin, fmax = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        dt, count = C.c_double(), _u64()
+        st = np.zeros(capacity, np.uint64)
+        xs = np.zeros(capacity, np.uint32)
+        ys = np.zeros(capacity, np.uint32)
+        vals = np.zeros(capacity)
+        sds = np.zeros(capacity)
+        self.check(self.lib.ref_dataset_load(
+            str(path).encode(), capacity, C.byref(n), C.byref(dt), C.byref(stochastic),
+            C.byref(fmin), C.byref(fmax), C.byref(count), st.ctypes.data_as(C.POINTER(_u64)),
+            xs.ctypes.data_as(_u32p), ys.ctypes.data_as(_u32p), _ptr(vals), _ptr(sds)))
+        k = count.value
+        return dict(n=n.value, dt=dt.value, stochastic=stochastic.value, forcing_min=fmin.value,
+                    forcing_max=fmax.value, steps=st[:k].copy(), x=xs[:k].copy(),
+                    y=ys[:k].copy(), value=vals[:k].copy(), sd=sds[:k].copy())
 
     def particle_log_likelihood(self, ds, q, particles, seed, replicates=None):
         """particle_log_likelihood, or averaged_particle_log_likelihood when replicates is

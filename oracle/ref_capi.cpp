@@ -247,6 +247,47 @@ int ref_bootstrap_filter(int n, double dt, int stochastic, int fmin, int fmax,
     });
 }
 
+// Dataset::save / Dataset::load
+int ref_dataset_save(int n, double dt, int stochastic, int fmin, int fmax, unsigned long long nobs,
+                     const unsigned long long *steps, const unsigned *xs, const unsigned *ys,
+                     const double *values, const double *sds, const char *path) {
+    return guarded([&] {
+        hzl::Dataset d;
+        d.n = static_cast<std::size_t>(n);
+        d.dt = dt;
+        d.stochastic = stochastic != 0;
+        d.forcing_min = fmin;
+        d.forcing_max = fmax;
+        for (unsigned long long i = 0; i < nobs; ++i)
+            d.observations.push_back({steps[i], xs[i], ys[i], values[i], sds[i]});
+        d.save(path);
+    });
+}
+int ref_dataset_load(const char *path, unsigned long long capacity, int *n, double *dt,
+                     int *stochastic, int *fmin, int *fmax, unsigned long long *count,
+                     unsigned long long *steps, unsigned *xs, unsigned *ys, double *values,
+                     double *sds) {
+    return guarded([&] {
+        const auto d = hzl::Dataset::load(path);
+        if (d.observations.size() > capacity)
+            throw std::invalid_argument("observation buffer too small");
+        *n = static_cast<int>(d.n);
+        *dt = d.dt;
+        *stochastic = d.stochastic ? 1 : 0;
+        *fmin = d.forcing_min;
+        *fmax = d.forcing_max;
+        *count = d.observations.size();
+        for (std::size_t i = 0; i < d.observations.size(); ++i) {
+            const auto &o = d.observations[i];
+            steps[i] = o.step;
+            xs[i] = static_cast<unsigned>(o.x);
+            ys[i] = static_cast<unsigned>(o.y);
+            values[i] = o.value;
+            sds[i] = o.standard_deviation;
+        }
+    });
+}
+
 // particle_log_likelihood (averaged = 0) / averaged_particle_log_likelihood (averaged = 1)
 int ref_particle_log_likelihood(int n, double dt, int stochastic, int fmin, int fmax,
                                 unsigned long long nobs, const unsigned long long *steps,

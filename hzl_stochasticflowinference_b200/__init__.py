@@ -155,6 +155,23 @@ def library() -> C.CDLL:
                                             _dp, C.POINTER(C.c_uint64),
                                             C.POINTER(hzlb_filter_record), C.c_size_t,
                                             C.POINTER(C.c_size_t), _dp]),
+        "hzlb_synthetic_observations": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters),
+                                                  C.c_double, C.c_uint64, C.c_uint64,
+                                                  C.c_double, C.c_uint64, C.c_int, C.c_int,
+                                                  C.POINTER(hzlb_dataset),
+                                                  C.POINTER(hzlb_observation), C.c_size_t,
+                                                  C.POINTER(C.c_size_t), _dp]),
+        "hzlb_solvers_create": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters),
+                                          C.POINTER(C.c_uint64), C.c_uint64, C.c_char_p, C.c_int,
+                                          C.c_int, C.POINTER(vp)]),
+        "hzlb_solvers_load": (C.c_int, [C.POINTER(C.c_char_p), C.c_uint64, C.c_int, C.c_int,
+                                        C.POINTER(vp)]),
+        "hzlb_solvers_destroy": (None, [vp]),
+        "hzlb_solvers_step": (C.c_int, [vp, C.c_double, C.c_uint64]),
+        "hzlb_solvers_diagnostics": (C.c_int, [vp, _dp]),
+        "hzlb_solvers_coefficients": (C.c_int, [vp, _dp, _dp]),
+        "hzlb_solvers_save": (C.c_int, [vp, C.c_uint64, C.c_char_p]),
+        "hzlb_solvers_shape": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_uint64)]),
         "hzlb_dataset_save": (C.c_int, [C.POINTER(hzlb_dataset), C.c_char_p]),
         "hzlb_dataset_validate": (C.c_int, [C.POINTER(hzlb_dataset)]),
         "hzlb_dataset_load": (C.c_int, [C.c_char_p, C.POINTER(hzlb_dataset),
@@ -597,6 +614,90 @@ def bootstrap_filter(ds: dict, p: Parameters, particles: int, seed: int,
                      recs[i].effective_particles, recs[i].maximum_weight] for i in range(k)])
     return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec.reshape(-1, 4),
                 means=means[:k].copy())
+
+
+def synthetic_observations(n: int, truth: Parameters, dt: float, steps: int, every: int,
+                           noise: float, seed: int, precision: int = 8, device: int = 0,
+                           truth_fields: bool = False):
+    """hzl::synthetic_observations (src/inference.cpp:258-288) with the truth run on the
+    device: the dataset dict the drivers take, and with truth_fields the (steps // every, n, n)
+    physical vorticity at the observation times as a second value."""
+    lib = library()
+    pc = truth.to_c()
+    header, count = hzlb_dataset(), C.c_size_t()
+    _check(lib.hzlb_synthetic_observations(n, C.byref(pc), dt, steps, every, noise, seed,
+                                           precision, device, C.byref(header), None, 0,
+                                           C.byref(count), None))
+    k = count.value
+    obs = (hzlb_observation * max(k, 1))()
+    fields = np.zeros((k // 8, n, n)) if truth_fields else None
+    _check(lib.hzlb_synthetic_observations(
+        n, C.byref(pc), dt, steps, every, noise, seed, precision, device, C.byref(header), obs,
+        k, C.byref(count), _p(fields) if truth_fields else None))
+    ds = dict(n=header.n, dt=header.dt, stochastic=header.stochastic,
+              forcing_min=header.forcing_min, forcing_max=header.forcing_max,
+              steps=np.array([obs[i].step for i in range(k)], np.uint64),
+              x=np.array([obs[i].x for i in range(k)], np.uint32),
+              y=np.array([obs[i].y for i in range(k)], np.uint32),
+              value=np.array([obs[i].value for i in range(k)]),
+              sd=np.array([obs[i].standard_deviation for i in range(k)]))
+    return (ds, fields) if truth_fields else ds
+
+
+class Solvers:
+    """A set of hzl::Solver instances (src/solver.cpp:120-254) advanced together on the device,
+    each savable as an HZL_CHECKPOINT_V1 file (Solver::save / Solver::load,
+    src/solver.cpp:434-491).  Solver i is Solver(n, p, seeds[i]) initialised with `initial`;
+    Solvers.load restores a set from checkpoint files written by either library."""
+
+    def __init__(self, n: int, p: Parameters, seeds, initial: str = "multimode",
+                 precision: int = 8, device: int = 0):
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+        self._h = C.c_void_p()
+        pc = p.to_c()
+        _check(library().hzlb_solvers_create(n, C.byref(pc),
+                                             seeds.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                             len(seeds), initial.encode(), precision, device,
+                                             C.byref(self._h)))
+        self.n, self.count = n, len(seeds)
+
+    @classmethod
+    def load(cls, paths, precision: int = 8, device: int = 0) -> "Solvers":
+        arr = (C.c_char_p * len(paths))(*[str(p).encode() for p in paths])
+        self = cls.__new__(cls)
+        self._h = C.c_void_p()
+        _check(library().hzlb_solvers_load(arr, len(paths), precision, device, C.byref(self._h)))
+        n, count = C.c_int(), C.c_uint64()
+        _check(library().hzlb_solvers_shape(self._h, C.byref(n), C.byref(count)))
+        self.n, self.count = n.value, count.value
+        return self
+
+    def step(self, dt: float, steps: int = 1) -> None:
+        _check(library().hzlb_solvers_step(self._h, dt, steps))
+
+    def diagnostics(self) -> np.ndarray:
+        out = np.zeros((self.count, 6))
+        _check(library().hzlb_solvers_diagnostics(self._h, _p(out)))
+        return out
+
+    def coefficients(self):
+        """(omega, latent forcing), each (count, n, n) complex over the whole spectrum."""
+        w = np.zeros((self.count, self.n, self.n), np.complex128)
+        f = np.zeros_like(w)
+        _check(library().hzlb_solvers_coefficients(self._h, w.view(np.float64).ctypes.data_as(_dp),
+                                                   f.view(np.float64).ctypes.data_as(_dp)))
+        return w, f
+
+    def save(self, member: int, path) -> None:
+        _check(library().hzlb_solvers_save(self._h, member, str(path).encode()))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().hzlb_solvers_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def save_dataset(ds: dict, path) -> None:

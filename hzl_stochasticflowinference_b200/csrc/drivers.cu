@@ -15,8 +15,12 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
 #include <limits>
 #include <random>
+#include <sstream>
+#include <string>
 
 namespace hzlb {
 namespace {
@@ -50,6 +54,13 @@ class NormalStream {
         spare_ = r * std::sin(angle);
         has_spare_ = true;
         return r * std::cos(angle);
+    }
+    // checkpoint text of the stream (solver.cpp:54-60): the engine's standard textual state,
+    // then the cached second normal
+    void write(std::ostream &out) const { out << engine_ << '\n' << has_spare_ << ' ' << spare_ << '\n'; }
+    void read(std::istream &in) {
+        if (!(in >> engine_ >> has_spare_ >> spare_) || !std::isfinite(spare_))
+            raise(HZLB_ERUNTIME, "invalid checkpoint random stream");
     }
 
   private:
@@ -166,6 +177,7 @@ class OuBank {
         midpoint_.swap(mid);
     }
     void reseed(int m, uint64_t seed) { streams_[m] = NormalStream(seed); }
+    NormalStream &stream(int m) { return streams_[m]; }
     std::vector<cd> &values() { return value_; }
     const std::vector<std::pair<int, int>> &modes() const { return modes_; }
 
@@ -367,6 +379,94 @@ void validate_dt(int n, const Params &p, double dt) {
         raise(HZLB_EINVAL, "invalid time step or diffusion stability limit exceeded");
 }
 
+// ---- HZL_CHECKPOINT_V1 (Solver::save / Solver::load, src/solver.cpp:434-491) ----------------
+// One member as the reference's Solver would hold it: n, time, parameters, its OU stream,
+// then omega and the latent forcing over the whole n x n spectrum (y outer, x inner).
+struct Checkpoint {
+    int n = 0;
+    double time = 0;
+    Params p{};
+    NormalStream stream;
+    std::vector<cd> omega, forcing;
+};
+
+void write_checkpoint(const std::string &path, const Checkpoint &c) {
+    std::ofstream out(path);
+    if (!out)
+        raise(HZLB_ERUNTIME, "cannot open checkpoint for writing");
+    out << std::setprecision(std::numeric_limits<double>::max_digits10);
+    out << "HZL_CHECKPOINT_V1\n"
+        << c.n << ' ' << c.time << '\n'
+        << c.p.nu << ' ' << c.p.alpha << ' ' << c.p.sigma << ' ' << c.p.tau << ' ' << c.p.kmin
+        << ' ' << c.p.kmax << '\n';
+    c.stream.write(out);
+    for (size_t i = 0; i < c.omega.size(); ++i)
+        out << c.omega[i].real() << ' ' << c.omega[i].imag() << ' ' << c.forcing[i].real() << ' '
+            << c.forcing[i].imag() << '\n';
+    if (!out)
+        raise(HZLB_ERUNTIME, "checkpoint write failed");
+}
+
+bool active_mode(int n, int x, int y) {
+    const int a = wave(x, n), b = wave(y, n);
+    return 3 * std::abs(a) < n && 3 * std::abs(b) < n && (x != 0 || y != 0);
+}
+
+// Solver::load's parse and checks, in its order and with its messages.  The device grid is
+// limited to 512.
+Checkpoint read_checkpoint(const std::string &path) {
+    std::ifstream in(path);
+    std::string magic;
+    size_t n = 0;
+    Checkpoint c;
+    double nu = 0, alpha = 0, sigma = 0, tau = 0;
+    int kmin = 0, kmax = 0;
+    if (!(in >> magic >> n >> c.time >> nu >> alpha >> sigma >> tau >> kmin >> kmax) ||
+        magic != "HZL_CHECKPOINT_V1" || !std::isfinite(c.time) || c.time < 0)
+        raise(HZLB_ERUNTIME, "invalid checkpoint header");
+    if (n < 8 || n > 4096 || (n & (n - 1)))
+        raise(HZLB_EINVAL, "grid must be a power of two between 8 and 4096");
+    c.n = static_cast<int>(n);
+    c.p = Params{nu, alpha, sigma, tau, kmin, kmax};
+    validate_params(c.n, c.p);
+    if (n > 512)
+        raise(HZLB_EINVAL, "grid must be a power of two between 8 and 512");
+    OuBank shell(c.n, c.p, std::vector<uint64_t>{0});   // the forced pairs ("empty forcing shell")
+    c.stream.read(in);
+    const size_t nn = n * n;
+    c.omega.assign(nn, cd(0, 0));
+    c.forcing.assign(nn, cd(0, 0));
+    for (size_t i = 0; i < nn; ++i) {
+        double a = 0, b = 0, f = 0, g = 0;
+        if (!(in >> a >> b >> f >> g) || !std::isfinite(a) || !std::isfinite(b) ||
+            !std::isfinite(f) || !std::isfinite(g))
+            raise(HZLB_ERUNTIME, "invalid checkpoint field");
+        c.omega[i] = cd(a, b);
+        c.forcing[i] = cd(f, g);
+    }
+    std::vector<bool> forced(nn, false);
+    for (const auto &[a, b] : shell.modes()) {
+        const int x = (a + c.n) % c.n, y = (b + c.n) % c.n;
+        forced[static_cast<size_t>(y) * n + x] = true;
+        forced[static_cast<size_t>((c.n - y) % c.n) * n + (c.n - x) % c.n] = true;
+    }
+    for (int y = 0; y < c.n; ++y)
+        for (int x = 0; x < c.n; ++x) {
+            const size_t i = static_cast<size_t>(y) * n + x,
+                         partner = static_cast<size_t>((c.n - y) % c.n) * n + (c.n - x) % c.n;
+            if ((!active_mode(c.n, x, y) && c.omega[i] != cd(0, 0)) ||
+                (!forced[i] && c.forcing[i] != cd(0, 0)) ||
+                std::abs(c.omega[i] - std::conj(c.omega[partner])) >
+                    1e-10 * (1 + std::abs(c.omega[i])) ||
+                c.forcing[i] != std::conj(c.forcing[partner]))
+                raise(HZLB_ERUNTIME, "checkpoint violates spectral constraints");
+        }
+    std::string trailing;
+    if (in >> trailing)
+        raise(HZLB_ERUNTIME, "unexpected checkpoint data");
+    return c;
+}
+
 } // namespace
 } // namespace hzlb
 
@@ -396,7 +496,182 @@ Params to_params(const hzlb_parameters *p) {
 }
 } // namespace
 
+// A set of reference Solvers (one OU stream each) advanced together on the device, with the
+// time each of them would hold (the sum of its steps' dt, as Solver::step accumulates it).
+struct hzlb_solvers {
+    std::unique_ptr<RefEnsemble> e;
+    double time = 0;
+};
+
+namespace {
+void check_grid(int n) {
+    if (n < 8 || n > 512 || (n & (n - 1)))
+        raise(HZLB_EINVAL, "grid must be a power of two between 8 and 512");
+}
+hzlb_solvers &solvers(hzlb_solvers *h) {
+    if (!h || !h->e)
+        raise(HZLB_EINVAL, "null solver handle");
+    return *h;
+}
+// latent forcing of member m over the whole spectrum (the pair's first index, its conjugate at
+// the partner)
+std::vector<cd> full_forcing(RefEnsemble &e, int m) {
+    const int n = e.n;
+    std::vector<cd> f(static_cast<size_t>(n) * n, cd(0, 0));
+    const auto &modes = e.bank.modes();
+    const size_t P = modes.size();
+    for (size_t k = 0; k < P; ++k) {
+        const int x = (modes[k].first + n) % n, y = (modes[k].second + n) % n;
+        const cd v = e.bank.values()[static_cast<size_t>(m) * P + k];
+        f[static_cast<size_t>(y) * n + x] = v;
+        f[static_cast<size_t>((n - y) % n) * n + (n - x) % n] = std::conj(v);
+    }
+    return f;
+}
+} // namespace
+
 extern "C" {
+
+HZLB_API int hzlb_solvers_create(int n, const hzlb_parameters *params, const uint64_t *seeds,
+                                 uint64_t count, const char *initial, int precision, int device,
+                                 hzlb_solvers **out) {
+    return guarded_driver([&] {
+        if (!out || !seeds)
+            raise(HZLB_EINVAL, "null argument");
+        *out = nullptr;
+        if (count == 0 || count > static_cast<uint64_t>(std::numeric_limits<int>::max()))
+            raise(HZLB_EINVAL, "solver count must be positive");
+        const Params p = to_params(params);
+        check_grid(n);
+        validate_params(n, p);
+        const std::string name = initial ? initial : "";
+        if (name != "taylor-green" && name != "multimode" && name != "zero")
+            raise(HZLB_EINVAL, "unknown initial condition");
+        auto h = std::make_unique<hzlb_solvers>();
+        h->e = std::make_unique<RefEnsemble>(n, p, std::vector<uint64_t>(seeds, seeds + count),
+                                             precision, device);
+        h->e->set_initial(name.c_str());
+        *out = h.release();
+    });
+}
+
+HZLB_API int hzlb_solvers_load(const char *const *paths, uint64_t count, int precision,
+                               int device, hzlb_solvers **out) {
+    return guarded_driver([&] {
+        if (!out || !paths)
+            raise(HZLB_EINVAL, "null argument");
+        *out = nullptr;
+        if (count == 0 || count > static_cast<uint64_t>(std::numeric_limits<int>::max()))
+            raise(HZLB_EINVAL, "solver count must be positive");
+        std::vector<Checkpoint> cps;
+        cps.reserve(count);
+        for (uint64_t i = 0; i < count; ++i) {
+            if (!paths[i])
+                raise(HZLB_EINVAL, "null path");
+            cps.push_back(read_checkpoint(paths[i]));
+            const Checkpoint &a = cps.front(), &b = cps.back();
+            if (b.n != a.n || b.time != a.time || b.p.nu != a.p.nu || b.p.alpha != a.p.alpha ||
+                b.p.sigma != a.p.sigma || b.p.tau != a.p.tau || b.p.kmin != a.p.kmin ||
+                b.p.kmax != a.p.kmax)
+                raise(HZLB_EINVAL, "checkpoints of one ensemble must share grid, parameters and time");
+        }
+        const int n = cps[0].n, M = static_cast<int>(count);
+        const size_t nn = static_cast<size_t>(n) * n;
+        auto h = std::make_unique<hzlb_solvers>();
+        h->e = std::make_unique<RefEnsemble>(n, cps[0].p, std::vector<uint64_t>(count, 0),
+                                             precision, device);
+        RefEnsemble &e = *h->e;
+        std::vector<double> spectra(2 * nn * count);
+        for (int m = 0; m < M; ++m)
+            std::memcpy(spectra.data() + 2 * nn * m, cps[m].omega.data(), sizeof(cd) * nn);
+        e.engine->set_state(spectra.data(), 0, M);
+        const auto &modes = e.bank.modes();
+        const size_t P = modes.size();
+        for (int m = 0; m < M; ++m) {
+            for (size_t k = 0; k < P; ++k) {
+                const int x = (modes[k].first + n) % n, y = (modes[k].second + n) % n;
+                e.bank.values()[static_cast<size_t>(m) * P + k] = cps[m].forcing[static_cast<size_t>(y) * n + x];
+            }
+            e.bank.stream(m) = cps[m].stream;
+        }
+        h->time = cps[0].time;
+        e.engine->set_time(h->time, 0);
+        *out = h.release();
+    });
+}
+
+HZLB_API void hzlb_solvers_destroy(hzlb_solvers *h) { delete h; }
+
+HZLB_API int hzlb_solvers_step(hzlb_solvers *h, double dt, uint64_t steps) {
+    return guarded_driver([&] {
+        hzlb_solvers &s = solvers(h);
+        validate_dt(s.e->n, s.e->p, dt);
+        for (uint64_t i = 0; i < steps; ++i) {
+            s.e->step(dt);
+            s.time += dt;
+        }
+        s.e->check_status();
+    });
+}
+
+HZLB_API int hzlb_solvers_diagnostics(hzlb_solvers *h, double *out) {
+    return guarded_driver([&] {
+        hzlb_solvers &s = solvers(h);
+        if (!out)
+            raise(HZLB_EINVAL, "null output");
+        s.e->upload_current_forcing();
+        s.e->engine->diagnostics(out);
+    });
+}
+
+HZLB_API int hzlb_solvers_coefficients(hzlb_solvers *h, double *omega, double *forcing) {
+    return guarded_driver([&] {
+        hzlb_solvers &s = solvers(h);
+        const size_t nn = static_cast<size_t>(s.e->n) * s.e->n;
+        if (omega)
+            s.e->engine->get_state(omega, 0, s.e->M);
+        if (forcing)
+            for (int m = 0; m < s.e->M; ++m) {
+                const auto f = full_forcing(*s.e, m);
+                std::memcpy(forcing + 2 * nn * m, f.data(), sizeof(cd) * nn);
+            }
+    });
+}
+
+HZLB_API int hzlb_solvers_shape(hzlb_solvers *h, int *n, uint64_t *count) {
+    return guarded_driver([&] {
+        hzlb_solvers &s = solvers(h);
+        if (!n || !count)
+            raise(HZLB_EINVAL, "null output");
+        *n = s.e->n;
+        *count = static_cast<uint64_t>(s.e->M);
+    });
+}
+
+HZLB_API int hzlb_solvers_save(hzlb_solvers *h, uint64_t member, const char *path) {
+    return guarded_driver([&] {
+        hzlb_solvers &s = solvers(h);
+        if (!path)
+            raise(HZLB_EINVAL, "null path");
+        if (member >= static_cast<uint64_t>(s.e->M))
+            raise(HZLB_EINVAL, "member out of range");
+        const int n = s.e->n, m = static_cast<int>(member);
+        const size_t nn = static_cast<size_t>(n) * n;
+        Checkpoint c;
+        c.n = n;
+        c.time = s.time;
+        c.p = s.e->p;
+        c.stream = s.e->bank.stream(m);
+        c.omega.resize(nn);
+        s.e->engine->get_state(reinterpret_cast<double *>(c.omega.data()), m, 1);
+        for (int y = 0; y < n; ++y)   // inactive modes are exactly zero in a Solver
+            for (int x = 0; x < n; ++x)
+                if (!active_mode(n, x, y))
+                    c.omega[static_cast<size_t>(y) * n + x] = cd(0, 0);
+        c.forcing = full_forcing(*s.e, m);
+        write_checkpoint(path, c);
+    });
+}
 
 HZLB_API int hzlb_run_ensemble(int n, const hzlb_parameters *params, double dt, uint64_t steps,
                                uint64_t count, uint64_t seed, int precision, int device,
@@ -419,6 +694,70 @@ HZLB_API int hzlb_run_ensemble(int n, const hzlb_parameters *params, double dt, 
         e.check_status();
         e.upload_current_forcing();
         e.engine->diagnostics(out);
+    });
+}
+
+// hzl::synthetic_observations(n, dt, steps, every, truth, noise, seed, truth_fields)
+// (src/inference.cpp:258-288): one truth member from "multimode" with OU forcing from
+// stream_seed(seed, 0), advanced on the device; every `every` steps, 8 point observations at
+// x = (j n/8 + 1) mod n, y = (j^2 + 3j + 2) mod n of the physical vorticity plus noise x
+// NormalStream(stream_seed(seed, 1)).  With observations NULL only *count and the header are
+// filled (a sizing call; nothing runs).
+HZLB_API int hzlb_synthetic_observations(int n, const hzlb_parameters *truth, double dt,
+                                         uint64_t steps, uint64_t every, double noise,
+                                         uint64_t seed, int precision, int device,
+                                         hzlb_dataset *header, hzlb_observation *observations,
+                                         size_t capacity, size_t *count, double *truth_fields) {
+    return guarded_driver([&] {
+        if (!header || !count)
+            raise(HZLB_EINVAL, "null output");
+        if (every == 0 || steps < every || !std::isfinite(noise) || noise <= 0)
+            raise(HZLB_EINVAL, "observation experiment requires steps >= every and positive noise");
+        const Params p = to_params(truth);
+        if (n < 8 || n > 512 || (n & (n - 1)))
+            raise(HZLB_EINVAL, "grid must be a power of two between 8 and 512");
+        validate_params(n, p);
+        validate_dt(n, p, dt);
+        if (n < 16)   // the reference's closing Dataset::validate
+            raise(HZLB_EINVAL, "invalid observation dataset");
+        const uint64_t groups = steps / every;
+        const size_t total = static_cast<size_t>(groups) * 8;
+        *count = total;
+        if (observations && capacity < total)
+            raise(HZLB_EINVAL, "observation buffer too small");
+        header->n = n;
+        header->dt = dt;
+        header->stochastic = p.sigma > 0 ? 1 : 0;
+        header->forcing_min = p.kmin;
+        header->forcing_max = p.kmax;
+        header->count = observations ? total : 0;
+        header->observations = observations;
+        if (!observations)
+            return;
+        RefEnsemble e(n, p, std::vector<uint64_t>{stream_seed(seed, 0)}, precision, device);
+        e.set_initial("multimode");
+        NormalStream random(stream_seed(seed, 1));
+        uint32_t xs[8], ys[8];
+        for (uint32_t j = 0; j < 8; ++j) {
+            xs[j] = static_cast<uint32_t>((j * static_cast<uint32_t>(n) / 8 + 1) % n);
+            ys[j] = static_cast<uint32_t>((j * j + 3 * j + 2) % static_cast<uint32_t>(n));
+        }
+        const size_t nn = static_cast<size_t>(n) * n;
+        size_t k = 0, g = 0;
+        for (uint64_t step = 1; step <= steps; ++step) {
+            e.step(dt);
+            if (step % every == 0) {
+                e.check_status();
+                double values[8];
+                e.engine->observe(xs, ys, 8, values);
+                if (truth_fields)
+                    e.engine->physical(truth_fields + g * nn);
+                for (int j = 0; j < 8; ++j)
+                    observations[k++] = {step, xs[j], ys[j], values[j] + noise * random(), noise};
+                ++g;
+            }
+        }
+        e.check_status();
     });
 }
 

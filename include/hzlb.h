@@ -261,6 +261,45 @@ typedef struct {
 HZLB_API int hzlb_run_ensemble(int n, const hzlb_parameters *params, double dt, uint64_t steps,
                                uint64_t count, uint64_t seed, int precision, int device,
                                double *out);
+/* A set of hzl::Solver instances advanced together on the device, with HZL_CHECKPOINT_V1
+ * files for each (include/hzl/solver.hpp:61-99, src/solver.cpp:120-138, 204-254, 434-491; RK4, the
+ * reference's default integrator).
+ * create: solver i is Solver(n, p, seeds[i]) after initialize(initial), initial one of
+ * "taylor-green", "multimode", "zero" (hzl::ensemble's members use seeds[i] =
+ * stream_seed(seed, i); the simulate command one solver with the seed itself).
+ * load: Solver::load of each file, with its checks and messages (HZLB_ERUNTIME for a malformed
+ * or inconsistent file); the files of one set must share grid, parameters and time.
+ * step: Solver::step(dt) `steps` times for every solver; the diffusion bound is checked first
+ * and the advective (CFL) bound after the steps (the reference checks it before each step).
+ * diagnostics: count x {time, energy, enstrophy, dissipation, injection, cfl_rate}.
+ * coefficients: count x n*n complex omega and/or latent forcing (either may be NULL).
+ * save: Solver::save of one solver; the random stream and forcing lines are the reference's
+ * exactly, omega equals the reference's to FP64 roundoff. */
+typedef struct hzlb_solvers hzlb_solvers;
+HZLB_API int hzlb_solvers_create(int n, const hzlb_parameters *params, const uint64_t *seeds,
+                                 uint64_t count, const char *initial, int precision, int device,
+                                 hzlb_solvers **out);
+HZLB_API int hzlb_solvers_load(const char *const *paths, uint64_t count, int precision,
+                               int device, hzlb_solvers **out);
+HZLB_API void hzlb_solvers_destroy(hzlb_solvers *h);
+HZLB_API int hzlb_solvers_step(hzlb_solvers *h, double dt, uint64_t steps);
+HZLB_API int hzlb_solvers_diagnostics(hzlb_solvers *h, double *out);
+HZLB_API int hzlb_solvers_coefficients(hzlb_solvers *h, double *omega, double *forcing);
+HZLB_API int hzlb_solvers_save(hzlb_solvers *h, uint64_t member, const char *path);
+/* Grid size and number of solvers of a set (no counterpart in the reference). */
+HZLB_API int hzlb_solvers_shape(hzlb_solvers *h, int *n, uint64_t *count);
+/* hzl::synthetic_observations(n, dt, steps, every, truth, noise, seed, truth_fields)
+ * (include/hzl/inference.hpp:47-49, src/inference.cpp:258-288): the truth run on the device.
+ * *count receives 8 x (steps / every); with observations NULL only *count and the header are
+ * filled and nothing runs, else capacity must hold *count entries.  truth_fields (optional):
+ * (steps / every) x n x n doubles, the physical vorticity at each observation time (the real
+ * part of the reference's truth fields).  Observation values equal the reference's to
+ * roundoff in FP64 (precision 8); the noise draws are the reference's exactly. */
+HZLB_API int hzlb_synthetic_observations(int n, const hzlb_parameters *truth, double dt,
+                                         uint64_t steps, uint64_t every, double noise,
+                                         uint64_t seed, int precision, int device,
+                                         hzlb_dataset *header, hzlb_observation *observations,
+                                         size_t capacity, size_t *count, double *truth_fields);
 /* hzl::bootstrap_filter(data, p, particles, seed, retain_states) (include/hzl/filter.hpp:17-18,
  * src/filter.cpp:38-126).  mean_vorticity (optional): capacity x n*n complex, the weighted
  * mean physical vorticity per record. */

@@ -258,6 +258,9 @@ class Reference:
         lib.ref_bootstrap_filter.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
                                              u64p, _u32p, _u32p, _dp, _dp, _dp, _u64, _u64, C.c_int,
                                              _dp, u64p, _u64, u64p, _dp, _dp]
+        lib.ref_solver_save.argtypes = [C.c_void_p, C.c_char_p]
+        lib.ref_solver_load.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+        lib.ref_solver_size.argtypes = [C.c_void_p]
         lib.ref_dataset_save.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
                                          u64p, _u32p, _u32p, _dp, _dp, C.c_char_p]
         ip = C.POINTER(C.c_int)
@@ -288,6 +291,15 @@ class Reference:
     def solver(self, n: int, p6, seed: int) -> "ReferenceSolver":
         return ReferenceSolver(self, n, p6, seed)
 
+    def solver_load(self, path) -> "ReferenceSolver":
+        """Solver::load (src/solver.cpp:453-491)."""
+        h = C.c_void_p()
+        self.check(self.lib.ref_solver_load(str(path).encode(), C.byref(h)))
+        s = ReferenceSolver.__new__(ReferenceSolver)
+        s.r, s.h = self, h
+        s.n = int(self.lib.ref_solver_size(h))
+        return s
+
     def shell_forcing(self, n: int, p6, seed: int) -> "ReferenceShellForcing":
         return ReferenceShellForcing(self, n, p6, seed)
 
@@ -298,7 +310,7 @@ class Reference:
         return out
 
     def synthetic_observations(self, n, dt, steps, every, p6, noise, seed):
-        cap = (steps // every) * 8 + 8
+        cap = (steps // every) * 8 + 8 if every else 8
         count = _u64()
         st = np.zeros(cap, np.uint64)
         xs = np.zeros(cap, np.uint32)
@@ -437,6 +449,10 @@ class ReferenceSolver:
 
     def initialize(self, name: str):
         self.r.check(self.r.lib.ref_solver_initialize(self.h, name.encode()))
+
+    def save(self, path):
+        """Solver::save (src/solver.cpp:434-452)."""
+        self.r.check(self.r.lib.ref_solver_save(self.h, str(path).encode()))
 
     def initialize_physical(self, field: np.ndarray):
         a = np.ascontiguousarray(field, dtype=np.complex128)

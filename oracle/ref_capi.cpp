@@ -156,6 +156,13 @@ int ref_solver_drift(void *h, const double *state, double *out) {
         from_field(s->drift(to_field(state, s->size() * s->size())), out);
     });
 }
+int ref_solver_save(void *h, const char *path) {
+    return guarded([&] { static_cast<hzl::Solver *>(h)->save(path); });
+}
+int ref_solver_load(const char *path, void **out) {
+    return guarded([&] { *out = new hzl::Solver(hzl::Solver::load(path)); });
+}
+int ref_solver_size(void *h) { return static_cast<int>(static_cast<hzl::Solver *>(h)->size()); }
 int ref_solver_reseed_future(void *h, unsigned long long seed) {
     return guarded([&] { static_cast<hzl::Solver *>(h)->reseed_future(seed); });
 }

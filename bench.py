@@ -289,6 +289,60 @@ def mixed_experiment() -> dict:
         return {"error": f"{type(exc).__name__}: {exc}"}
 
 
+LIKELIHOOD_CASES = [
+    # name, n, dt, steps, every, noise, particles, replicates, reference sample (particles, replicates)
+    ("calibration objective", 16, 0.01, 150, 10, 0.02, 32, 3, (32, 3)),
+    ("batched replicates", 64, 0.005, 150, 10, 0.02, 256, 8, (32, 1)),
+]
+
+
+def likelihood_experiment(cpu: bool) -> dict:
+    """averaged_particle_log_likelihood (src/filter.cpp:150-165) on a synthetic stochastic
+    dataset made by the device truth run (synthetic_observations, the reference's defaults:
+    truth nu 0.03, alpha 0.1, sigma 0.2, tau 0.5, shell 2..3, 8 sites every 10 steps): every
+    replicate's particles advance as one ensemble.  Seconds per likelihood evaluation (wall
+    clock, host OU forcing and resampling included) against the reference library's own
+    function on the host (one thread per call, as it runs), timed on a bounded sample of
+    particles x replicates and scaled to the workload (its cost is linear in both)."""
+    try:
+        import hzl_stochasticflowinference_b200 as hz
+        truth = hz.Parameters(0.03, 0.1, 0.2, 0.5, 2, 3)
+        q = np.log([0.03, 0.1, 0.2, 0.5])
+        out = []
+        for name, n, dt, steps, every, noise, P, R, (rp, rr) in LIKELIHOOD_CASES:
+            ds = hz.synthetic_observations(n, truth, dt, steps, every, noise, 314159)
+            hz.averaged_particle_log_likelihood(ds, q, P, R, 123)   # set-up, first-touch
+            reps = 3
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                ll = hz.averaged_particle_log_likelihood(ds, q, P, R, 123)
+            sec = (time.perf_counter() - t0) / reps
+            row = {"workload": f"{name}: {n}^2, {steps} steps of dt {dt}, {len(ds['steps'])} "
+                               f"observations, {P} particles x {R} replicates",
+                   "seconds": sec, "member_steps_per_s": P * R * steps / sec,
+                   "log_likelihood": ll}
+            if cpu:
+                try:
+                    from oracle.oracle import Reference
+                    ref = Reference()
+                    t0 = time.perf_counter()
+                    ref_ll = ref.particle_log_likelihood(ds, q, rp, 123, replicates=rr)
+                    rs = (time.perf_counter() - t0) * (P * R) / (rp * rr)
+                    row["reference_cpu"] = {
+                        "seconds": rs, "member_steps_per_s": P * R * steps / rs,
+                        "sample": f"{rp} particles x {rr} replicates, scaled by {P * R // (rp * rr)}",
+                        "cores": 1}
+                    row["speedup"] = rs / sec
+                    if (rp, rr) == (P, R):
+                        row["reference_log_likelihood"] = ref_ll
+                except Exception as exc:
+                    row["reference_cpu"] = {"sample": f"unavailable: {exc}"}
+            out.append(row)
+        return {"cases": out}
+    except Exception as exc:   # report, never lose the main line
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def learned_experiment() -> dict:
     """The learned-forecast EnKF twin experiment (hzl_stochasticflowinference_b200.learned) at
     its full size; wall-clock per cycle (forecast + analysis + fallback) with the GPU
@@ -329,6 +383,9 @@ def run_case(case: str, steps: int, warmup: int) -> None:
     steps, warmup = max(1, min(steps, 10)), max(1, min(warmup, 3))
     ev = lambda: torch.cuda.Event(enable_timing=True)   # noqa: E731
     out = {"case": case}
+    if case == "likelihood":
+        print(json.dumps({"case": case, **likelihood_experiment(True)}), flush=True)
+        return
     if case == "gemm":
         lib = hz.library()
         fn = lib.hzlb_gemm
@@ -397,7 +454,7 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
-    ap.add_argument("--case", choices=["gemm", "enkf", "learned"])
+    ap.add_argument("--case", choices=["gemm", "enkf", "learned", "likelihood"])
     args = ap.parse_args()
     if args.case:
         run_case(args.case, args.steps, args.warmup)
@@ -515,7 +572,7 @@ def main():
                    "sample": f"unavailable: {exc}"}
 
     ens.close()
-    learned = gpu_ref = fp64 = filters = mixed = None
+    learned = gpu_ref = fp64 = filters = mixed = likelihood = None
     if rank == 0 and world == 1:
         fp64 = fp64_sample(hz, torch, N)
         if not args.no_cpu_baseline:
@@ -524,6 +581,7 @@ def main():
             learned = learned_experiment()
             filters = filter_experiment(not args.no_cpu_baseline)
             mixed = mixed_experiment()
+            likelihood = likelihood_experiment(not args.no_cpu_baseline)
 
     if rank == 0:
         out = {
@@ -553,6 +611,7 @@ def main():
             "learned": learned,
             "filters": filters,
             "mixed": mixed,
+            "likelihood": likelihood,
         }
         print(json.dumps(out), flush=True)
     if pg:

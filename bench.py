@@ -343,6 +343,49 @@ def likelihood_experiment(cpu: bool) -> dict:
         return {"error": f"{type(exc).__name__}: {exc}"}
 
 
+def tangent_experiment(cpu: bool, n: int = 128, count: int = 1024, sample: int = 16) -> dict:
+    """Batched Solver::linearized_drift / adjoint_drift (src/solver.cpp:264-324), FP64, `count`
+    (state, field) pairs of n^2 spectra per call from host memory (wall clock, transfers
+    included), against the reference library's own functions on the host (one thread, one pair
+    per call as its adjoint loop calls them), timed on `sample` pairs and scaled to `count`."""
+    try:
+        import hzl_stochasticflowinference_b200 as hz
+        rng = np.random.default_rng(SEED)
+        k = np.fft.fftfreq(n, 1 / n).astype(int)
+        mask = (3 * np.abs(k)[None, :] < n) & (3 * np.abs(k)[:, None] < n)
+        mask[0, 0] = False
+
+        def fields(c):
+            return np.fft.fft2(rng.normal(size=(c, n, n)), axes=(1, 2)) / n ** 2 * mask
+
+        w, d = fields(count), fields(count)
+        p = hz.Parameters(0.02, 0.1, 0.2, 0.5, 2, 3)
+        out = {"workload": f"{count} pairs at {n}^2 per call, FP64, host arrays"}
+        for name, fn in (("linearized_drift", hz.linearized_drift), ("adjoint_drift", hz.adjoint_drift)):
+            fn(n, p, w[:8], d[:8])
+            t0 = time.perf_counter()
+            fn(n, p, w, d)
+            sec = time.perf_counter() - t0
+            row = {"seconds": sec, "pairs_per_s": count / sec}
+            if cpu:
+                try:
+                    from oracle.oracle import Reference, params6
+                    s = Reference().solver(n, params6(0.02, 0.1, 0.2, 0.5, 2, 3), 1)
+                    t0 = time.perf_counter()
+                    for i in range(sample):
+                        getattr(s, name)(w[i], d[i])
+                    rs = (time.perf_counter() - t0) / sample
+                    row["reference_cpu"] = {"pairs_per_s": 1 / rs, "cores": 1,
+                                            "sample": f"{sample} pairs, one call each"}
+                    row["speedup"] = (count / sec) * rs
+                except Exception as exc:
+                    row["reference_cpu"] = {"sample": f"unavailable: {exc}"}
+            out[name] = row
+        return out
+    except Exception as exc:   # report, never lose the main line
+        return {"error": f"{type(exc).__name__}: {exc}"}
+
+
 def learned_experiment() -> dict:
     """The learned-forecast EnKF twin experiment (hzl_stochasticflowinference_b200.learned) at
     its full size; wall-clock per cycle (forecast + analysis + fallback) with the GPU
@@ -385,6 +428,9 @@ def run_case(case: str, steps: int, warmup: int) -> None:
     out = {"case": case}
     if case == "likelihood":
         print(json.dumps({"case": case, **likelihood_experiment(True)}), flush=True)
+        return
+    if case == "tangent":
+        print(json.dumps({"case": case, **tangent_experiment(True)}), flush=True)
         return
     if case == "gemm":
         lib = hz.library()
@@ -454,7 +500,7 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
-    ap.add_argument("--case", choices=["gemm", "enkf", "learned", "likelihood"])
+    ap.add_argument("--case", choices=["gemm", "enkf", "learned", "likelihood", "tangent"])
     args = ap.parse_args()
     if args.case:
         run_case(args.case, args.steps, args.warmup)
@@ -572,7 +618,7 @@ def main():
                    "sample": f"unavailable: {exc}"}
 
     ens.close()
-    learned = gpu_ref = fp64 = filters = mixed = likelihood = None
+    learned = gpu_ref = fp64 = filters = mixed = likelihood = tangent = None
     if rank == 0 and world == 1:
         fp64 = fp64_sample(hz, torch, N)
         if not args.no_cpu_baseline:
@@ -582,6 +628,7 @@ def main():
             filters = filter_experiment(not args.no_cpu_baseline)
             mixed = mixed_experiment()
             likelihood = likelihood_experiment(not args.no_cpu_baseline)
+            tangent = tangent_experiment(not args.no_cpu_baseline)
 
     if rank == 0:
         out = {
@@ -612,6 +659,7 @@ def main():
             "filters": filters,
             "mixed": mixed,
             "likelihood": likelihood,
+            "tangent": tangent,
         }
         print(json.dumps(out), flush=True)
     if pg:

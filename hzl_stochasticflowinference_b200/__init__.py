@@ -161,6 +161,10 @@ def library() -> C.CDLL:
                                                   C.POINTER(hzlb_dataset),
                                                   C.POINTER(hzlb_observation), C.c_size_t,
                                                   C.POINTER(C.c_size_t), _dp]),
+        "hzlb_linearized_drift": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), _dp, _dp,
+                                            C.c_uint64, C.c_int, _dp]),
+        "hzlb_adjoint_drift": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), _dp, _dp,
+                                         C.c_uint64, C.c_int, _dp]),
         "hzlb_solvers_create": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters),
                                           C.POINTER(C.c_uint64), C.c_uint64, C.c_char_p, C.c_int,
                                           C.c_int, C.POINTER(vp)]),
@@ -642,6 +646,31 @@ def synthetic_observations(n: int, truth: Parameters, dt: float, steps: int, eve
               value=np.array([obs[i].value for i in range(k)]),
               sd=np.array([obs[i].standard_deviation for i in range(k)]))
     return (ds, fields) if truth_fields else ds
+
+
+def _drift_pairs(fn, n, p, states, second, device):
+    a = np.ascontiguousarray(states, dtype=np.complex128).reshape(-1, n, n)
+    b = np.ascontiguousarray(second, dtype=np.complex128).reshape(-1, n, n)
+    if a.shape != b.shape:
+        raise HzlbInvalidArgument(HZLB_EINVAL, "drift state size mismatch")
+    out = np.zeros_like(a)
+    pc = p.to_c()
+    _check(fn(n, C.byref(pc), a.view(np.float64).ctypes.data_as(_dp),
+              b.view(np.float64).ctypes.data_as(_dp), a.shape[0], device,
+              out.view(np.float64).ctypes.data_as(_dp)))
+    return out
+
+
+def linearized_drift(n: int, p: Parameters, states, directions, device: int = 0) -> np.ndarray:
+    """hzl::Solver::linearized_drift (src/solver.cpp:264-292) for a batch of (state,
+    direction) pairs, (count, n, n) complex spectra each."""
+    return _drift_pairs(library().hzlb_linearized_drift, n, p, states, directions, device)
+
+
+def adjoint_drift(n: int, p: Parameters, states, cotangents, device: int = 0) -> np.ndarray:
+    """hzl::Solver::adjoint_drift (src/solver.cpp:293-324) for a batch of (state, cotangent)
+    pairs, (count, n, n) complex spectra each."""
+    return _drift_pairs(library().hzlb_adjoint_drift, n, p, states, cotangents, device)
 
 
 class Solvers:

@@ -261,6 +261,20 @@ typedef struct {
 HZLB_API int hzlb_run_ensemble(int n, const hzlb_parameters *params, double dt, uint64_t steps,
                                uint64_t count, uint64_t seed, int precision, int device,
                                double *out);
+/* hzl::Solver::linearized_drift(state, direction) and Solver::adjoint_drift(state, cotangent)
+ * (include/hzl/solver.hpp:70-71, src/solver.cpp:264-324) for `count` pairs at once, FP64 on
+ * the device: states, directions / cotangents and out are count x n*n complex spectra in the
+ * reference's Field layout (y outer, x inner).  The Hermitian part of each input on the active
+ * (dealiased) modes is used, which is what the reference reads of the projected fields it
+ * passes (its physical fields keep their real part only); out is zero off the active modes.
+ * params: the solver's parameters (viscosity and friction enter; the forcing shell is
+ * validated as the Solver constructor does). */
+HZLB_API int hzlb_linearized_drift(int n, const hzlb_parameters *params, const double *states,
+                                   const double *directions, uint64_t count, int device,
+                                   double *out);
+HZLB_API int hzlb_adjoint_drift(int n, const hzlb_parameters *params, const double *states,
+                                const double *cotangents, uint64_t count, int device,
+                                double *out);
 /* A set of hzl::Solver instances advanced together on the device, with HZL_CHECKPOINT_V1
  * files for each (include/hzl/solver.hpp:61-99, src/solver.cpp:120-138, 204-254, 434-491; RK4, the
  * reference's default integrator).

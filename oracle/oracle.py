@@ -259,6 +259,8 @@ class Reference:
                                              u64p, _u32p, _u32p, _dp, _dp, _dp, _u64, _u64, C.c_int,
                                              _dp, u64p, _u64, u64p, _dp, _dp]
         lib.ref_solver_save.argtypes = [C.c_void_p, C.c_char_p]
+        lib.ref_solver_linearized_drift.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        lib.ref_solver_adjoint_drift.argtypes = [C.c_void_p, _dp, _dp, _dp]
         lib.ref_solver_load.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
         lib.ref_solver_size.argtypes = [C.c_void_p]
         lib.ref_dataset_save.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
@@ -449,6 +451,22 @@ class ReferenceSolver:
 
     def initialize(self, name: str):
         self.r.check(self.r.lib.ref_solver_initialize(self.h, name.encode()))
+
+    def linearized_drift(self, state, direction):
+        """Solver::linearized_drift (src/solver.cpp:264-292)."""
+        a = np.ascontiguousarray(state, dtype=np.complex128)
+        b = np.ascontiguousarray(direction, dtype=np.complex128)
+        out = np.zeros((self.n, self.n), np.complex128)
+        self.r.check(self.r.lib.ref_solver_linearized_drift(self.h, _ptr(a), _ptr(b), _ptr(out)))
+        return out
+
+    def adjoint_drift(self, state, cotangent):
+        """Solver::adjoint_drift (src/solver.cpp:293-324)."""
+        a = np.ascontiguousarray(state, dtype=np.complex128)
+        b = np.ascontiguousarray(cotangent, dtype=np.complex128)
+        out = np.zeros((self.n, self.n), np.complex128)
+        self.r.check(self.r.lib.ref_solver_adjoint_drift(self.h, _ptr(a), _ptr(b), _ptr(out)))
+        return out
 
     def save(self, path):
         """Solver::save (src/solver.cpp:434-452)."""

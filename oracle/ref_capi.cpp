@@ -156,6 +156,22 @@ int ref_solver_drift(void *h, const double *state, double *out) {
         from_field(s->drift(to_field(state, s->size() * s->size())), out);
     });
 }
+int ref_solver_linearized_drift(void *h, const double *state, const double *direction,
+                                double *out) {
+    return guarded([&] {
+        auto *s = static_cast<hzl::Solver *>(h);
+        const auto c = s->size() * s->size();
+        from_field(s->linearized_drift(to_field(state, c), to_field(direction, c)), out);
+    });
+}
+int ref_solver_adjoint_drift(void *h, const double *state, const double *cotangent,
+                             double *out) {
+    return guarded([&] {
+        auto *s = static_cast<hzl::Solver *>(h);
+        const auto c = s->size() * s->size();
+        from_field(s->adjoint_drift(to_field(state, c), to_field(cotangent, c)), out);
+    });
+}
 int ref_solver_save(void *h, const char *path) {
     return guarded([&] { static_cast<hzl::Solver *>(h)->save(path); });
 }

@@ -381,9 +381,46 @@ def tangent_experiment(cpu: bool, n: int = 128, count: int = 1024, sample: int =
                 except Exception as exc:
                     row["reference_cpu"] = {"sample": f"unavailable: {exc}"}
             out[name] = row
+        out["likelihood_adjoint"] = adjoint_gradient_sample(cpu)
         return out
     except Exception as exc:   # report, never lose the main line
         return {"error": f"{type(exc).__name__}: {exc}"}
+
+
+def adjoint_gradient_sample(cpu: bool, vectors: int = 64, sample: int = 2) -> dict:
+    """likelihood_adjoint (src/adjoint.cpp:43-161) for `vectors` (log nu, log alpha) points in
+    one call, on a deterministic dataset from the device truth run with the reference's
+    observation defaults (16^2, 150 steps of dt 0.01, 8 sites every 10 steps), checkpoint
+    stride 20; against the reference library's one call per point on one host thread."""
+    import hzl_stochasticflowinference_b200 as hz
+    ds = hz.synthetic_observations(16, hz.Parameters(0.03, 0.1, 0.0, 0.5, 2, 3), 0.01, 150, 10,
+                                   0.02, 314159)
+    rng = np.random.default_rng(SEED)
+    q = np.stack([rng.uniform(np.log(0.01), np.log(0.08), vectors),
+                  rng.uniform(np.log(0.05), np.log(0.3), vectors)], axis=1)
+    hz.likelihood_adjoint(ds, q[:2], 20)
+    t0 = time.perf_counter()
+    got = hz.likelihood_adjoint(ds, q, 20)
+    sec = time.perf_counter() - t0
+    row = {"workload": f"{vectors} parameter vectors per call, 16^2, 150 steps, stride 20",
+           "seconds": sec, "gradients_per_s": vectors / sec,
+           "replayed_steps": int(got[0]["replayed_steps"])}
+    if cpu:
+        try:
+            from oracle.oracle import Reference
+            ref = Reference()
+            t0 = time.perf_counter()
+            for i in range(sample):
+                r = ref.likelihood_adjoint(ds, q[i], 20)
+            rs = (time.perf_counter() - t0) / sample
+            row["reference_cpu"] = {"gradients_per_s": 1 / rs, "cores": 1,
+                                    "sample": f"{sample} points, one call each"}
+            row["speedup"] = (vectors / sec) * rs
+            row["max_rel_gradient_difference_sampled"] = float(np.max(
+                np.abs(got[sample - 1]["gradient"] - r["gradient"]) / np.abs(r["gradient"])))
+        except Exception as exc:
+            row["reference_cpu"] = {"sample": f"unavailable: {exc}"}
+    return row
 
 
 def learned_experiment() -> dict:

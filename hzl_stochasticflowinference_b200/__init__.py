@@ -80,6 +80,12 @@ class hzlb_enkf_record(C.Structure):
                 ("posterior_spread", C.c_double), ("is_forecast", C.c_int)]
 
 
+class hzlb_adjoint_evaluation(C.Structure):
+    _fields_ = [("value", C.c_double), ("gradient", C.c_double * 2),
+                ("checkpoint_fields", C.c_uint64), ("peak_block_fields", C.c_uint64),
+                ("replayed_steps", C.c_uint64)]
+
+
 class HzlbError(RuntimeError):
     """A failure reported through the C ABI (std::runtime_error in the reference)."""
 
@@ -161,6 +167,9 @@ def library() -> C.CDLL:
                                                   C.POINTER(hzlb_dataset),
                                                   C.POINTER(hzlb_observation), C.c_size_t,
                                                   C.POINTER(C.c_size_t), _dp]),
+        "hzlb_likelihood_adjoint": (C.c_int, [C.POINTER(hzlb_dataset), _dp, C.c_uint64,
+                                              C.c_uint64, C.c_int,
+                                              C.POINTER(hzlb_adjoint_evaluation)]),
         "hzlb_linearized_drift": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), _dp, _dp,
                                             C.c_uint64, C.c_int, _dp]),
         "hzlb_adjoint_drift": (C.c_int, [C.c_int, C.POINTER(hzlb_parameters), _dp, _dp,
@@ -646,6 +655,21 @@ def synthetic_observations(n: int, truth: Parameters, dt: float, steps: int, eve
               value=np.array([obs[i].value for i in range(k)]),
               sd=np.array([obs[i].standard_deviation for i in range(k)]))
     return (ds, fields) if truth_fields else ds
+
+
+def likelihood_adjoint(ds: dict, log_parameters, checkpoint_stride: int = 20,
+                       device: int = 0) -> list[dict]:
+    """hzl::likelihood_adjoint (src/adjoint.cpp:43-161) for one or many (log nu, log alpha)
+    vectors at once: objective value, gradient and the checkpoint counters of each."""
+    q = np.ascontiguousarray(log_parameters, dtype=np.float64).reshape(-1, 2)
+    dc, keep = _dataset_c(ds)
+    out = (hzlb_adjoint_evaluation * max(len(q), 1))()
+    _check(library().hzlb_likelihood_adjoint(C.byref(dc), _p(q), len(q), checkpoint_stride,
+                                             device, out))
+    return [dict(value=out[i].value, gradient=np.array(out[i].gradient[:]),
+                 checkpoint_fields=out[i].checkpoint_fields,
+                 peak_block_fields=out[i].peak_block_fields,
+                 replayed_steps=out[i].replayed_steps) for i in range(len(q))]
 
 
 def _drift_pairs(fn, n, p, states, second, device):

@@ -275,6 +275,21 @@ HZLB_API int hzlb_linearized_drift(int n, const hzlb_parameters *params, const d
 HZLB_API int hzlb_adjoint_drift(int n, const hzlb_parameters *params, const double *states,
                                 const double *cotangents, uint64_t count, int device,
                                 double *out);
+/* hzl::AdjointEvaluation (include/hzl/inference.hpp:55-58). */
+typedef struct {
+    double value, gradient[2];
+    uint64_t checkpoint_fields, peak_block_fields, replayed_steps;
+} hzlb_adjoint_evaluation;
+/* hzl::likelihood_adjoint(data, log_parameters, checkpoint_stride) (include/hzl/inference.hpp:
+ * 59-60, src/adjoint.cpp:43-161) for `count` parameter vectors at once (log_parameters: count x
+ * {log nu, log alpha}): the deterministic "multimode" run with checkpoints every
+ * checkpoint_stride steps, the Gaussian objective of the observations and its gradient by the
+ * discrete adjoint of RK4, FP64 on the device.  A vector outside [-12, 0]^2 or past the
+ * explicit diffusion bound gets value +inf as in the reference; the others advance together.
+ * HZLB_EINVAL for stochastic data or a zero stride (the reference's std::invalid_argument). */
+HZLB_API int hzlb_likelihood_adjoint(const hzlb_dataset *data, const double *log_parameters,
+                                     uint64_t count, uint64_t checkpoint_stride, int device,
+                                     hzlb_adjoint_evaluation *out);
 /* A set of hzl::Solver instances advanced together on the device, with HZL_CHECKPOINT_V1
  * files for each (include/hzl/solver.hpp:61-99, src/solver.cpp:120-138, 204-254, 434-491; RK4, the
  * reference's default integrator).

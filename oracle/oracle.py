@@ -263,6 +263,9 @@ class Reference:
         lib.ref_solver_adjoint_drift.argtypes = [C.c_void_p, _dp, _dp, _dp]
         lib.ref_solver_load.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
         lib.ref_solver_size.argtypes = [C.c_void_p]
+        lib.ref_likelihood_adjoint.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int,
+                                               _u64, u64p, _u32p, _u32p, _dp, _dp, _dp, _u64, _dp,
+                                               _dp, u64p]
         lib.ref_dataset_save.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _u64,
                                          u64p, _u32p, _u32p, _dp, _dp, C.c_char_p]
         ip = C.POINTER(C.c_int)
@@ -356,6 +359,19 @@ class Reference:
         g = groups.value
         return dict(log_likelihood=ll.value, resampling_events=ev.value, records=rec[:g].copy(),
                     means=means[:g].copy())
+
+    def likelihood_adjoint(self, ds, q, stride=20):
+        """likelihood_adjoint (src/adjoint.cpp:43-161)."""
+        args, keep = self._ds_args(ds)
+        qa = np.ascontiguousarray(q, dtype=np.float64)
+        value = C.c_double()
+        grad = np.zeros(2)
+        counters = np.zeros(3, np.uint64)
+        self.check(self.lib.ref_likelihood_adjoint(*args, _ptr(qa), stride, C.byref(value),
+                                                   _ptr(grad),
+                                                   counters.ctypes.data_as(C.POINTER(_u64))))
+        return dict(value=value.value, gradient=grad, checkpoint_fields=int(counters[0]),
+                    peak_block_fields=int(counters[1]), replayed_steps=int(counters[2]))
 
     def dataset_save(self, ds, path):
         """Dataset::save (src/inference.cpp:214-226)."""

@@ -270,6 +270,25 @@ int ref_bootstrap_filter(int n, double dt, int stochastic, int fmin, int fmax,
     });
 }
 
+// likelihood_adjoint: value, gradient[2], counters[3]
+int ref_likelihood_adjoint(int n, double dt, int stochastic, int fmin, int fmax,
+                           unsigned long long nobs, const unsigned long long *steps,
+                           const unsigned *xs, const unsigned *ys, const double *values,
+                           const double *sds, const double *q2, unsigned long long stride,
+                           double *value, double *gradient, unsigned long long *counters) {
+    return guarded([&] {
+        const auto d = dataset(static_cast<std::size_t>(n), dt, stochastic, fmin, fmax, nobs, steps,
+                               xs, ys, values, sds);
+        const auto r = hzl::likelihood_adjoint(d, hzl::Vector(q2, q2 + 2), stride);
+        *value = r.objective.value;
+        gradient[0] = r.objective.gradient.size() > 0 ? r.objective.gradient[0] : 0;
+        gradient[1] = r.objective.gradient.size() > 1 ? r.objective.gradient[1] : 0;
+        counters[0] = r.checkpoint_fields;
+        counters[1] = r.peak_block_fields;
+        counters[2] = r.replayed_steps;
+    });
+}
+
 // Dataset::save / Dataset::load
 int ref_dataset_save(int n, double dt, int stochastic, int fmin, int fmax, unsigned long long nobs,
                      const unsigned long long *steps, const unsigned *xs, const unsigned *ys,

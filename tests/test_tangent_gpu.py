@@ -88,3 +88,51 @@ def test_invalid_arguments(hzlb):
     bad[0, 1, 1] = np.nan
     with pytest.raises(hzlb.HzlbInvalidArgument, match="nonfinite"):
         hzlb.linearized_drift(16, p, bad, w)
+
+
+def _deterministic_dataset(reference, n=16, steps=30, every=10, seed=271):
+    p6 = params6(0.03, 0.1, 0.0, 0.5, 2, 3)
+    return reference.synthetic_observations(n, 0.01, steps, every, p6, 0.05, seed)
+
+
+@pytest.mark.parametrize("stride", [1, 7, 20])
+def test_likelihood_adjoint_matches_reference(hzlb, reference, stride):
+    """Value, gradient and counters of the reference's likelihood_adjoint for several
+    parameter vectors in one call (src/adjoint.cpp:43-161)."""
+    ds = _deterministic_dataset(reference)
+    qs = np.array([[np.log(0.03), np.log(0.1)], [np.log(0.05), np.log(0.2)],
+                   [np.log(0.01), np.log(0.05)], [-0.5, -3.0]])
+    got = hzlb.likelihood_adjoint(ds, qs, stride)
+    for q, g in zip(qs, got):
+        ref = reference.likelihood_adjoint(ds, q, stride)
+        assert abs(g["value"] - ref["value"]) <= 1e-11 * abs(ref["value"])
+        np.testing.assert_allclose(g["gradient"], ref["gradient"], rtol=1e-9, atol=1e-12)
+        for key in ("checkpoint_fields", "peak_block_fields", "replayed_steps"):
+            assert g[key] == ref[key], key
+
+
+def test_likelihood_adjoint_gradient_by_differences(hzlb, reference):
+    """The gradient is the derivative of the device objective (central differences)."""
+    ds = _deterministic_dataset(reference, n=32, steps=40, every=10)
+    q = np.array([np.log(0.02), np.log(0.08)])
+    h = 1e-5
+    pts = [q, q + [h, 0], q - [h, 0], q + [0, h], q - [0, h]]
+    res = hzlb.likelihood_adjoint(ds, np.array(pts), 10)
+    fd = [(res[1]["value"] - res[2]["value"]) / (2 * h), (res[3]["value"] - res[4]["value"]) / (2 * h)]
+    np.testing.assert_allclose(res[0]["gradient"], fd, rtol=1e-5)
+
+
+def test_likelihood_adjoint_exits(hzlb, reference):
+    ds = _deterministic_dataset(reference)
+    got = hzlb.likelihood_adjoint(ds, [[0.5, -1.0], [-1.0, np.nan], [-13.0, -1.0]], 5)
+    for g in got:
+        assert g["value"] == np.inf and list(g["gradient"]) == [0, 0]
+        assert reference.likelihood_adjoint(ds, [0.5, -1.0], 5)["value"] == np.inf
+    # past the explicit diffusion bound
+    big = dict(ds, dt=1.0)
+    assert hzlb.likelihood_adjoint(big, [[-1.0, -1.0]], 5)[0]["value"] == np.inf
+    assert reference.likelihood_adjoint(big, [-1.0, -1.0], 5)["value"] == np.inf
+    with pytest.raises(hzlb.HzlbInvalidArgument, match="positive checkpoint stride"):
+        hzlb.likelihood_adjoint(ds, [[-1.0, -1.0]], 0)
+    with pytest.raises(hzlb.HzlbInvalidArgument, match="deterministic data"):
+        hzlb.likelihood_adjoint(dict(ds, stochastic=1), [[-1.0, -1.0]], 5)

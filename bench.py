@@ -667,6 +667,7 @@ def main():
             likelihood = likelihood_experiment(not args.no_cpu_baseline)
             tangent = tangent_experiment(not args.no_cpu_baseline)
 
+    model_bytes = 32 * 8 * N * (N // 2 + 1) + 16 * 8 * N * N
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": world,
@@ -683,7 +684,13 @@ def main():
                          "traffic": traffic, "algorithmic_bytes": dom[2],
                          "launch_ms": dom[3],
                          "row_kernel": {"ms": row_ms, "gbs": row_gbs},
-                         "column_kernel": {"ms": col_ms, "gbs": col_gbs}},
+                         "column_kernel": {"ms": col_ms, "gbs": col_gbs},
+                         # the whole-step byte model B32(N) = 32 S + 16 P of a schedule that
+                         # moves five real fields per stage (S = 8 N (N/2+1), P = 8 N^2 bytes);
+                         # this design moves fewer bytes, so this fraction exceeds 1
+                         "step_model": {"bytes_per_member_step": model_bytes,
+                                        "achieved": value * model_bytes / 1e9,
+                                        "frac": value * model_bytes / 1e9 / peak}},
             "cpu_baseline": cpu,
             "gpu_reference": gpu_ref,
             "fp64": fp64,

@@ -8,8 +8,9 @@ larger than L2 (126 MB), so every step streams from HBM.
 
 Legs:
   value        device-resident throughput (CUDA events on the library's stream, max over ranks)
-  e2e          the same step through the C ABI with the whole ensemble state copied
-               host->device (pinned) before and device->host after every step
+  e2e          the same step through the C ABI (hzlb_step_host) with the whole ensemble
+               state read from pinned host memory and written back every step, the
+               copies of each member chunk overlapping the stepping of the others
   roofline     dominant kernel: algorithmic bytes per launch / mean launch duration
   cpu_baseline the reference's own CPU solver (oracle/_ref, hzl::ensemble on all host
                threads) on a bounded sample of the same grid size
@@ -626,18 +627,16 @@ def main():
     host_in = torch.from_numpy(ens.get_state_compact().view(np.float32)).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
     e2e_steps = max(3, args.steps // 2)
+    # every step reads the whole state from pinned host memory and writes the result back
+    # (hzlb_step_host: member chunks whose copies overlap the stepping of the others)
     for _ in range(2):
-        ens.set_state_compact_ptr(host_in.data_ptr(), 0, M)
-        ens.step(DT, 1)
-        ens.get_state_compact_ptr(host_out.data_ptr(), 0, M)
+        ens.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), DT, 1)
     barrier()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for _ in range(e2e_steps):
-        ens.set_state_compact_ptr(host_in.data_ptr(), 0, M)
-        ens.step(DT, 1)
-        ens.get_state_compact_ptr(host_out.data_ptr(), 0, M)
+        ens.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), DT, 1)
     t1.record(stream)
     ens.synchronize()
     barrier()

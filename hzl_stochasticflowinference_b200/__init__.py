@@ -123,6 +123,7 @@ def library() -> C.CDLL:
         "hzlb_compact_size": (C.c_size_t, [vp]),
         "hzlb_set_forcing": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
         "hzlb_step": (C.c_int, [vp, C.c_double, C.c_uint64]),
+        "hzlb_step_host": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, C.c_int]),
         "hzlb_status": (C.c_int, [vp, _u32p]),
         "hzlb_synchronize": (C.c_int, [vp]),
         "hzlb_stream": (C.c_void_p, [vp]),
@@ -374,6 +375,14 @@ class Ensemble:
 
     def get_state_compact_ptr(self, ptr: int, first: int, count: int):
         _check(self._lib.hzlb_get_state_compact(self._h, C.c_void_p(ptr), first, count))
+
+    def step_host_ptr(self, in_ptr: int, out_ptr: int, dt: float, nsteps: int = 1,
+                      chunk_members: int = 0):
+        """nsteps steps of a host-resident ensemble state (compact layout, all members) read
+        from in_ptr and written to out_ptr, copies overlapping the stepping in member chunks
+        (hzlb_step_host); pinned host buffers give the overlap."""
+        _check(self._lib.hzlb_step_host(self._h, C.c_void_p(in_ptr), C.c_void_p(out_ptr), dt,
+                                        nsteps, chunk_members))
 
     def set_forcing(self, spectra: np.ndarray, first: int = 0):
         s = _c128(spectra).reshape(-1, self.n, self.n)

@@ -17,6 +17,20 @@ constexpr double kPi = 3.141592653589793238462643383279502884;
 bool valid_grid(int n) { return n >= 8 && n <= 512 && (n & (n - 1)) == 0; }
 int wave(int i, int n) { return i < n / 2 ? i : i - n; }
 
+// The step counter and status of an ensemble after chunks of it were stepped with their own
+// control words: every chunk ends at the same step; status bits accumulate.
+__global__ void merge_chunk_control(StepControl *main, const StepControl *chunks, int count,
+                                    unsigned long long step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        unsigned status = 0;
+        for (int i = 0; i < count; ++i)
+            status |= chunks[i].status;
+        main->status |= status;
+        main->step = step;
+        main->arrivals = 0;
+    }
+}
+
 template <typename R> class EngineT final : public Engine {
   public:
     explicit EngineT(const hzlb_config &c) : cfg_(c) {
@@ -76,6 +90,11 @@ template <typename R> class EngineT final : public Engine {
         for (auto &e : fevent_)
             if (e)
                 cudaEventDestroy(e);
+        for (auto &e : pipe_events_)
+            cudaEventDestroy(e);
+        for (cudaStream_t t : {copy_in_, copy_out_, compute2_})
+            if (t)
+                cudaStreamDestroy(t);
         if (stream_)
             cudaStreamDestroy(stream_);
     }
@@ -481,6 +500,106 @@ template <typename R> class EngineT final : public Engine {
         time += dt * static_cast<double>(nsteps);
         step_index += nsteps;
     }
+    // Steps the ensemble whose state lives on the host: members [f, f+k) of each chunk are
+    // copied in, stepped and copied out, the copies of one chunk overlapping the stepping of
+    // the others (copy-in stream -> one of two compute streams -> copy-out stream, ordered by
+    // events).
+    // Each chunk runs with its own step-control word, started at the current step; the
+    // ensemble's counter and status are merged afterwards.  Chunk boundaries keep every
+    // chunk's state 16-byte aligned for the bulk copies.
+    void step_host(const void *in, void *out, double dt, uint64_t nsteps, int chunk) override {
+        const int largest = (n_ - 1) / 3;
+        if (!std::isfinite(dt) || dt <= 0 ||
+            dt * (2 * cfg_.nu * largest * largest + cfg_.alpha) > 2.5)
+            raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");
+        if (!in || !out)
+            raise(HZLB_EINVAL, "null host state");
+        if (ou_)
+            raise(HZLB_EINVAL, "host-pipelined stepping does not advance device OU forcing");
+        const size_t bytes_per = sizeof(cx<R>) * compact_;
+        int q = 1;   // members per 16 bytes of alignment
+        while ((static_cast<size_t>(q) * bytes_per) % 16 != 0)
+            ++q;
+        if (chunk <= 0)
+            chunk = (M_ + 7) / 8;
+        chunk = std::min(M_, (chunk + q - 1) / q * q);
+        const int chunks = (M_ + chunk - 1) / chunk;
+        for (cudaStream_t *t : {&copy_in_, &copy_out_, &compute2_})
+            if (!*t)
+                cuda_check(cudaStreamCreateWithFlags(t, cudaStreamNonBlocking), "create stream");
+        while (pipe_events_.size() < static_cast<size_t>(2 * chunks + 3)) {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
+            pipe_events_.push_back(e);
+        }
+        chunk_ctl_.ensure(sizeof(StepControl) * chunks, "allocate chunk control");
+        std::vector<StepControl> init(chunks);
+        for (auto &c : init)
+            c = StepControl{step_index, 0u, 0u};
+        cuda_check(cudaMemcpyAsync(chunk_ctl_.ptr, init.data(), sizeof(StepControl) * chunks,
+                                   cudaMemcpyHostToDevice, stream_),
+                   "initialise chunk control");
+        cudaEvent_t start = pipe_events_[2 * chunks], end = pipe_events_[2 * chunks + 1],
+                    side = pipe_events_[2 * chunks + 2];
+        cuda_check(cudaEventRecord(start, stream_), "record event");
+        cuda_check(cudaStreamWaitEvent(copy_in_, start, 0), "order copy stream");
+        cuda_check(cudaStreamWaitEvent(compute2_, start, 0), "order compute stream");
+        const auto *src = static_cast<const unsigned char *>(in);
+        auto *dst = static_cast<unsigned char *>(out);
+        StepControl *ctl = chunk_ctl_.as<StepControl>();
+        for (int i = 0; i < chunks; ++i) {
+            const int f = i * chunk, k = std::min(chunk, M_ - f);
+            const size_t off = static_cast<size_t>(f) * compact_, bytes = bytes_per * k;
+            cuda_check(cudaMemcpyAsync(omega_.as<cx<R>>() + off, src + bytes_per * f, bytes,
+                                       cudaMemcpyHostToDevice, copy_in_),
+                       "host state upload");
+            cuda_check(cudaEventRecord(pipe_events_[2 * i], copy_in_), "record event");
+            // consecutive chunks alternate between two compute streams, so that one chunk's
+            // kernels fill the SMs left idle by the last work items of the other's
+            const cudaStream_t cs = (i & 1) ? compute2_ : stream_;
+            cuda_check(cudaStreamWaitEvent(cs, pipe_events_[2 * i], 0), "order step");
+            ColumnArgs<R> a = column_args(dt);
+            RowArgs<R> r = row_args();
+            a.omega += off;
+            a.ystage += off;
+            a.acc += off;
+            a.w += static_cast<size_t>(f) * n_ * 2 * C_;
+            a.nl += static_cast<size_t>(f) * 2 * C_ * n_;
+            if (a.forcing && a.forcing_stride)
+                a.forcing += static_cast<size_t>(f) * a.forcing_stride;
+            a.member_base += static_cast<unsigned>(f);
+            a.members = k;
+            a.ctl = ctl + i;
+            r.w = a.w;
+            r.nl = nl_.as<cx<R>>() + static_cast<size_t>(f) * 2 * C_ * n_;
+            r.members = k;
+            r.ctl = ctl + i;
+            a.stage = 0;
+            cuda_check(launch_column<R>(n_, a, cs), "launch start column pass");
+            for (uint64_t st = 0; st < nsteps; ++st)
+                for (int stage = 1; stage <= 4; ++stage) {
+                    r.cfl_scale = stage == 1 ? dt * n_ / (2 * kPi) : 0.0;
+                    cuda_check(launch_row<R>(n_, r, cs), "launch row pass");
+                    a.stage = stage;
+                    cuda_check(launch_column<R>(n_, a, cs), "launch column pass");
+                }
+            cuda_check(cudaEventRecord(pipe_events_[2 * i + 1], cs), "record event");
+            cuda_check(cudaStreamWaitEvent(copy_out_, pipe_events_[2 * i + 1], 0), "order download");
+            cuda_check(cudaMemcpyAsync(dst + bytes_per * f, omega_.as<cx<R>>() + off, bytes,
+                                       cudaMemcpyDeviceToHost, copy_out_),
+                       "host state download");
+        }
+        cuda_check(cudaEventRecord(side, compute2_), "record event");
+        cuda_check(cudaStreamWaitEvent(stream_, side, 0), "join compute streams");
+        merge_chunk_control<<<1, 32, 0, stream_>>>(ctl_.as<StepControl>(), ctl, chunks,
+                                                    step_index + nsteps);
+        cuda_check(cudaGetLastError(), "merge chunk control");
+        cuda_check(cudaEventRecord(end, copy_out_), "record event");
+        cuda_check(cudaStreamWaitEvent(stream_, end, 0), "order library stream");
+        w_valid_ = true;
+        time += dt * static_cast<double>(nsteps);
+        step_index += nsteps;
+    }
     void step_profiled(double dt, uint64_t nsteps, double *row_ms, double *col_ms) override {
         const int largest = (n_ - 1) / 3;
         if (!std::isfinite(dt) || dt <= 0 ||
@@ -854,6 +973,9 @@ template <typename R> class EngineT final : public Engine {
     int fbuf_next_ = 0;
     std::vector<Graph> graphs_;
     bool w_valid_ = false;
+    cudaStream_t copy_in_ = nullptr, copy_out_ = nullptr, compute2_ = nullptr;
+    std::vector<cudaEvent_t> pipe_events_;
+    DeviceBuffer chunk_ctl_;
 };
 
 } // namespace

@@ -125,6 +125,16 @@ HZLB_API int hzlb_get_forcing_compact(hzlb_ensemble *h, double *out, int first, 
  * HZLB_EINVAL for a nonpositive/nonfinite dt or dt * (2 nu K^2 + alpha) > 2.5
  * (cuda_solver.cu:205-208). */
 HZLB_API int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps);
+/* No counterpart in the reference (its CudaSolver copies each member's state in and out around
+ * every step, cuda_solver.cu:173-235).  The ensemble state lives on the host: state_in is read
+ * and state_out written (both all members, the compact layout of the configured precision, as
+ * hzlb_set_state_compact; they may be the same buffer), nsteps steps in between.  The members
+ * go in chunks of about chunk_members (0: an eighth of the ensemble), each chunk's copies
+ * overlapping the stepping of the others; pinned host buffers are needed for the overlap.
+ * Results equal hzlb_set_state_compact + hzlb_step + hzlb_get_state_compact bit for bit.
+ * Asynchronous on the handle's stream; device OU forcing is not supported here. */
+HZLB_API int hzlb_step_host(hzlb_ensemble *h, const void *state_in, void *state_out, double dt,
+                            uint64_t nsteps, int chunk_members);
 /* Waits for the handle's stream; returns the accumulated status bits and clears them. */
 HZLB_API int hzlb_status(hzlb_ensemble *h, uint32_t *status);
 HZLB_API int hzlb_synchronize(hzlb_ensemble *h);

@@ -1,0 +1,91 @@
+"""hzlb_step_host: the ensemble state read from and written to host memory around the steps,
+in member chunks whose copies overlap the stepping.  The results are bit-identical with
+hzlb_set_state_compact + hzlb_step + hzlb_get_state_compact for every chunk size (odd sizes are
+rounded so that each chunk's state stays 16-byte aligned), in FP32 and FP64, and the noise
+counter and status carry over to later steps."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import device_synthetic
+
+pytestmark = pytest.mark.gpu
+
+
+def _pair(hzlb, n, members, precision):
+    kmax = min(4, (n - 1) // 3)
+    a = device_synthetic(hzlb, n, members, precision, 5e-4, 0.05, 11, wavenumber=kmax,
+                         noise_kmax=kmax)
+    b = device_synthetic(hzlb, n, members, precision, 5e-4, 0.05, 11, wavenumber=kmax,
+                         noise_kmax=kmax)
+    return a, b
+
+
+def _pinned_state(e, dtype):
+    state = e.get_state_compact()
+    host = torch.from_numpy(np.ascontiguousarray(state).view(dtype)).pin_memory()
+    return host, torch.empty_like(host).pin_memory()
+
+
+@pytest.mark.parametrize("n,members,precision,chunk", [
+    (256, 48, 4, 0), (256, 48, 4, 7), (256, 48, 4, 48), (256, 48, 4, 1000),
+    (128, 33, 4, 5), (128, 33, 8, 3), (64, 10, 8, 1)])
+def test_bit_identical_with_device_stepping(hzlb, n, members, precision, chunk):
+    dt, steps = 5e-4, 3
+    a, b = _pair(hzlb, n, members, precision)
+    dtype = np.float32 if precision == 4 else np.float64
+    host_in, host_out = _pinned_state(a, dtype)
+    a.set_state_compact_ptr(host_in.data_ptr(), 0, members)
+    a.step(dt, steps)
+    want = a.get_state_compact()
+    b.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), dt, steps, chunk)
+    b.synchronize()
+    got = host_out.numpy().view(want.dtype).reshape(want.shape)
+    assert np.array_equal(got, want)
+    assert b.status() == 0
+    # the counter (noise) and the state carry on: one more ordinary step agrees too
+    a.step(dt, 1)
+    b.step(dt, 1)
+    assert np.array_equal(a.get_state_compact(), b.get_state_compact())
+    a.close()
+    b.close()
+
+
+def test_in_place_buffer_and_repeated_calls(hzlb):
+    a, b = _pair(hzlb, 128, 16, 4)
+    host, _ = _pinned_state(a, np.float32)
+    for _ in range(3):
+        a.set_state_compact_ptr(host.data_ptr(), 0, 16)
+        a.step(5e-4, 1)
+        a.get_state_compact_ptr(host.data_ptr(), 0, 16)
+    a.synchronize()
+    want = host.numpy().copy()
+    host2, _ = _pinned_state(b, np.float32)
+    for _ in range(3):
+        b.step_host_ptr(host2.data_ptr(), host2.data_ptr(), 5e-4, 1, 4)
+    b.synchronize()
+    assert np.array_equal(host2.numpy(), want)
+    a.close()
+    b.close()
+
+
+def test_cfl_violation_is_flagged_in_a_chunk(hzlb):
+    a, _ = _pair(hzlb, 64, 8, 8)
+    state = a.get_state_compact()
+    state[5] *= 1e4                       # one member far too fast for dt
+    host = torch.from_numpy(np.ascontiguousarray(state).view(np.float64)).pin_memory()
+    a.step_host_ptr(host.data_ptr(), host.data_ptr(), 0.01, 1, 2)
+    assert a.status() & hzlb.STATUS_CFL
+    a.close()
+
+
+def test_invalid_calls(hzlb):
+    a, _ = _pair(hzlb, 32, 4, 4)
+    host, out = _pinned_state(a, np.float32)
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        a.step_host_ptr(host.data_ptr(), out.data_ptr(), -1.0, 1, 0)
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        a.step_host_ptr(0, out.data_ptr(), 1e-3, 1, 0)
+    a.close()

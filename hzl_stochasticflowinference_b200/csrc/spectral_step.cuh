@@ -34,9 +34,11 @@
 
 namespace hzlb {
 
-// E (elements per thread) keeps a line inside one warp; FP64 uses fewer registers per thread.
+// E (elements per thread) keeps a line inside one warp.  16 elements (two radix-16 passes at
+// 256) beat 8 (three passes, twice the threads per line) in both precisions: measured at 256^2,
+// FP32 0.63 against 1.00 ms per column launch, FP64 252k against 221k member-steps/s.
 template <typename R, int N> struct Cfg {
-    static constexpr int E = sizeof(R) == 4 ? (N < 16 ? N : 16) : (N <= 256 ? (N < 8 ? N : 8) : 16);
+    static constexpr int E = N < 16 ? N : 16;
     static constexpr int T = N / E;
     static constexpr int K = (N - 1) / 3;
     static constexpr int C = K + 1;          // retained kx columns

@@ -50,8 +50,9 @@ template <typename R> class EngineT final : public Engine {
         compact_ = static_cast<size_t>(C_) * LD_;
         fcols_ = c.forcing_kmax < 0 ? 0 : std::min(c.forcing_kmax + 1, C_);
         fcount_ = fcols_ == 0 ? 0 : (c.forcing_per_member ? M_ : 1);
-        if (c.noise_sigma > 0 && (c.noise_kmax < 1 || 3 * c.noise_kmax >= n_))
-            raise(HZLB_EINVAL, "noise shell must lie strictly inside the dealiased grid");
+        if (c.noise_sigma > 0 && (c.noise_kmax < 1 || 3 * c.noise_kmax >= n_ ||
+                                  c.noise_kmax > NOISE_KMAX_CAP))
+            raise(HZLB_EINVAL, "noise shell must lie strictly inside the dealiased grid, radius <= 15");
         int devices = 0;
         cuda_check(cudaGetDeviceCount(&devices), "query CUDA devices");
         if (c.device < 0 || c.device >= devices)

@@ -190,8 +190,9 @@ extern "C" HZLB_API int hzlb_step_noalloc(const hzlb_config *config, double dt, 
         if (!std::isfinite(c.nu) || c.nu < 0 || !std::isfinite(c.alpha) || c.alpha < 0 ||
             !std::isfinite(c.noise_sigma) || c.noise_sigma < 0)
             raise(HZLB_EINVAL, "nu, alpha and noise sigma must be finite and nonnegative");
-        if (c.noise_sigma > 0 && (c.noise_kmax < 1 || 3 * c.noise_kmax >= c.n))
-            raise(HZLB_EINVAL, "noise shell must lie strictly inside the dealiased grid");
+        if (c.noise_sigma > 0 && (c.noise_kmax < 1 || 3 * c.noise_kmax >= c.n ||
+                                  c.noise_kmax > NOISE_KMAX_CAP))
+            raise(HZLB_EINVAL, "noise shell must lie strictly inside the dealiased grid, radius <= 15");
         const int largest = (c.n - 1) / 3;
         if (!std::isfinite(dt) || dt <= 0 || dt * (2 * c.nu * largest * largest + c.alpha) > 2.5)
             raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");

@@ -144,6 +144,16 @@ template <int N, int T, int r> __device__ __forceinline__ int band_j(int p) {
         return compact_j<N>(p);
 }
 
+// Largest radius of the additive noise shell 1 <= |k| <= noise_kmax on grids of 48^2 and up (on
+// smaller grids the shell is bounded by the retained band K <= 15 anyway).  With it, only the
+// register positions whose ky can lie in |ky| <= 15 carry the noise draw, so the final stage's
+// body holds 2 copies of it at 256^2 instead of 16.
+constexpr int NOISE_KMAX_CAP = 15;
+template <int N, int T, int r> struct NoiseBand {
+    static constexpr int lo = r * T, hi = r * T + T - 1;
+    static constexpr bool possible = lo <= NOISE_KMAX_CAP || hi >= N - NOISE_KMAX_CAP;
+};
+
 // Block-uniform bounded wait: thread 0 polls, the outcome is shared through `flag`, then
 // every thread observes the completed phase.  Returns false on every thread on timeout.
 __device__ __forceinline__ bool block_wait(uint64_t *bar, uint32_t parity, volatile int *flag) {
@@ -337,7 +347,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                         // w += dt/6 (k1 + 2 k2 + 2 k3 + k4)   (solver.cpp:233-234)
                         cx<R> w1 = wn + scale(dt / 6, s_a[j] + kk);
                         const int kk2 = kxc * kxc + ky * ky;
-                        if (a.noise_scale > 0 && kk2 >= 1 && kk2 <= a.noise_kmax2) {
+                        if (NoiseBand<N, T, r>::possible && a.noise_scale > 0 && kk2 >= 1 &&
+                            kk2 <= a.noise_kmax2) {
                             double xi1, xi2;
                             const bool rep = kxc > 0 || ky > 0;
                             philox_normal_pair(a.seed, a.member_base + m, step_sh,

@@ -76,7 +76,8 @@ typedef struct {
     int forcing_kmax;          /* forcing stored for columns kx <= forcing_kmax; -1: no forcing */
     int forcing_per_member;    /* 0: one forcing field shared by all members; 1: one per member */
     double noise_sigma;        /* Euler-Maruyama noise amplitude after each step; 0: off */
-    int noise_kmax;            /* noise on modes with 1 <= |k|^2 <= noise_kmax^2 */
+    int noise_kmax;            /* noise on modes with 1 <= |k|^2 <= noise_kmax^2; needs
+                                  3 noise_kmax < n and noise_kmax <= 15 */
     uint64_t seed;             /* Philox key for the noise */
     uint32_t member_base;      /* global index of member 0 (Philox key; sharding offset) */
     int device;                /* CUDA device ordinal */

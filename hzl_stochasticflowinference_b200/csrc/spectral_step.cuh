@@ -589,9 +589,16 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         }
         __syncthreads();
         cx<R> *dst = a.nl + static_cast<size_t>(m) * 2 * C * N;
-        for (int i = threadIdx.x; i < 2 * C * TY; i += blockDim.x) {
-            const int t2 = i % TY, fk = i / TY;
-            dst[static_cast<size_t>(fk) * N + y0 + t2] = nlt[fk * TY + (t2 ^ swz<TY>(fk))];
+        // entry (fk, t2) of the staged products goes to column fk, row y0 + t2; the threads
+        // cover fk * TY + t2 in order, so each keeps one t2 and steps fk
+        static_assert(G::ROW_THREADS % TY == 0, "whole staged columns per pass");
+        constexpr int FSTEP = G::ROW_THREADS / TY;
+        {
+            const int t2 = threadIdx.x % TY;
+            cx<R> *row = dst + y0 + t2;
+#pragma unroll 4
+            for (int fk = threadIdx.x / TY; fk < 2 * C; fk += FSTEP)
+                row[static_cast<size_t>(fk) * N] = nlt[fk * TY + (t2 ^ swz<TY>(fk))];
         }
         // the next item's transforms write the line buffers only after its tile barrier and
         // the block barrier that follows it

@@ -1,11 +1,15 @@
 // FP64 dense linear algebra for the EnKF innovation system (p x p, p up to a few thousand):
-// a tiled SIMT GEMM with arbitrary operand strides, a blocked right-looking Cholesky whose
-// diagonal blocks are factored and inverted in shared memory, and blocked forward
-// substitution for many right-hand sides built from the same GEMM.  FP64 stays here on
-// purpose: the innovation Cholesky and solve are the one place the analysis needs it.
+// GEMMs with arbitrary operand strides (cuBLAS DGEMM for the plain products, a tiled SIMT
+// kernel for the in-place panel update and strides cuBLAS cannot express), a blocked
+// right-looking Cholesky whose diagonal blocks are factored and inverted in shared memory, and
+// blocked forward substitution for many right-hand sides built from the same GEMM.  FP64 stays
+// here on purpose: the innovation Cholesky and solve are the one place the analysis needs it.
 #pragma once
 #include "common.cuh"
 
+#include <algorithm>
+#include <cstdint>
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 namespace hzlb {
@@ -106,8 +110,93 @@ template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const G
     }
 }
 
+// A strided operand as a row-major block: rows x cols with leading dimension ld (ld 0 if the
+// strides are not of that form).
+struct Block {
+    const double *p;
+    long long rows, cols, ld;
+};
+inline Block a_block(const GemmArgs &g) {
+    if (g.sak == 1)
+        return {g.A, g.M, g.K, g.sam};
+    if (g.sam == 1)
+        return {g.A, g.K, g.M, g.sak};
+    return {g.A, g.M, g.K, 0};
+}
+inline Block b_block(const GemmArgs &g) {
+    if (g.sbn == 1)
+        return {g.B, g.K, g.N, g.sbk};
+    if (g.sbk == 1)
+        return {g.B, g.N, g.K, g.sbn};
+    return {g.B, g.K, g.N, 0};
+}
+// Whether two blocks may share an element: exact for blocks of one leading dimension (both
+// no wider than it), else by address extent.
+inline bool may_overlap(const Block &x, const Block &y) {
+    const auto lo = [](const Block &b) { return reinterpret_cast<std::uintptr_t>(b.p); };
+    const auto hi = [](const Block &b) {
+        return reinterpret_cast<std::uintptr_t>(b.p) +
+               sizeof(double) * static_cast<std::uintptr_t>((b.rows - 1) * b.ld + b.cols);
+    };
+    if (x.ld == 0 || y.ld == 0 || x.ld != y.ld || x.cols > x.ld || y.cols > y.ld)
+        return !(hi(x) <= lo(y) || hi(y) <= lo(x)) || x.ld == 0 || y.ld == 0;
+    const long long L = x.ld;
+    const long long d = (static_cast<long long>(lo(x)) - static_cast<long long>(lo(y))) /
+                        static_cast<long long>(sizeof(double));
+    long long q = d / L, r = d % L;
+    if (r < 0) {
+        r += L;
+        --q;
+    }
+    const auto meet = [](long long a0, long long a1, long long b0, long long b1) {
+        return a0 < b1 && b0 < a1;
+    };
+    // x's columns [r, r + cols) in y's rows q..; the part past the edge wraps to the next row
+    const long long first = std::min(x.cols, L - r);
+    if (meet(q, q + x.rows, 0, y.rows) && meet(r, r + first, 0, y.cols))
+        return true;
+    if (x.cols > first && meet(q + 1, q + 1 + x.rows, 0, y.rows) && meet(0, x.cols - first, 0, y.cols))
+        return true;
+    return false;
+}
+
+// One cuBLAS handle per device and host thread (kept until exit).
+inline cublasHandle_t cublas_handle() {
+    thread_local cublasHandle_t handles[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+        return nullptr;
+    if (!handles[dev] && cublasCreate(&handles[dev]) != CUBLAS_STATUS_SUCCESS)
+        handles[dev] = nullptr;
+    return handles[dev];
+}
+
+// The row-major product through column-major DGEMM: C^T = alpha B^T A^T + beta C^T.  Returns
+// false (nothing done) when the operands do not fit (non-unit strides, or an operand sharing
+// an element with C, which DGEMM forbids).
+inline bool gemm_cublas(const GemmArgs &g, cudaStream_t s) {
+    const Block a = a_block(g), b = b_block(g), c{g.C, g.M, g.N, g.ldc};
+    if (a.ld == 0 || b.ld == 0 || g.K <= 0 || g.ldc < g.N || may_overlap(a, c) || may_overlap(b, c))
+        return false;
+    cublasHandle_t h = cublas_handle();
+    if (!h || cublasSetStream(h, s) != CUBLAS_STATUS_SUCCESS)
+        return false;
+    // op(X) = B^T (N x K), op(Y) = A^T (K x M)
+    const cublasOperation_t ox = g.sbn == 1 ? CUBLAS_OP_N : CUBLAS_OP_T;
+    const cublasOperation_t oy = g.sak == 1 ? CUBLAS_OP_N : CUBLAS_OP_T;
+    const long long ldx = g.sbn == 1 ? g.sbk : g.sbn, ldy = g.sak == 1 ? g.sam : g.sak;
+    if (ldx > INT32_MAX || ldy > INT32_MAX || g.ldc > INT32_MAX)
+        return false;
+    return cublasDgemm(h, ox, oy, g.N, g.M, g.K, &g.alpha, g.B, static_cast<int>(ldx), g.A,
+                       static_cast<int>(ldy), &g.beta, g.C, static_cast<int>(g.ldc)) ==
+           CUBLAS_STATUS_SUCCESS;
+}
+
+// lower: only C[m][n], n <= m, is wanted (the cuBLAS path writes the whole of C).
 inline cudaError_t gemm(const GemmArgs &g, cudaStream_t s, bool lower = false) {
     if (g.M <= 0 || g.N <= 0)
+        return cudaSuccess;
+    if (gemm_cublas(g, s))
         return cudaSuccess;
     const dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
     if (lower)

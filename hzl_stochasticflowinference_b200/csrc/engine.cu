@@ -733,9 +733,41 @@ template <typename R> class EngineT final : public Engine {
         for (size_t o = 0; o < p; ++o)
             if (x[o] >= static_cast<uint32_t>(n_) || y[o] >= static_cast<uint32_t>(n_))
                 raise(HZLB_EINVAL, "observation location out of bounds");
+        obs_.ensure(sizeof(double) * std::max<size_t>(p, 1) * M_, "allocate observations");
+        // the row pairs (2q, 2q+1) the observation rows lie in; when they are fewer than all
+        // the rows, only those are transformed (the same values, see field_row_pairs_inverse)
+        std::vector<int> pairs;
+        for (size_t o = 0; o < p; ++o)
+            pairs.push_back(static_cast<int>(y[o] >> 1));
+        std::sort(pairs.begin(), pairs.end());
+        pairs.erase(std::unique(pairs.begin(), pairs.end()), pairs.end());
+        if (p > 0 && 2 * pairs.size() < static_cast<size_t>(n_)) {
+            const size_t np = pairs.size();
+            std::vector<uint32_t> host(2 * p + np);
+            for (size_t o = 0; o < p; ++o) {
+                host[o] = x[o];
+                const size_t q = std::lower_bound(pairs.begin(), pairs.end(), static_cast<int>(y[o] >> 1)) -
+                                 pairs.begin();
+                host[p + o] = static_cast<uint32_t>(2 * q + (y[o] & 1));
+            }
+            for (size_t q = 0; q < np; ++q)
+                host[2 * p + q] = static_cast<uint32_t>(pairs[q]);
+            obs_xy_.ensure(sizeof(uint32_t) * host.size(), "allocate observation points");
+            cuda_check(cudaMemcpyAsync(obs_xy_.ptr, host.data(), sizeof(uint32_t) * host.size(),
+                                       cudaMemcpyHostToDevice, stream_),
+                       "upload observation points");
+            phys_.ensure(sizeof(R) * static_cast<size_t>(n_) * n_ * M_, "allocate physical fields");
+            const unsigned *dx = obs_xy_.as<unsigned>();
+            cuda_check(launch_observe_rows<R>(n_, omega_.as<cx<R>>(), static_cast<long long>(compact_),
+                                              nl_.as<cx<R>>(), phys_.as<R>(),
+                                              reinterpret_cast<const int *>(dx + 2 * p),
+                                              static_cast<int>(np), dx, dx + p, static_cast<int>(p),
+                                              tw_.as<cx<R>>(), M_, obs_.as<double>(), stream_),
+                       "launch observation operator");
+            return;
+        }
         physical_device();
         obs_xy_.ensure(sizeof(uint32_t) * 2 * std::max<size_t>(p, 1), "allocate observation points");
-        obs_.ensure(sizeof(double) * std::max<size_t>(p, 1) * M_, "allocate observations");
         cuda_check(cudaMemcpyAsync(obs_xy_.ptr, x, sizeof(uint32_t) * p, cudaMemcpyHostToDevice, stream_),
                    "upload observation points");
         cuda_check(cudaMemcpyAsync(obs_xy_.as<uint32_t>() + p, y, sizeof(uint32_t) * p,

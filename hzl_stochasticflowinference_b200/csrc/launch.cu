@@ -84,6 +84,16 @@ template <typename R, int N> struct L {
         field_row_inverse<R, N><<<row_grid(members), G::ROW_THREADS, prow_smem, s>>>(cols, phys, tw);
         return cudaGetLastError();
     }
+    static cudaError_t observe_rows(const cx<R> *field, long long stride, cx<R> *cols, R *rows,
+                                    const int *pairs, int npairs, const cx<R> *tw, int members,
+                                    cudaStream_t s) {
+        field_column_inverse<R, N><<<col_grid(members), G::COL_THREADS, pcol_smem, s>>>(
+            field, stride, cols, tw);
+        const dim3 grid(members, (npairs + G::TY / 2 - 1) / (G::TY / 2));
+        field_row_pairs_inverse<R, N><<<grid, G::ROW_THREADS, prow_smem, s>>>(cols, pairs, npairs,
+                                                                              rows, tw);
+        return cudaGetLastError();
+    }
     static cudaError_t vmax(const cx<R> *w, unsigned long long *bits, const cx<R> *tw, int members,
                             cudaStream_t s) {
         velocity_max<R, N><<<row_grid(members), G::ROW_THREADS, prow_smem, s>>>(w, bits, tw);
@@ -140,6 +150,12 @@ template <typename R, int N> struct DoPhysical {
         return L<R, N>::physical(f, st, c, p, tw, m, s);
     }
 };
+template <typename R, int N> struct DoObserveRows {
+    static cudaError_t run(const cx<R> *f, long long st, cx<R> *c, R *rows, const int *pairs,
+                           int npairs, const cx<R> *tw, int m, cudaStream_t s) {
+        return L<R, N>::observe_rows(f, st, c, rows, pairs, npairs, tw, m, s);
+    }
+};
 template <typename R, int N> struct DoVmax {
     static cudaError_t run(const cx<R> *w, unsigned long long *b, const cx<R> *tw, int m,
                            cudaStream_t s) {
@@ -191,6 +207,22 @@ cudaError_t launch_gather(const R *phys, int n, const unsigned *xs, const unsign
                                                                               members, out);
     return cudaGetLastError();
 }
+template <typename R>
+cudaError_t launch_observe_rows(int n, const cx<R> *field, long long stride, cx<R> *cols,
+                                R *rows, const int *pairs, int npairs, const unsigned *xs,
+                                const unsigned *slots, int p, const cx<R> *tw, int members,
+                                double *out, cudaStream_t s) {
+    if (npairs <= 0 || p <= 0)
+        return cudaSuccess;
+    cudaError_t e = dispatch<R, DoObserveRows>(n, field, stride, cols, rows, pairs, npairs, tw,
+                                               members, s);
+    if (e != cudaSuccess)
+        return e;
+    const long long total = static_cast<long long>(members) * p;
+    gather_rows<R><<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(
+        rows, 2 * npairs, n, xs, slots, p, members, out);
+    return cudaGetLastError();
+}
 template <typename R> KernelShape kernel_shape(int n) {
     KernelShape k{};
     dispatch<R, DoShape>(n, k);
@@ -210,6 +242,10 @@ template <typename R> KernelShape kernel_shape(int n) {
                                                int, double *, cudaStream_t);                       \
     template cudaError_t launch_gather<R>(const R *, int, const unsigned *, const unsigned *, int, \
                                           int, double *, cudaStream_t);                            \
+    template cudaError_t launch_observe_rows<R>(int, const cx<R> *, long long, cx<R> *, R *,       \
+                                                const int *, int, const unsigned *,                \
+                                                const unsigned *, int, const cx<R> *, int,         \
+                                                double *, cudaStream_t);                           \
     template KernelShape kernel_shape<R>(int);
 HZLB_INSTANTIATE(float)
 HZLB_INSTANTIATE(double)

@@ -30,6 +30,13 @@ cudaError_t launch_diagnostics(int n, const cx<R> *omega, const cx<R> *forcing, 
 template <typename R>
 cudaError_t launch_gather(const R *phys, int n, const unsigned *xs, const unsigned *ys, int p,
                           int members, double *out, cudaStream_t s);
+// The physical rows of the listed row pairs at p points (the observation operator of a point
+// set): column inverse transforms of every member, row transforms of the pairs only, gather.
+template <typename R>
+cudaError_t launch_observe_rows(int n, const cx<R> *field, long long stride, cx<R> *cols,
+                                R *rows, const int *pairs, int npairs, const unsigned *xs,
+                                const unsigned *slots, int p, const cx<R> *tw, int members,
+                                double *out, cudaStream_t s);
 template <typename R> KernelShape kernel_shape(int n);
 
 } // namespace hzlb

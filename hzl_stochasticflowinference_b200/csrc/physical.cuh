@@ -185,6 +185,66 @@ __global__ void integral_diagnostics(const cx<R> *omega, const cx<R> *forcing,
     }
 }
 
+// Inverse row transforms of the listed row pairs only (rows 2 q_i and 2 q_i + 1 for each
+// entry q_i of pairs, the pairs that observation rows lie in), packed two rows per complex
+// transform exactly as field_row_inverse packs them, so every value equals the full
+// transform's: out[m][2 i + h][x], h = 0, 1.
+template <typename R, int N>
+__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
+    field_row_pairs_inverse(const cx<R> *cols, const int *pairs, int npairs, R *out,
+                            const cx<R> *tw_g) {
+    using G = Cfg<R, N>;
+    constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
+    cx<R> *lines = tw + G::TWE;
+    load_pass_twiddles<N, G::E, R>(tw, tw_g);
+    __syncthreads();
+    const int g = threadIdx.x / T, t = threadIdx.x % T, m = blockIdx.x;
+    const int q = blockIdx.y * (TY / 2) + g;
+    const bool active = g < TY / 2 && q < npairs;
+    const int ya = active ? 2 * pairs[q] : 0;
+    const cx<R> *src = cols + static_cast<size_t>(m) * C * N;
+    cx<R> z[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int pos = t + r * T;
+        cx<R> za = mk<R>(0, 0), zb = mk<R>(0, 0);
+        if (pos <= K) {
+            za = src[static_cast<size_t>(pos) * N + ya];
+            zb = src[static_cast<size_t>(pos) * N + ya + 1];
+            if (pos == 0) {
+                za.y = 0;
+                zb.y = 0;
+            }
+        } else if (pos >= N - K) {
+            za = conj(src[static_cast<size_t>(N - pos) * N + ya]);
+            zb = conj(src[static_cast<size_t>(N - pos) * N + ya + 1]);
+        }
+        z[r] = mk<R>(za.x - zb.y, za.y + zb.x);
+    }
+    fft_line<N, E, +1, R>(z, lines + g * G::BUF, tw, t);
+    if (active) {
+        R *da = out + (static_cast<size_t>(m) * npairs + q) * 2 * N;
+#pragma unroll
+        for (int r = 0; r < E; ++r) {
+            da[t + r * T] = z[r].x;
+            da[N + t + r * T] = z[r].y;
+        }
+    }
+}
+
+// Sample rows of physical fields at p points: out[m][o] = rows[m][slot_o][x_o].
+template <typename R>
+__global__ void gather_rows(const R *rows, int nrows, int n, const unsigned *xs,
+                            const unsigned *slots, int p, int members, double *out) {
+    const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= static_cast<long long>(members) * p)
+        return;
+    const int m = static_cast<int>(i / p), o = static_cast<int>(i % p);
+    out[i] = rows[(static_cast<size_t>(m) * nrows + slots[o]) * n + xs[o]];
+}
+
 // Sample the physical fields at p points: out[m][o] = phys[m][y_o][x_o].
 template <typename R>
 __global__ void gather_points(const R *phys, int n, const unsigned *xs, const unsigned *ys, int p,

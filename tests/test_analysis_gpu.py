@@ -8,7 +8,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from helpers import rel_l2
+from helpers import device_synthetic, rel_l2
 from hzl_stochasticflowinference_b200 import sharding
 from oracle.oracle import params6
 
@@ -183,3 +183,27 @@ def test_device_perturbations_match_philox(hzlb, oracle, precision, tol):
     assert abs(na - nb_) < 1e-12 * max(1.0, abs(nb_))
     assert rel_l2(a.get_state_compact().astype(np.complex128),
                   b.get_state_compact().astype(np.complex128)) < tol
+
+
+@pytest.mark.parametrize("precision", [4, 8])
+@pytest.mark.parametrize("points", ["sparse", "scattered", "strided", "all rows"])
+def test_observation_rows_equal_the_physical_field(hzlb, precision, points):
+    """The observation operator transforms only the row pairs its points lie in; every value
+    is the full physical field's, bit for bit, for any point set."""
+    n, members = 64, 5
+    e = device_synthetic(hzlb, n, members, precision, 1e-3, 0.05, 3)
+    e.step(1e-3, 3)
+    rng = np.random.default_rng(4)
+    if points == "sparse":
+        xs, ys = np.array([3, 17, 63]), np.array([0, 0, 63])
+    elif points == "scattered":
+        xs, ys = rng.integers(0, n, 40), rng.integers(0, n, 40)
+    elif points == "strided":
+        g = np.arange(0, n, 8)
+        xs, ys = np.tile(g, len(g)), np.repeat(g, len(g))
+    else:
+        xs, ys = rng.integers(0, n, 3 * n), np.arange(3 * n) % n
+    got = e.observe(xs, ys)
+    phys = e.physical()
+    assert np.array_equal(got, phys[:, ys, xs])
+    e.close()

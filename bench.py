@@ -96,6 +96,12 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: let its first sample arrive (at most 3 s)
+            # so that the samples cover the timed region that follows
+            deadline = time.time() + 3.0
+            while not self.lines and time.time() < deadline and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.lines.clear()
         except OSError:
             self.proc = None
         return self

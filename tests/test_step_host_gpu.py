@@ -89,3 +89,28 @@ def test_invalid_calls(hzlb):
     with pytest.raises(hzlb.HzlbInvalidArgument):
         a.step_host_ptr(0, out.data_ptr(), 1e-3, 1, 0)
     a.close()
+
+
+def test_per_member_forcing_offsets(hzlb):
+    """Per-member forcing: each chunk reads its own members' forcing."""
+    n, members = 64, 12
+    outs = []
+    for use_host in (False, True):
+        cfg = hzlb.Config(n=n, members=members, precision=8, nu=1e-3, alpha=0.05,
+                          forcing_kmax=4, forcing_per_member=True, noise_sigma=0.02,
+                          noise_kmax=4, seed=9)
+        e = hzlb.Ensemble(cfg)
+        e.set_state(np.array([hzlb.grf_spectrum(n, 9, m) for m in range(members)]))
+        e.set_forcing(np.array([(1 + 0.1 * m) * hzlb.kolmogorov_forcing(n, 0.1, 4)
+                                for m in range(members)]))
+        e.set_time(0.0, 0)
+        if use_host:
+            host, out = _pinned_state(e, np.float64)
+            e.step_host_ptr(host.data_ptr(), out.data_ptr(), 1e-3, 2, 3)
+            e.synchronize()
+            outs.append(out.numpy().copy())
+        else:
+            e.step(1e-3, 2)
+            outs.append(np.ascontiguousarray(e.get_state_compact()).view(np.float64).reshape(-1))
+        e.close()
+    assert np.array_equal(outs[0].reshape(-1), outs[1].reshape(-1))

@@ -278,6 +278,19 @@ void check_inputs(int n, const hzlb_parameters *p) {
         raise(HZLB_EINVAL, "forcing shell must lie strictly inside the dealiased grid");
 }
 
+// Restores the calling thread's current device when the call that selected another ends.
+struct DeviceRestore {
+    int previous = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&previous) != cudaSuccess)
+            previous = -1;
+    }
+    ~DeviceRestore() {
+        if (previous >= 0)
+            cudaSetDevice(previous);
+    }
+};
+
 // Device scratch for batched drifts of up to `capacity` members on an n x n grid, one stream.
 // Every operation takes per-member viscosity and friction (device arrays).
 class Workspace {
@@ -844,6 +857,7 @@ HZLB_API int hzlb_linearized_drift(int n, const hzlb_parameters *params, const d
             raise(HZLB_EINVAL, "null argument");
         if (count > (1u << 24))
             raise(HZLB_EINVAL, "too many drift pairs");
+        DeviceRestore restore;
         drift_batch(n, *params, states, directions, static_cast<int>(count), false, out, device);
     });
 }
@@ -858,6 +872,7 @@ HZLB_API int hzlb_likelihood_adjoint(const hzlb_dataset *data, const double *log
             raise(HZLB_EINVAL, "too many parameter vectors");
         if (count == 0)
             return;
+        DeviceRestore restore;
         likelihood_adjoint_batch(data, log_parameters, static_cast<int>(count),
                                  static_cast<size_t>(checkpoint_stride), device, out);
     });
@@ -874,6 +889,7 @@ HZLB_API int hzlb_adjoint_drift(int n, const hzlb_parameters *params, const doub
             raise(HZLB_EINVAL, "null argument");
         if (count > (1u << 24))
             raise(HZLB_EINVAL, "too many drift pairs");
+        DeviceRestore restore;
         drift_batch(n, *params, states, cotangents, static_cast<int>(count), true, out, device);
     });
 }

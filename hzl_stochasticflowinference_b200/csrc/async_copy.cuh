@@ -1,5 +1,5 @@
 // Bulk asynchronous global->shared copies (the TMA bulk-copy engine of sm_90/sm_100a) with
-// mbarrier completion, and the waits on them.  Every wait is bounded: a wait that gives up
+// mbarrier completion, shared->global copies in bulk async-groups, and the waits on them.  Every wait is bounded: a wait that gives up
 // reports failure so the caller can set STATUS_TIMEOUT and leave the kernel instead of hanging.
 #pragma once
 #include <cstdint>
@@ -34,6 +34,25 @@ __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32
                  "[%3];" ::"r"(smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+// Bulk copy shared -> global of `bytes` (multiple of 16; both addresses 16-byte aligned), in
+// this thread's current bulk async-group.  Whole 16-byte chunks reach L2 as full sectors, so
+// no partially written sector waits there for a fill from DRAM.
+__device__ __forceinline__ void bulk_copy_s2g(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+                 "r"(smem_u32(src)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// Waits until every committed shared -> global copy of this thread has read its source.
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// Waits until every committed shared -> global copy of this thread has completed.
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t done;

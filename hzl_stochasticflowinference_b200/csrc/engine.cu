@@ -66,7 +66,8 @@ template <typename R> class EngineT final : public Engine {
         omega_.ensure(cb * compact_ * M_ + 16, "allocate GPU state");
         ystage_.ensure(cb * compact_ * M_ + 16, "allocate GPU stage input");
         acc_.ensure(cb * compact_ * M_ + 16, "allocate GPU RK accumulator");
-        w_.ensure(cb * 2 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU velocity columns");
+        w_.ensure(cb * 2 * velocity_row_stride<R>(n_) * static_cast<size_t>(n_) * M_,
+                  "allocate GPU velocity rows");
         nl_.ensure(cb * 2 * C_ * static_cast<size_t>(n_) * M_, "allocate GPU product rows");
         if (fcount_)
             forcing_.ensure(cb * static_cast<size_t>(fcols_) * LD_ * fcount_, "allocate GPU forcing");
@@ -564,7 +565,7 @@ template <typename R> class EngineT final : public Engine {
             a.omega += off;
             a.ystage += off;
             a.acc += off;
-            a.w += static_cast<size_t>(f) * n_ * 2 * C_;
+            a.w += static_cast<size_t>(f) * n_ * 2 * velocity_row_stride<R>(n_);
             a.nl += static_cast<size_t>(f) * 2 * C_ * n_;
             if (a.forcing && a.forcing_stride)
                 a.forcing += static_cast<size_t>(f) * a.forcing_stride;

@@ -71,7 +71,7 @@ template <typename R> Layout layout(int n, int members) {
     l.ystage = l.omega + state;
     l.acc = l.ystage + state;
     l.w = l.acc + state;
-    l.nl = l.w + align256(cb * 2 * n * C * members);
+    l.nl = l.w + align256(cb * 2 * n * velocity_row_stride<R>(n) * members);
     l.total = l.nl + align256(cb * 2 * n * C * members);
     return l;
 }

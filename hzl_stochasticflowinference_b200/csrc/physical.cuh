@@ -89,7 +89,7 @@ template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     velocity_max(const cx<R> *w, unsigned long long *vmax_bits, const cx<R> *tw_g) {
     using G = Cfg<R, N>;
-    constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
+    constexpr int E = G::E, T = G::T, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     cx<R> *tw = reinterpret_cast<cx<R> *>(smem_raw);
     cx<R> *lines = tw + G::TWE;
@@ -97,12 +97,12 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS)
     __syncthreads();
     const int g = threadIdx.x / T, t = threadIdx.x % T, m = blockIdx.x;
     const bool active = g < TY / 2;
-    const cx<R> *wm = w + static_cast<size_t>(m) * N * 2 * C;   // rows [y][field][kx]
+    const cx<R> *wm = w + static_cast<size_t>(m) * N * 2 * G::CW;   // rows [y][field][kx]
     double best = 0;
 #pragma unroll 1
     for (int h = 0; h < 2; ++h) {
         const int y = blockIdx.y * TY + (active ? 2 * g + h : 0);
-        const cx<R> *u = wm + static_cast<size_t>(y) * 2 * C, *v = u + C;
+        const cx<R> *u = wm + static_cast<size_t>(y) * 2 * G::CW, *v = u + G::CW;
         cx<R> z[E];
 #pragma unroll
         for (int r = 0; r < E; ++r) {

@@ -23,7 +23,8 @@
 //                  FFT of (v^2 - u^2) + i (u v), keeping kx = 0..K of each.
 // HBM layouts (complex R):
 //   state / stage input / accumulator  [m][kx][j]          (K+1) x (2K+1) per member
-//   velocity rows W                    [m][y][field][kx]   N x 2 x (K+1)   (u^, v^ per row)
+//   velocity rows W                    [m][y][field][kx]   N x 2 x CW      (u^, v^ per row;
+//                                                                           kx > K zero pad)
 //   product columns NL                 [m][field][kx][y]   2 x (K+1) x N   (v^2-u^2, u v)
 // so each row tile of W and each column group of NL is one contiguous bulk copy.
 #pragma once
@@ -33,6 +34,19 @@
 #include <type_traits>
 
 namespace hzlb {
+
+// Row stride of the velocity rows W in complex entries: C rounded up so that every row starts
+// on a 32-byte sector boundary and each column group's run of LPB entries covers whole sectors
+// (the last group also writes the zero pad entries).  No partially written sector of W then
+// waits in L2 for the neighbouring group's stores, which at large ensembles were evicted first
+// and cost a read of the sector from DRAM.
+template <typename R> __host__ __device__ constexpr int velocity_row_stride(int n) {
+    const int e = n < 16 ? n : 16, t = n / e, c = (n - 1) / 3 + 1;
+    const int lpb = t >= 64 ? 1 : 64 / t;
+    const int per32 = 32 / (2 * static_cast<int>(sizeof(R)));
+    const int q = lpb > per32 ? lpb : per32;
+    return (c + q - 1) / q * q;
+}
 
 // E (elements per thread) keeps a line inside one warp.  16 elements (two radix-16 passes at
 // 256) beat 8 (three passes, twice the threads per line) in both precisions: measured at 256^2,
@@ -48,6 +62,7 @@ template <typename R, int N> struct Cfg {
     static constexpr int LPB = T >= 64 ? 1 : 64 / T;
     static constexpr int COL_THREADS = LPB * T;
     static constexpr int NCG = (C + LPB - 1) / LPB;   // column groups per member
+    static constexpr int CW = velocity_row_stride<R>(N);   // row stride of W
     // state window per array: LPB columns plus one entry of 16-byte alignment slack, rounded
     // up to whole 16-byte chunks
     static constexpr int PER16 = 16 / (2 * static_cast<int>(sizeof(R)));
@@ -61,7 +76,7 @@ template <typename R, int N> struct Cfg {
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
     static constexpr int GROUPS = TY * T >= 32 ? TY : 32 / T;
     static constexpr int ROW_THREADS = GROUPS * T;
-    static constexpr int TILE = TY * 2 * C;           // row tile, complex entries
+    static constexpr int TILE = TY * 2 * CW;          // row tile, complex entries
     static constexpr int TWE = pass_twiddle_entries<N, E>() > 0 ? pass_twiddle_entries<N, E>() : 1;
 };
 
@@ -83,7 +98,7 @@ struct StepControl {
 
 template <typename R> struct ColumnArgs {
     const cx<R> *nl;        // [M][2][C][N]
-    cx<R> *w;               // [M][N][2][C]
+    cx<R> *w;               // [M][N][2][CW]
     cx<R> *omega;           // [M][C][LD]
     cx<R> *ystage;          // [M][C][LD]
     cx<R> *acc;             // [M][C][LD]
@@ -103,7 +118,7 @@ template <typename R> struct ColumnArgs {
 };
 
 template <typename R> struct RowArgs {
-    const cx<R> *w;       // [M][N][2][C]
+    const cx<R> *w;       // [M][N][2][CW]
     cx<R> *nl;            // [M][2][C][N]
     const cx<R> *tw;
     double cfl_scale;     // dt * N / (2 pi); > 0 enables the stage-1 CFL check
@@ -236,6 +251,24 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             bulk_copy_g2s(stbuf + 2 * G::ST_STRIDE, a.acc + base, bytes, &bars[2]);
         }
     };
+    // writes the item's columns of one state array from its window region (updated in place)
+    // back to HBM: the whole 16-byte chunks as one bulk copy, the at most PER16 - 1 entries
+    // before the first and after the last chunk boundary by plain stores (thread 0 alone)
+    auto store_window = [&](cx<R> *dst, int region, int it) {
+        const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
+        const int nl = min(LPB, C - kx0);
+        const size_t off = (static_cast<size_t>(m) * C + kx0) * LD;
+        const size_t end = off + static_cast<size_t>(nl) * LD;
+        const cx<R> *src = stbuf + region * G::ST_STRIDE + static_cast<int>(off % G::PER16);
+        const size_t a0 = min(end, (off + G::PER16 - 1) / G::PER16 * G::PER16);
+        const size_t a1 = max(a0, end / G::PER16 * G::PER16);
+        for (size_t e = off; e < a0; ++e)
+            dst[e] = src[e - off];
+        if (a1 > a0)
+            bulk_copy_s2g(dst + a0, src + (a0 - off), static_cast<uint32_t>((a1 - a0) * sizeof(cx<R>)));
+        for (size_t e = a1; e < end; ++e)
+            dst[e] = src[e - off];
+    };
 
     const int line = threadIdx.x / T, t = threadIdx.x % T;
     if (threadIdx.x < 32 && forward && static_cast<int>(blockIdx.x) < items)
@@ -254,9 +287,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
         int shift;
         uint32_t sbytes;
         window(it, shift, sbytes);
-        const cx<R> *s_w = stbuf + shift + line * LD, *s_y = s_w + G::ST_STRIDE,
-                    *s_a = s_w + 2 * G::ST_STRIDE;
-        const size_t cbase = (static_cast<size_t>(m) * C + kxc) * LD;
+        // this line's columns in the window regions, updated in place by the epilogue
+        cx<R> *s_w = stbuf + shift + line * LD, *s_y = s_w + G::ST_STRIDE,
+              *s_a = s_w + 2 * G::ST_STRIDE;
         const R kxr = static_cast<R>(kxc);
 
         cx<R> y[E];   // next stage input at this thread's positions (zero outside the band)
@@ -330,19 +363,18 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                             kk = kk + a.forcing[static_cast<size_t>(m) * a.forcing_stride +
                                                 static_cast<size_t>(kxc) * LD + j];
                     }
-                    const size_t idx = cbase + j;
                     if constexpr (S == 1) {
-                        a.acc[idx] = kk;
+                        s_a[j] = kk;
                         y[r] = wn + scale(dt / 2, kk);
-                        a.ystage[idx] = y[r];
+                        s_y[j] = y[r];
                     } else if constexpr (S == 2) {
-                        a.acc[idx] = s_a[j] + scale(static_cast<R>(2.0), kk);
+                        s_a[j] = s_a[j] + scale(static_cast<R>(2.0), kk);
                         y[r] = wn + scale(dt / 2, kk);
-                        a.ystage[idx] = y[r];
+                        s_y[j] = y[r];
                     } else if constexpr (S == 3) {
-                        a.acc[idx] = s_a[j] + scale(static_cast<R>(2.0), kk);
+                        s_a[j] = s_a[j] + scale(static_cast<R>(2.0), kk);
                         y[r] = wn + scale(dt, kk);
-                        a.ystage[idx] = y[r];
+                        s_y[j] = y[r];
                     } else {
                         // w += dt/6 (k1 + 2 k2 + 2 k3 + k4)   (solver.cpp:233-234)
                         cx<R> w1 = wn + scale(dt / 6, s_a[j] + kk);
@@ -358,13 +390,27 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                                             static_cast<R>(rep ? s * xi2 : -(s * xi2)));
                         }
                         bad |= !(isfinite(w1.x) && isfinite(w1.y));
-                        a.omega[idx] = w1;
+                        s_w[j] = w1;
                         y[r] = w1;
                     }
                 }
             });
             if (bad)
                 atomicOr(&a.ctl->status, STATUS_NONFINITE);
+            // the item's new state leaves from the window in bulk; the window is reused below
+            // and by the next item's copies once the engine has read it
+            fence_proxy_async_shared();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                if constexpr (S == 4) {
+                    store_window(a.omega, 0, it);
+                } else {
+                    store_window(a.ystage, 1, it);
+                    store_window(a.acc, 2, it);
+                }
+                bulk_commit();
+                bulk_wait_read_all();
+            }
         }
 
         if (a.emit) {
@@ -392,7 +438,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             });
             cx<R> *wst = stbuf + LPB * G::LS;   // one field's rows [N][LPB]
             const int nl = min(LPB, C - kx0);
-            cx<R> *dst = a.w + static_cast<size_t>(m) * N * 2 * C + kx0;
+            // runs of the group's columns and, in the last group, of the zero pad up to CW
+            const int nw = min(LPB, G::CW - kx0);
+            cx<R> *dst = a.w + static_cast<size_t>(m) * N * 2 * G::CW + kx0;
 #pragma unroll 1
             for (int f = 0; f < 2; ++f) {
                 static_for<0, E>([&](auto rc) {
@@ -414,14 +462,16 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 __syncthreads();
                 for (int i = threadIdx.x; i < N * LPB; i += blockDim.x) {
                     const int l = i % LPB, yy = i / LPB;
-                    if (l < nl)
-                        dst[(static_cast<size_t>(yy) * 2 + f) * C + l] = wst[yy * LPB + (l ^ swz<LPB>(yy))];
+                    if (l < nw)
+                        dst[(static_cast<size_t>(yy) * 2 + f) * G::CW + l] = wst[yy * LPB + (l ^ swz<LPB>(yy))];
                 }
             }
         }
         fence_proxy_async_shared();   // this thread's shared-memory accesses precede the next bulk copies
         __syncthreads();              // buffers of this item are free for the next copies
     }
+    if (threadIdx.x == 0)
+        bulk_wait_all();   // this block's state stores are complete before it leaves
     if (timed_out) {
         if (threadIdx.x == 0)
             atomicOr(&a.ctl->status, STATUS_TIMEOUT);
@@ -494,7 +544,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // input tile [TY][2][C], refilled with the next item's tile as soon as every row has read
+    // input tile [TY][2][CW], refilled with the next item's tile as soon as every row has read
     // its entries; FFT line buffers [GROUPS][BUF], reused once every row has finished its
     // transforms as the staging of the product spectra [2C][TY] (swizzled rows)
     cx<R> *tile = reinterpret_cast<cx<R> *>(smem_raw);
@@ -517,7 +567,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
     auto issue = [&](int it) {
         const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
         mbar_arrive_expect(&bar, tile_bytes);
-        bulk_copy_g2s(tile, a.w + (static_cast<size_t>(m) * N + y0) * 2 * C, tile_bytes, &bar);
+        bulk_copy_g2s(tile, a.w + (static_cast<size_t>(m) * N + y0) * 2 * G::CW, tile_bytes, &bar);
     };
     if (threadIdx.x == 0 && static_cast<int>(blockIdx.x) < items)
         issue(blockIdx.x);
@@ -534,9 +584,9 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
                 atomicOr(&a.ctl->status, STATUS_TIMEOUT);
             return;   // uniform across the block
         }
-        const cx<R> *row = tile + ty * 2 * C;
+        const cx<R> *row = tile + ty * 2 * G::CW;
         cx<R> z[E];
-        pack_row<N, E, R>(z, row, row + C, t);
+        pack_row<N, E, R>(z, row, row + G::CW, t);
         // every row holds its inputs in registers: stream the next item's tile in
         fence_proxy_async_shared();
         __syncthreads();

@@ -61,11 +61,11 @@ DT = 2.5e-4
 SIGMA = 0.05
 SEED = 42
 METRIC = "ensemble member-steps/s at 256^2"
-# DRAM bytes (read + write) per member per launch, from one ncu capture of 256 members at
-# 256^2 FP32 (profiles/row_kernel_256sq_fp32.md, profiles/column_kernel_256sq_fp32.md; the
-# column figure is the mean of its four RK-stage launches, like its algorithmic bytes); the
-# traffic grows in proportion to the members processed, so a full launch is this x members.
-NCU_TRAFFIC_PER_MEMBER = {"row_kernel": 524129.0, "column_kernel": 1001999.0}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per member per launch, from one
+# single-pass ncu capture of this benchmark's own 2048-member launches at 256^2 FP32 (the
+# column figure is the mean of its four RK-stage launches, like its algorithmic bytes),
+# scaled by the members processed for other ensemble sizes.
+NCU_TRAFFIC_PER_MEMBER = {"row_kernel": 690983.0, "column_kernel": 1186247.0}
 
 
 def peaks():

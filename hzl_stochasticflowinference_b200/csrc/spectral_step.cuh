@@ -35,16 +35,17 @@
 
 namespace hzlb {
 
-// Row stride of the velocity rows W in complex entries: C rounded up to whole 32-byte sectors,
-// so that every row starts on a sector boundary.  A column group's run of LPB entries (a whole
-// number of sectors while LPB >= 4 in FP32, >= 2 in FP64: n <= 256 and n <= 512) then covers
-// whole sectors, the last group's including the zero pad up to the stride.  No partially
-// written sector of W waits in L2 for the neighbouring group's stores, which at large ensembles
-// were evicted first and cost a read of the sector from DRAM.
+// Row stride of the velocity rows W in complex entries: C rounded up so that every row starts
+// on a 32-byte sector boundary and each column group's run of LPB entries covers whole sectors
+// (the last group also writes the zero pad entries).  No partially written sector of W then
+// waits in L2 for the neighbouring group's stores, which at large ensembles were evicted first
+// and cost a read of the sector from DRAM.
 template <typename R> __host__ __device__ constexpr int velocity_row_stride(int n) {
-    const int c = (n - 1) / 3 + 1;
+    const int e = n < 16 ? n : 16, t = n / e, c = (n - 1) / 3 + 1;
+    const int lpb = t >= 64 ? 1 : 64 / t;
     const int per32 = 32 / (2 * static_cast<int>(sizeof(R)));
-    return (c + per32 - 1) / per32 * per32;
+    const int q = lpb > per32 ? lpb : per32;
+    return (c + q - 1) / q * q;
 }
 
 // E (elements per thread) keeps a line inside one warp.  16 elements (two radix-16 passes at

@@ -195,6 +195,38 @@ def test_batch_composition_independence(hzlb):
     np.testing.assert_array_equal(small.get_state_compact(), big.get_state_compact(4, 2))
 
 
+@pytest.mark.parametrize("precision,members", [(4, 2048), (8, 512)])
+def test_batch_independence_at_benchmark_size(hzlb, precision, members):
+    """At the benchmark's own size (256^2, 2048 FP32 members; 512 in FP64) the first, a middle
+    and the last two members are bit-identical with the same members stepped alone in a
+    two-member ensemble (member_base selects their noise streams): the whole-ensemble column
+    groups, state windows and velocity rows address every member correctly."""
+    n, dt, seed = 256, 2.5e-4, 42
+    ctype = np.complex64 if precision == 4 else np.complex128
+    w0 = hzlb.full_to_compact(hzlb.grf_spectrum(n, seed, 0), n)[0].astype(ctype)
+
+    def run(count, base):
+        cfg = hzlb.Config(n=n, members=count, precision=precision, nu=2.5e-4, alpha=0.0,
+                          forcing_kmax=0, noise_sigma=0.05, noise_kmax=4, seed=seed,
+                          member_base=base)
+        e = hzlb.Ensemble(cfg)
+        e.set_state_compact(np.repeat(w0[None], count, 0))
+        e.set_forcing(hzlb.kolmogorov_forcing(n)[None])
+        e.set_time(0.0, 0)
+        e.step(dt, 3)
+        return e
+
+    big = run(members, 0)
+    assert big.status() == 0
+    for first in (0, members // 2 - 1, members - 2):
+        small = run(2, first)
+        np.testing.assert_array_equal(small.get_state_compact(), big.get_state_compact(first, 2))
+        small.close()
+    # the members differ (their noise does), so the comparison is not of copies of one field
+    assert not np.array_equal(big.get_state_compact(0, 1), big.get_state_compact(members - 1, 1))
+    big.close()
+
+
 def test_cfl_violation_is_flagged(hzlb):
     n = 32
     e = hzlb.Ensemble(hzlb.Config(n=n, members=1, precision=8, nu=0.0))

@@ -13,9 +13,10 @@ Reference correspondences (paths relative to the reference repository):
 * :meth:`Ensemble.diagnostics` -- ``Solver::diagnostics`` per member (src/solver.cpp:381-397).
 * :meth:`Ensemble.observe` -- ``Solver::physical_vorticity`` sampled at sensors
   (src/solver.cpp:398-402).
-* :meth:`Ensemble.pf_loglik`, :func:`pf_weights`, :func:`systematic_resample`,
-  :meth:`Ensemble.gather` -- the weight and resample steps of ``bootstrap_filter``
-  (src/filter.cpp:66-120).
+* :meth:`Ensemble.pf_assimilate` (with :meth:`Ensemble.pf_reset`), :meth:`Ensemble.pf_loglik`,
+  :meth:`Ensemble.pf_weights`, :meth:`Ensemble.resample`, :meth:`Ensemble.gather` -- the
+  weight and resample steps of ``bootstrap_filter`` (src/filter.cpp:65-120), in FP64 on the
+  device.
 * :meth:`Ensemble.inflate`, :meth:`Ensemble.enkf_analysis` -- the analysis of
   ``ensemble_kalman_filter`` (src/filter.cpp:237-321) in batched form.
 """
@@ -52,6 +53,11 @@ class hzlb_parameters(C.Structure):
     _fields_ = [("viscosity", C.c_double), ("friction", C.c_double),
                 ("forcing_sigma", C.c_double), ("forcing_tau", C.c_double),
                 ("forcing_min", C.c_int), ("forcing_max", C.c_int)]
+
+
+class hzlb_pf_record(C.Structure):
+    _fields_ = [("increment", C.c_double), ("ess", C.c_double), ("max_weight", C.c_double),
+                ("resampled", C.c_int32), ("collapsed", C.c_int32)]
 
 
 class hzlb_observation(C.Structure):
@@ -134,7 +140,12 @@ def library() -> C.CDLL:
         "hzlb_physical": (C.c_int, [vp, _dp]),
         "hzlb_observe": (C.c_int, [vp, _u32p, _u32p, C.c_size_t, _dp]),
         "hzlb_pf_loglik": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp]),
-        "hzlb_pf_weights": (C.c_int, [_dp, C.c_size_t, _dp, _dp, _dp, _dp]),
+        "hzlb_pf_weights": (C.c_int, [vp, _dp, C.c_size_t, _dp, _dp, _dp, _dp]),
+        "hzlb_pf_reset": (C.c_int, [vp, C.c_int]),
+        "hzlb_pf_assimilate": (C.c_int, [vp, _u32p, _u32p, _dp, _dp, C.c_size_t, _dp,
+                                         C.POINTER(C.c_uint8), C.POINTER(hzlb_pf_record), _u32p,
+                                         _dp]),
+        "hzlb_pf_get_weights": (C.c_int, [vp, _dp]),
         "hzlb_systematic_resample": (C.c_int, [vp, _dp, C.c_size_t, C.c_double, _u32p]),
         "hzlb_gather_members": (C.c_int, [vp, _u32p]),
         "hzlb_inflate": (C.c_int, [vp, C.c_double]),
@@ -445,6 +456,57 @@ class Ensemble:
         _check(self._lib.hzlb_pf_loglik(self._h, _pu(x), _pu(y), _p(v), _p(s), len(x), _p(lw)))
         return lw
 
+    def pf_weights(self, log_weights):
+        """(weights, increment, ess, max_weight) of host log-weights (filter.cpp:76-92),
+        computed on this ensemble's device."""
+        lw = _f64(log_weights)
+        w = np.zeros_like(lw)
+        inc, ess, mw = C.c_double(), C.c_double(), C.c_double()
+        _check(self._lib.hzlb_pf_weights(self._h, _p(lw), len(lw), _p(w), C.byref(inc),
+                                         C.byref(ess), C.byref(mw)))
+        return w, inc.value, ess.value, mw.value
+
+    def pf_reset(self, particles: int | None = None):
+        """members / particles independent filters, device weights reset to 1/particles."""
+        particles = self.members if particles is None else int(particles)
+        _check(self._lib.hzlb_pf_reset(self._h, particles))
+        self._pf_particles = particles
+
+    def pf_assimilate(self, x, y, values, sd, u=None, active=None, weighted_mean: bool = False):
+        """One observation time of every segment's bootstrap filter on the device
+        (hzlb_pf_assimilate).  u: per-segment uniforms (negative: no resampling) or None.
+        Returns dict(increment, ess, max_weight, resampled, collapsed: per-segment arrays,
+        ancestors: members, mean: (segments, compact) complex128 when weighted_mean)."""
+        x, y, v, s = _u32(x), _u32(y), _f64(values), _f64(sd)
+        segments = self.members // self._particles() if u is None and active is None else None
+        if u is not None:
+            uu = _f64(np.atleast_1d(u))
+            segments = len(uu)
+        if active is not None:
+            act = np.ascontiguousarray(np.asarray(active, np.uint8))
+            segments = len(act)
+        recs = (hzlb_pf_record * segments)()
+        anc = np.zeros(self.members, np.uint32)
+        mean = np.zeros((segments, self.compact_size), np.complex128) if weighted_mean else None
+        _check(self._lib.hzlb_pf_assimilate(
+            self._h, _pu(x), _pu(y), _p(v), _p(s), len(x), None if u is None else _p(uu),
+            None if active is None else act.ctypes.data_as(C.POINTER(C.c_uint8)), recs, _pu(anc),
+            None if mean is None else mean.view(np.float64).ctypes.data_as(_dp)))
+        out = {k: np.array([getattr(r, k) for r in recs])
+               for k in ("increment", "ess", "max_weight", "resampled", "collapsed")}
+        out["ancestors"] = anc
+        if mean is not None:
+            out["mean"] = mean
+        return out
+
+    def _particles(self) -> int:
+        return getattr(self, "_pf_particles", self.members)
+
+    def pf_get_weights(self) -> np.ndarray:
+        out = np.zeros(self.members)
+        _check(self._lib.hzlb_pf_get_weights(self._h, _p(out)))
+        return out
+
     def resample(self, weights, u: float) -> np.ndarray:
         w = _f64(weights)
         out = np.zeros(len(w), np.uint32)
@@ -523,24 +585,6 @@ class Ensemble:
         ptr = C.c_void_p()
         _check(self._lib.hzlb_state_device(self._h, C.byref(ptr)))
         return ptr.value
-
-
-def pf_weights(log_weights):
-    """(weights, increment, ess, max_weight) as in filter.cpp:76-92."""
-    lw = _f64(log_weights)
-    w = np.zeros_like(lw)
-    inc, ess, mw = C.c_double(), C.c_double(), C.c_double()
-    _check(library().hzlb_pf_weights(_p(lw), len(lw), _p(w), C.byref(inc), C.byref(ess),
-                                     C.byref(mw)))
-    return w, inc.value, ess.value, mw.value
-
-
-def systematic_resample(weights, u: float) -> np.ndarray:
-    """Host systematic resampling (filter.cpp:102-112); see Ensemble.resample for the device."""
-    w = _f64(weights)
-    out = np.zeros(len(w), np.uint32)
-    _check(library().hzlb_systematic_resample(None, _p(w), len(w), u, _pu(out)))
-    return out
 
 
 def grf_spectrum(n: int, seed: int, member: int) -> np.ndarray:

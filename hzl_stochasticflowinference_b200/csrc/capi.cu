@@ -161,34 +161,22 @@ int hzlb_pf_loglik(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, const
         need(log_weights, "log_weights");
         if (p == 0)
             return;
+        need(x, "x");
+        need(y, "y");
         need(values, "values");
         need(sd, "sd");
-        auto &e = engine(h);
-        const size_t members = static_cast<size_t>(e.members());
-        std::vector<double> field(members * p);
-        e.observe(x, y, p, field.data());
-        // filter.cpp:66-74, member by member in the reference's order of operations
-        const double log_two_pi = std::log(2 * 3.141592653589793238462643383279502884);
-        for (size_t m = 0; m < members; ++m) {
-            double value = log_weights[m];
-            for (size_t o = 0; o < p; ++o) {
-                const double residual = (field[m * p + o] - values[o]) / sd[o];
-                value -= 0.5 * residual * residual + std::log(sd[o]) + 0.5 * log_two_pi;
-            }
-            log_weights[m] = value;
-        }
+        engine(h).pf_loglik(x, y, values, sd, p, log_weights);
     });
 }
-
-int hzlb_pf_weights(const double *log_weights, size_t count, double *weights, double *increment,
-                    double *ess, double *max_weight) {
+int hzlb_pf_weights(hzlb_ensemble *h, const double *log_weights, size_t count, double *weights,
+                    double *increment, double *ess, double *max_weight) {
     return guarded([&] {
         need(log_weights, "log_weights");
         need(weights, "weights");
         need(increment, "increment");
         need(ess, "ess");
         need(max_weight, "max_weight");
-        hzlb::pf_weights_host(log_weights, count, weights, increment, ess, max_weight);
+        engine(h).pf_weights(log_weights, count, weights, increment, ess, max_weight);
     });
 }
 int hzlb_systematic_resample(hzlb_ensemble *h, const double *weights, size_t count, double u,
@@ -200,10 +188,30 @@ int hzlb_systematic_resample(hzlb_ensemble *h, const double *weights, size_t cou
             hzlb::raise(HZLB_EINVAL, "resampling needs at least one weight");
         if (!std::isfinite(u) || u < 0 || u >= 1)
             hzlb::raise(HZLB_EINVAL, "resampling uniform must lie in [0, 1)");
-        if (h)
-            engine(h).resample(weights, count, u, ancestors);
-        else
-            hzlb::systematic_resample_host(weights, count, u, ancestors);
+        engine(h).resample(weights, count, u, ancestors);
+    });
+}
+int hzlb_pf_reset(hzlb_ensemble *h, int particles) {
+    return guarded([&] { engine(h).pf_reset(particles); });
+}
+int hzlb_pf_assimilate(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, const double *values,
+                       const double *sd, size_t p, const double *u, const uint8_t *active,
+                       hzlb_pf_record *records, uint32_t *ancestors, double *weighted_mean) {
+    return guarded([&] {
+        need(records, "records");
+        if (p) {
+            need(x, "x");
+            need(y, "y");
+            need(values, "values");
+            need(sd, "sd");
+        }
+        engine(h).pf_assimilate(x, y, values, sd, p, u, active, records, ancestors, weighted_mean);
+    });
+}
+int hzlb_pf_get_weights(hzlb_ensemble *h, double *weights) {
+    return guarded([&] {
+        need(weights, "weights");
+        engine(h).pf_get_weights(weights);
     });
 }
 int hzlb_gather_members(hzlb_ensemble *h, const uint32_t *ancestors) {

@@ -780,12 +780,18 @@ HZLB_API int hzlb_bootstrap_filter(const hzlb_dataset *data, const hzlb_paramete
         const int M = static_cast<int>(count), n = ds.n;
         RefEnsemble e(n, p, M, seed, precision, device);
         e.set_initial("multimode");
-        std::vector<double> weights(M, 1 / static_cast<double>(M)), logs(M), w(M);
+        // weights live on the device (uniform 1/M); the resampling uniform is drawn ahead
+        // and kept until a resampling consumes it, so the engine's sequence is the reference's
+        e.engine->pf_reset(M);
         std::mt19937_64 resampling(stream_seed(seed, std::numeric_limits<uint64_t>::max()));
+        bool pending = false;
+        double next_u = 0;
         double ll = 0;
         uint64_t events = 0;
         size_t nrec = 0, current = 0, begin = 0, group = 0;
         const size_t nn = static_cast<size_t>(n) * n;
+        std::vector<uint32_t> anc(M);
+        std::vector<double> mean;
         while (begin < ds.obs.size()) {
             const uint64_t target = ds.obs[begin].step;
             size_t end = begin;
@@ -794,59 +800,52 @@ HZLB_API int hzlb_bootstrap_filter(const hzlb_dataset *data, const hzlb_paramete
             for (uint64_t s = current; s < target; ++s)
                 e.step(ds.dt);
             e.check_status();
-            // log-weights (filter.cpp:65-75)
+            // log-weights, normalisation and (when the ESS falls below M/2 before the last
+            // observation time) resampling and the member gather, on the device
+            // (filter.cpp:65-112)
             const size_t p_count = end - begin;
             std::vector<uint32_t> xs(p_count), ys(p_count);
+            std::vector<double> vals(p_count), sds(p_count);
             for (size_t o = 0; o < p_count; ++o) {
-                xs[o] = ds.obs[begin + o].x;
-                ys[o] = ds.obs[begin + o].y;
+                const auto &ob = ds.obs[begin + o];
+                xs[o] = ob.x;
+                ys[o] = ob.y;
+                vals[o] = ob.value;
+                sds[o] = ob.standard_deviation;
             }
-            std::vector<double> field(static_cast<size_t>(M) * p_count);
-            e.engine->observe(xs.data(), ys.data(), p_count, field.data());
-            const double half_log_two_pi = 0.5 * std::log(2 * kPi);
-            for (int i = 0; i < M; ++i) {
-                double value = weights[i] > 0 ? std::log(weights[i])
-                                              : -std::numeric_limits<double>::infinity();
-                for (size_t o = 0; o < p_count; ++o) {
-                    const auto &ob = ds.obs[begin + o];
-                    const double residual = (field[i * p_count + o] - ob.value) / ob.standard_deviation;
-                    value -= 0.5 * residual * residual + std::log(ob.standard_deviation) +
-                             half_log_two_pi;
+            double u = -1;
+            if (end < ds.obs.size()) {
+                if (!pending) {
+                    next_u = static_cast<double>(resampling() >> 11) * 0x1.0p-53;
+                    pending = true;
                 }
-                logs[i] = value;
+                u = next_u;
             }
-            double maximum = logs[0];
-            for (int i = 1; i < M; ++i)
-                if (maximum < logs[i])
-                    maximum = logs[i];
-            if (!std::isfinite(maximum)) {
+            const bool want_mean = retain_states && mean_vorticity && nrec < capacity;
+            if (want_mean)
+                mean.resize(2 * e.engine->compact_size());
+            hzlb_pf_record rec{};
+            e.engine->pf_assimilate(xs.data(), ys.data(), vals.data(), sds.data(), p_count, &u,
+                                    nullptr, &rec, anc.data(), want_mean ? mean.data() : nullptr);
+            if (rec.collapsed) {
                 ll = -std::numeric_limits<double>::infinity();
                 break;
             }
-            double inc = 0, ess = 0, mw = 0;
-            pf_weights_host(logs.data(), M, w.data(), &inc, &ess, &mw);
-            weights = w;
-            ll += inc;
+            ll += rec.increment;
             if (nrec < capacity) {
-                records[nrec] = {target, inc, ess, mw};
-                if (retain_states && mean_vorticity) {
-                    std::vector<double> mean(2 * e.engine->compact_size());
-                    e.engine->member_sum(weights.data(), 0.0, mean.data());
+                records[nrec] = {target, rec.increment, rec.ess, rec.max_weight};
+                if (want_mean) {
                     auto full = compact_to_full(n, mean);
                     host_fft2(n, full, true);
                     std::memcpy(mean_vorticity + 2 * nrec * nn, full.data(), sizeof(cd) * nn);
                 }
             }
             ++nrec;
-            if (ess < static_cast<double>(M) / 2 && end < ds.obs.size()) {
-                const double u = static_cast<double>(resampling() >> 11) * 0x1.0p-53;
-                std::vector<uint32_t> anc(M);
-                e.engine->resample(weights.data(), M, u, anc.data());
-                e.engine->gather(anc.data());
+            if (rec.resampled) {
+                pending = false;
                 e.bank.gather(anc);
                 for (int i = 0; i < M; ++i)
                     e.bank.reseed(i, stream_seed(seed, (group + 1) * count + i));
-                std::fill(weights.begin(), weights.end(), 1 / static_cast<double>(M));
                 ++events;
             }
             current = target;
@@ -912,8 +911,13 @@ HZLB_API int hzlb_particle_log_likelihood(const hzlb_dataset *data, const double
         }
         RefEnsemble e(n, p, member_seed, precision, device);
         e.set_initial("multimode");
-        std::vector<double> weights(M, 1 / static_cast<double>(P)), ll(R, 0.0), logs(P), w(P);
-        std::vector<char> done(R, 0);
+        // R segments of P particles, weights on the device; each replicate's resampling
+        // uniform is drawn ahead and kept until its segment resamples
+        e.engine->pf_reset(P);
+        std::vector<double> ll(R, 0.0), u(R, -1.0), next_u(R, 0.0);
+        std::vector<uint8_t> active(R, 1), pending(R, 0);
+        std::vector<hzlb_pf_record> recs(R);
+        std::vector<uint32_t> anc(M);
         std::vector<std::mt19937_64> resampling;
         for (int r = 0; r < R; ++r)
             resampling.emplace_back(stream_seed(rseed[r], std::numeric_limits<uint64_t>::max()));
@@ -928,72 +932,60 @@ HZLB_API int hzlb_particle_log_likelihood(const hzlb_dataset *data, const double
             e.check_status();
             const size_t pc = end - begin;
             std::vector<uint32_t> xs(pc), ys(pc);
+            std::vector<double> vals(pc), sds(pc);
             for (size_t o = 0; o < pc; ++o) {
-                xs[o] = ds.obs[begin + o].x;
-                ys[o] = ds.obs[begin + o].y;
+                const auto &ob = ds.obs[begin + o];
+                xs[o] = ob.x;
+                ys[o] = ob.y;
+                vals[o] = ob.value;
+                sds[o] = ob.standard_deviation;
             }
-            std::vector<double> field(static_cast<size_t>(M) * pc);
-            e.engine->observe(xs.data(), ys.data(), pc, field.data());
-            const double half_log_two_pi = 0.5 * std::log(2 * kPi);
-            std::vector<uint32_t> anc(M);
-            for (int i = 0; i < M; ++i)
-                anc[i] = static_cast<uint32_t>(i);
-            bool any_resampled = false;
+            const bool may_resample = end < ds.obs.size();
+            for (int r = 0; r < R; ++r) {
+                u[r] = -1;
+                if (active[r] && may_resample) {
+                    if (!pending[r]) {
+                        next_u[r] = static_cast<double>(resampling[r]() >> 11) * 0x1.0p-53;
+                        pending[r] = 1;
+                    }
+                    u[r] = next_u[r];
+                }
+            }
+            e.engine->pf_assimilate(xs.data(), ys.data(), vals.data(), sds.data(), pc, u.data(),
+                                    active.data(), recs.data(), anc.data(), nullptr);
             std::vector<int> resampled_replicates, retired;
             for (int r = 0; r < R; ++r) {
-                if (done[r])
+                if (!active[r])
                     continue;
-                const double *wr = weights.data() + static_cast<size_t>(r) * P;
-                for (int j = 0; j < P; ++j) {
-                    double value = wr[j] > 0 ? std::log(wr[j]) : ninf;
-                    for (size_t o = 0; o < pc; ++o) {
-                        const auto &ob = ds.obs[begin + o];
-                        const double residual =
-                            (field[static_cast<size_t>(r * P + j) * pc + o] - ob.value) / ob.standard_deviation;
-                        value -= 0.5 * residual * residual + std::log(ob.standard_deviation) + half_log_two_pi;
-                    }
-                    logs[j] = value;
-                }
-                double maximum = logs[0];
-                for (int j = 1; j < P; ++j)
-                    if (maximum < logs[j])
-                        maximum = logs[j];
-                if (!std::isfinite(maximum)) {
+                if (recs[r].collapsed) {
                     ll[r] = ninf;
-                    done[r] = 1;
+                    active[r] = 0;
                     retired.push_back(r);
                     continue;
                 }
-                double inc = 0, ess = 0, mw = 0;
-                pf_weights_host(logs.data(), P, w.data(), &inc, &ess, &mw);
-                std::copy(w.begin(), w.end(), weights.begin() + static_cast<size_t>(r) * P);
-                ll[r] += inc;
-                if (ess < static_cast<double>(P) / 2 && end < ds.obs.size()) {
-                    const double u = static_cast<double>(resampling[r]() >> 11) * 0x1.0p-53;
-                    std::vector<uint32_t> local(P);
-                    systematic_resample_host(w.data(), P, u, local.data());
-                    for (int j = 0; j < P; ++j)
-                        anc[r * P + j] = static_cast<uint32_t>(r * P) + local[j];
-                    std::fill(weights.begin() + static_cast<size_t>(r) * P,
-                              weights.begin() + static_cast<size_t>(r + 1) * P, 1 / static_cast<double>(P));
+                ll[r] += recs[r].increment;
+                if (recs[r].resampled) {
+                    pending[r] = 0;
                     resampled_replicates.push_back(r);
-                    any_resampled = true;
                 }
             }
-            const auto live = std::find(done.begin(), done.end(), 0);
-            if (live == done.end())
+            const auto live = std::find(active.begin(), active.end(), 1);
+            if (live == active.end())
                 break;
             // a replicate that has ended stops being weighted; its members are overwritten by
             // a copy of a live member so that they stay finite while the others advance
+            // (the resampled segments were gathered on the device already)
             if (!retired.empty()) {
-                const uint32_t source = static_cast<uint32_t>((live - done.begin()) * P);
+                const uint32_t source = static_cast<uint32_t>((live - active.begin()) * P);
+                std::vector<uint32_t> patch(M);
+                for (int i = 0; i < M; ++i)
+                    patch[i] = static_cast<uint32_t>(i);
                 for (int r : retired)
                     for (int j = 0; j < P; ++j)
-                        anc[r * P + j] = source;
-                any_resampled = true;
+                        anc[r * P + j] = patch[r * P + j] = source;
+                e.engine->gather(patch.data());
             }
-            if (any_resampled) {
-                e.engine->gather(anc.data());
+            if (!resampled_replicates.empty() || !retired.empty()) {
                 e.bank.gather(anc);
                 for (int r : resampled_replicates)
                     for (int j = 0; j < P; ++j)

@@ -787,6 +787,179 @@ template <typename R> class EngineT final : public Engine {
         cuda_check(cudaStreamSynchronize(stream_), "observation download");
     }
 
+    // ---- particle filter on the device (filter.cpp:65-120) -----------------------------
+    static constexpr int kPfThreads = 256;
+    double half_log_two_pi() const { return 0.5 * std::log(2 * kPi); }
+    void pf_ensure() {
+        if (pf_particles_ == 0)
+            pf_reset(M_);
+    }
+    void pf_reset(int particles) override {
+        if (particles < 2)
+            raise(HZLB_EINVAL, "particle filter needs at least two particles");
+        if (M_ % particles != 0)
+            raise(HZLB_EINVAL, "ensemble members must be a multiple of the particle count");
+        const int segments = M_ / particles;
+        pfw_.ensure(sizeof(double) * 3 * static_cast<size_t>(M_), "allocate particle weights");
+        pfrec_.ensure(sizeof(PfRecord) * segments, "allocate particle records");
+        pfctl_.ensure(sizeof(double) * segments + segments + 16, "allocate particle controls");
+        anc_.ensure(sizeof(unsigned) * M_, "allocate ancestors");
+        std::vector<double> w(M_, 1 / static_cast<double>(particles));
+        cuda_check(cudaMemcpyAsync(pfw_.ptr, w.data(), sizeof(double) * M_, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "reset particle weights");
+        cuda_check(cudaStreamSynchronize(stream_), "reset particle weights");
+        pf_particles_ = particles;
+    }
+    void pf_get_weights(double *out) override {
+        pf_ensure();
+        cuda_check(cudaMemcpyAsync(out, pfw_.ptr, sizeof(double) * M_, cudaMemcpyDeviceToHost, stream_),
+                   "download particle weights");
+        cuda_check(cudaStreamSynchronize(stream_), "download particle weights");
+    }
+    // observed values and uncertainties of p observations into a device buffer (2p doubles)
+    const double *pf_upload_obs(const double *values, const double *sd, size_t p) {
+        for (size_t o = 0; o < p; ++o)
+            if (!std::isfinite(values[o]) || !std::isfinite(sd[o]) || sd[o] <= 0)
+                raise(HZLB_EINVAL, "observations must be finite and have positive uncertainty");
+        pfobs_.ensure(sizeof(double) * 2 * std::max<size_t>(p, 1), "allocate observations");
+        cuda_check(cudaMemcpyAsync(pfobs_.ptr, values, sizeof(double) * p, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "upload observations");
+        cuda_check(cudaMemcpyAsync(pfobs_.as<double>() + p, sd, sizeof(double) * p,
+                                   cudaMemcpyHostToDevice, stream_),
+                   "upload observation errors");
+        return pfobs_.as<double>();
+    }
+    void pf_loglik(const uint32_t *x, const uint32_t *y, const double *values, const double *sd,
+                   size_t p, double *log_weights) override {
+        pf_ensure();
+        const double *ob = pf_upload_obs(values, sd, p);
+        observe_device(x, y, p);
+        double *logs = pfw_.as<double>() + M_;
+        cuda_check(cudaMemcpyAsync(logs, log_weights, sizeof(double) * M_, cudaMemcpyHostToDevice,
+                                   stream_),
+                   "upload log-weights");
+        pf_loglik_kernel<<<(M_ + 127) / 128, 128, 0, stream_>>>(
+            obs_.as<double>(), static_cast<int>(p), ob, ob + p, half_log_two_pi(), nullptr, logs, M_,
+            M_, nullptr);
+        cuda_check(cudaGetLastError(), "launch particle log-likelihood");
+        cuda_check(cudaMemcpyAsync(log_weights, logs, sizeof(double) * M_, cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "download log-weights");
+        cuda_check(cudaStreamSynchronize(stream_), "particle log-likelihood");
+    }
+    void pf_weights(const double *logs, size_t count, double *w, double *inc, double *ess,
+                    double *mw) override {
+        if (count < 2)
+            raise(HZLB_EINVAL, "particle filter needs at least two particles");
+        if (count > (1u << 24))
+            raise(HZLB_EINVAL, "too many particle weights");
+        // logs, weights, scratch, then the record and ancestors
+        const size_t bytes = sizeof(double) * 3 * count + sizeof(PfRecord) + sizeof(unsigned) * count;
+        pfone_.ensure(bytes + 64, "allocate particle weights");
+        double *dl = pfone_.as<double>(), *dw = dl + count, *dx = dw + count;
+        PfRecord *rec = reinterpret_cast<PfRecord *>(dx + count);
+        unsigned *anc = reinterpret_cast<unsigned *>(rec + 1);
+        cuda_check(cudaMemcpyAsync(dl, logs, sizeof(double) * count, cudaMemcpyHostToDevice, stream_),
+                   "upload log-weights");
+        pf_normalise_kernel<kPfThreads><<<1, kPfThreads, 0, stream_>>>(
+            dl, dw, dx, static_cast<int>(count), nullptr, nullptr, rec, anc);
+        cuda_check(cudaGetLastError(), "launch particle weights");
+        PfRecord r{};
+        cuda_check(cudaMemcpyAsync(&r, rec, sizeof r, cudaMemcpyDeviceToHost, stream_),
+                   "download particle record");
+        cuda_check(cudaMemcpyAsync(w, dw, sizeof(double) * count, cudaMemcpyDeviceToHost, stream_),
+                   "download particle weights");
+        cuda_check(cudaStreamSynchronize(stream_), "particle weights");
+        if (r.collapsed)
+            raise(HZLB_ERUNTIME, "particle likelihood collapsed numerically");
+        *inc = r.increment;
+        *ess = r.ess;
+        *mw = r.max_weight;
+    }
+    void pf_assimilate(const uint32_t *x, const uint32_t *y, const double *values, const double *sd,
+                       size_t p, const double *u, const uint8_t *active, hzlb_pf_record *records,
+                       uint32_t *ancestors, double *weighted_mean) override {
+        static_assert(sizeof(PfRecord) == sizeof(hzlb_pf_record), "record layouts agree");
+        pf_ensure();
+        const int P = pf_particles_, S = M_ / P;
+        const double *ob = pf_upload_obs(values, sd, p);
+        if (u)
+            for (int s = 0; s < S; ++s)
+                if (!(u[s] < 1) || std::isnan(u[s]))
+                    raise(HZLB_EINVAL, "resampling uniform must lie in [0, 1) (negative: none)");
+        double *du = pfctl_.as<double>();
+        unsigned char *dact = reinterpret_cast<unsigned char *>(du + S);
+        if (u)
+            cuda_check(cudaMemcpyAsync(du, u, sizeof(double) * S, cudaMemcpyHostToDevice, stream_),
+                       "upload resampling uniforms");
+        if (active)
+            cuda_check(cudaMemcpyAsync(dact, active, S, cudaMemcpyHostToDevice, stream_),
+                       "upload segment flags");
+        double *w = pfw_.as<double>(), *logs = w + M_, *scratch = logs + M_;
+        PfRecord *rec = pfrec_.as<PfRecord>();
+        unsigned *anc = anc_.as<unsigned>();
+        if (p > 0) {
+            observe_device(x, y, p);
+        } else {
+            obs_.ensure(sizeof(double) * M_, "allocate observations");
+        }
+        // records of inactive segments stay zero (nothing resampled there)
+        cuda_check(cudaMemsetAsync(rec, 0, sizeof(PfRecord) * S, stream_), "clear particle records");
+        pf_loglik_kernel<<<(M_ + 127) / 128, 128, 0, stream_>>>(
+            obs_.as<double>(), static_cast<int>(p), ob, ob + p, half_log_two_pi(), w, logs, M_, P,
+            active ? dact : nullptr);
+        pf_normalise_kernel<kPfThreads><<<S, kPfThreads, 0, stream_>>>(
+            logs, w, scratch, P, u ? du : nullptr, active ? dact : nullptr, rec, anc);
+        cuda_check(cudaGetLastError(), "launch particle weights");
+        if (weighted_mean) {
+            aux_.ensure(sizeof(double) * 2 * compact_ * S + sizeof(double) * M_, "allocate weighted mean");
+            const dim3 g(static_cast<unsigned>(std::min<size_t>((compact_ + 255) / 256, 2048)), S);
+            segment_weighted_sum<R><<<g, 256, 0, stream_>>>(omega_.as<cx<R>>(), w,
+                                                            static_cast<long long>(compact_), P,
+                                                            aux_.as<double>());
+            cuda_check(cudaGetLastError(), "launch weighted mean");
+            cuda_check(cudaMemcpyAsync(weighted_mean, aux_.ptr, sizeof(double) * 2 * compact_ * S,
+                                       cudaMemcpyDeviceToHost, stream_),
+                       "download weighted mean");
+        }
+        if (u) {
+            pf_reset_resampled<<<(M_ + 255) / 256, 256, 0, stream_>>>(w, rec, M_, P);
+            const dim3 gg(std::max<int>(1, static_cast<int>(std::min<size_t>((compact_ + 255) / 256, 64))), M_);
+            pf_gather_resampled<R><<<gg, 256, 0, stream_>>>(omega_.as<cx<R>>(), ystage_.as<cx<R>>(),
+                                                            anc, rec, P, static_cast<long long>(compact_));
+            pf_commit_resampled<R><<<gg, 256, 0, stream_>>>(ystage_.as<cx<R>>(), omega_.as<cx<R>>(),
+                                                            rec, P, static_cast<long long>(compact_));
+            if (fcount_ > 1) {
+                const long long fb = static_cast<long long>(fcols_) * LD_;
+                const dim3 fg(std::max<int>(1, static_cast<int>(std::min<long long>((fb + 255) / 256, 64))), M_);
+                pf_gather_resampled<R><<<fg, 256, 0, stream_>>>(forcing_.as<cx<R>>(), ystage_.as<cx<R>>(),
+                                                                anc, rec, P, fb);
+                pf_commit_resampled<R><<<fg, 256, 0, stream_>>>(ystage_.as<cx<R>>(), forcing_.as<cx<R>>(),
+                                                                rec, P, fb);
+            }
+            cuda_check(cudaGetLastError(), "launch resampled gather");
+        }
+        std::vector<PfRecord> host(S);
+        cuda_check(cudaMemcpyAsync(host.data(), rec, sizeof(PfRecord) * S, cudaMemcpyDeviceToHost,
+                                   stream_),
+                   "download particle records");
+        if (ancestors)
+            cuda_check(cudaMemcpyAsync(ancestors, anc, sizeof(unsigned) * M_, cudaMemcpyDeviceToHost,
+                                       stream_),
+                       "download ancestors");
+        cuda_check(cudaStreamSynchronize(stream_), "particle filter update");
+        for (int s = 0; s < S; ++s)
+            if (!active || active[s])
+                std::memcpy(&records[s], &host[s], sizeof(PfRecord));
+        for (int s = 0; s < S; ++s)
+            if (host[s].resampled && (!active || active[s])) {
+                w_valid_ = false;
+                break;
+            }
+    }
+
     // ---- filters --------------------------------------------------------------------
     void resample(const double *w, size_t count, double u, uint32_t *anc) override {
         scratch_d_.ensure(sizeof(double) * 2 * count, "allocate resampling weights");
@@ -1001,7 +1174,8 @@ template <typename R> class EngineT final : public Engine {
     size_t compact_ = 0;
     cudaStream_t stream_ = nullptr;
     DeviceBuffer omega_, ystage_, acc_, w_, nl_, forcing_, ctl_, tw_, phys_, scratch_d_, vbits_,
-        obs_xy_, obs_, anc_, enkf_, aux_, split_;
+        obs_xy_, obs_, anc_, enkf_, aux_, split_, pfw_, pfrec_, pfctl_, pfobs_, pfone_;
+    int pf_particles_ = 0;
     PinnedBuffer staging_, fstage_[2];
     cudaEvent_t fevent_[2] = {nullptr, nullptr};
     int fbuf_next_ = 0;
@@ -1020,43 +1194,6 @@ std::unique_ptr<Engine> make_engine(const hzlb_config &c) {
     if (c.precision == 8)
         return std::make_unique<EngineT<double>>(c);
     raise(HZLB_EINVAL, "precision must be 4 (FP32) or 8 (FP64)");
-}
-
-void pf_weights_host(const double *logs, size_t count, double *w, double *inc, double *ess,
-                     double *mw) {
-    if (count < 2)
-        raise(HZLB_EINVAL, "particle filter needs at least two particles");
-    double maximum = logs[0];
-    for (size_t i = 1; i < count; ++i)
-        if (maximum < logs[i])
-            maximum = logs[i];
-    if (!std::isfinite(maximum))
-        raise(HZLB_ERUNTIME, "particle likelihood collapsed numerically");
-    double total = 0;
-    for (size_t i = 0; i < count; ++i)
-        total += std::exp(logs[i] - maximum);
-    const double increment = maximum + std::log(total);
-    double squared = 0, max_weight = 0;
-    for (size_t i = 0; i < count; ++i) {
-        w[i] = std::exp(logs[i] - increment);
-        squared += w[i] * w[i];
-        max_weight = std::max(max_weight, w[i]);
-    }
-    *inc = increment;
-    *ess = 1 / squared;
-    *mw = max_weight;
-}
-
-void systematic_resample_host(const double *w, size_t count, double u, uint32_t *anc) {
-    size_t ancestor = 0;
-    double cumulative = w[0];
-    const double start = u / static_cast<double>(count);
-    for (size_t i = 0; i < count; ++i) {
-        const double position = start + static_cast<double>(i) / static_cast<double>(count);
-        while (position > cumulative && ancestor + 1 < count)
-            cumulative += w[++ancestor];
-        anc[i] = static_cast<uint32_t>(ancestor);
-    }
 }
 
 } // namespace hzlb

@@ -99,6 +99,17 @@ class Engine {
     virtual void physical(double *out) = 0;
     virtual void observe(const uint32_t *x, const uint32_t *y, size_t p, double *out) = 0;
     virtual void resample(const double *w, size_t count, double u, uint32_t *anc) = 0;
+    // particle filter on the device (filter.cpp:65-120); see hzlb_pf_* in hzlb.h
+    virtual void pf_reset(int particles) = 0;
+    virtual void pf_get_weights(double *out) = 0;
+    virtual void pf_loglik(const uint32_t *x, const uint32_t *y, const double *values,
+                           const double *sd, size_t p, double *log_weights) = 0;
+    virtual void pf_weights(const double *logs, size_t count, double *w, double *inc, double *ess,
+                            double *mw) = 0;
+    virtual void pf_assimilate(const uint32_t *x, const uint32_t *y, const double *values,
+                               const double *sd, size_t p, const double *u, const uint8_t *active,
+                               hzlb_pf_record *records, uint32_t *ancestors,
+                               double *weighted_mean) = 0;
     virtual void gather(const uint32_t *ancestors) = 0;
     virtual void inflate(double inflation) = 0;
     virtual EnkfResult enkf(const EnkfRequest &request) = 0;
@@ -164,10 +175,5 @@ int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp 
 
 // Message returned by hzlb_last_error() on this thread.
 void set_last_error(const std::string &message);
-
-// Host-side reference-order particle weights and systematic resampling (filter.cpp:76-112).
-void pf_weights_host(const double *logs, size_t count, double *w, double *inc, double *ess,
-                     double *mw);
-void systematic_resample_host(const double *w, size_t count, double u, uint32_t *anc);
 
 } // namespace hzlb

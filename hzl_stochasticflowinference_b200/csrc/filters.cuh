@@ -5,6 +5,8 @@
 #pragma once
 #include "common.cuh"
 
+#include <math_constants.h>
+
 namespace hzlb {
 
 // Systematic resampling (filter.cpp:102-112).  One thread forms the cumulative weights with
@@ -35,6 +37,216 @@ __global__ void systematic_resample_kernel(const double *w, double *cum, int cou
         }
         ancestors[i] = static_cast<unsigned>(lo);
     }
+}
+
+// ---- particle-filter weights (filter.cpp:65-112) ------------------------------------
+// Outcome of one observation time for one segment (an independent filter over `particles`
+// consecutive members); the layout of hzlb_pf_record.
+struct PfRecord {
+    double increment, ess, max_weight;
+    int resampled, collapsed;
+};
+
+// log w_m of every member (one thread per member): the prior term -- the log of the member's
+// normalised weight (minus infinity for a zero weight) when `prior` is set, else the value
+// already in logs[m] -- then, observation by observation in the reference's order,
+//   value -= 0.5 r^2 + log sd_o + half_log_two_pi,   r = (H x_m - y_o) / sd_o
+// (filter.cpp:65-75).  Every product and sum is rounded on its own (no fused multiply-add),
+// as the reference's CPU build evaluates them.  hx is members x p (observe_device); members of
+// inactive segments are left as they are.
+__global__ void pf_loglik_kernel(const double *hx, int p, const double *values, const double *sd,
+                                 double half_log_two_pi, const double *prior, double *logs,
+                                 int members, int particles, const unsigned char *active) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < members; m += gridDim.x * blockDim.x) {
+        if (active && !active[m / particles])
+            continue;
+        double value;
+        if (prior)
+            value = prior[m] > 0 ? log(prior[m]) : -CUDART_INF;
+        else
+            value = logs[m];
+        const double *h = hx + static_cast<size_t>(m) * p;
+        for (int o = 0; o < p; ++o) {
+            const double r = __ddiv_rn(__dsub_rn(h[o], values[o]), sd[o]);
+            const double term = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(0.5, r), r), log(sd[o])),
+                                          half_log_two_pi);
+            value = __dsub_rn(value, term);
+        }
+        logs[m] = value;
+    }
+}
+
+template <int TPB> __device__ __forceinline__ double block_max(double v, double *red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();   // `red` may still be read from an earlier call
+    if ((threadIdx.x & 31) == 0)
+        red[threadIdx.x / 32] = v;
+    __syncthreads();
+    double r = red[0];
+#pragma unroll
+    for (int w = 1; w < TPB / 32; ++w)
+        r = fmax(r, red[w]);
+    return r;
+}
+
+// One block per segment s of `particles` members (filter.cpp:76-112), skipped when active[s]
+// is 0 (identity ancestors, record untouched):
+//  * maximum: the first log-weight, then every larger one (std::max_element: a NaN in first
+//    place is the maximum, NaNs elsewhere are passed over); not finite -> collapsed, nothing
+//    else changes;
+//  * increment = max + log(sum_j exp(l_j - max)), the sum formed left to right by one thread;
+//  * w_j = exp(l_j - increment) (written to `weights`), ESS = 1 / sum_j w_j^2 (left to right,
+//    each square rounded before the sum), largest weight;
+//  * with u[s] in [0, 1) and ESS < particles / 2: systematic resampling -- the cumulative
+//    weights left to right by one thread, each position u/P + i/P located by binary search
+//    (the first ancestor whose cumulative weight is not below it, as the reference's walk
+//    stops), ancestors as member indices.  The weights keep their normalised values (the
+//    reset to 1/P follows in pf_reset_resampled, after any weighted mean of this time).
+// `scratch` holds `members` doubles.
+template <int TPB>
+__global__ void __launch_bounds__(TPB)
+    pf_normalise_kernel(const double *logs, double *weights, double *scratch, int particles,
+                        const double *u, const unsigned char *active, PfRecord *rec,
+                        unsigned *anc) {
+    __shared__ double red[TPB / 32];
+    __shared__ double total_sh;
+    const int s = blockIdx.x, tid = threadIdx.x;
+    const size_t base = static_cast<size_t>(s) * particles;
+    const double *l = logs + base;
+    double *w = weights + base, *x = scratch + base;
+    unsigned *as = anc + base;
+    const auto identity = [&] {
+        for (int i = tid; i < particles; i += TPB)
+            as[i] = static_cast<unsigned>(base + i);
+    };
+    if (active && !active[s]) {
+        identity();
+        return;
+    }
+    double mx = l[0];
+    if (!isnan(mx))
+        for (int i = tid; i < particles; i += TPB)
+            mx = fmax(mx, l[i]);
+    mx = isnan(l[0]) ? l[0] : block_max<TPB>(mx, red);
+    if (!isfinite(mx)) {
+        identity();
+        if (tid == 0)
+            rec[s] = PfRecord{-CUDART_INF, 0.0, 0.0, 0, 1};
+        return;
+    }
+    for (int i = tid; i < particles; i += TPB)
+        x[i] = exp(__dsub_rn(l[i], mx));
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0;
+        for (int i = 0; i < particles; ++i)
+            t = __dadd_rn(t, x[i]);
+        total_sh = t;
+    }
+    __syncthreads();
+    const double increment = __dadd_rn(mx, log(total_sh));
+    double mw = 0;
+    for (int i = tid; i < particles; i += TPB) {
+        const double wi = exp(__dsub_rn(l[i], increment));
+        w[i] = wi;
+        x[i] = wi;
+        mw = fmax(mw, wi);
+    }
+    mw = block_max<TPB>(mw, red);
+    if (tid == 0) {
+        double q = 0;
+        for (int i = 0; i < particles; ++i)
+            q = __dadd_rn(q, __dmul_rn(x[i], x[i]));
+        total_sh = q;
+    }
+    __syncthreads();
+    const double ess = 1.0 / total_sh;
+    const bool resample = u && u[s] >= 0.0 && ess < static_cast<double>(particles) / 2;
+    if (resample) {
+        if (tid == 0) {
+            double c = w[0];
+            x[0] = c;
+            for (int a = 1; a < particles; ++a) {
+                c = __dadd_rn(c, w[a]);
+                x[a] = c;
+            }
+        }
+        __syncthreads();
+        const double start = u[s] / static_cast<double>(particles);
+        for (int i = tid; i < particles; i += TPB) {
+            const double position = __dadd_rn(start, static_cast<double>(i) / static_cast<double>(particles));
+            int lo = 0, hi = particles - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (position > x[mid])
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            as[i] = static_cast<unsigned>(base + lo);
+        }
+    } else {
+        identity();
+    }
+    if (tid == 0)
+        rec[s] = PfRecord{increment, ess, mw, resample ? 1 : 0, 0};
+}
+
+// out[s][e] = sum over the members j of segment s, in member order, of w_j x_j[e] (the
+// bootstrap filter's weighted mean, filter.cpp:113-120), as interleaved doubles; grid.y =
+// segments.  Inactive and collapsed segments are written too (their weights as they stand).
+template <typename R>
+__global__ void segment_weighted_sum(const cx<R> *x, const double *w, long long block, int particles,
+                                     double *out) {
+    const int s = blockIdx.y;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x) {
+        double sr = 0, si = 0;
+        for (int j = 0; j < particles; ++j) {
+            const size_t m = static_cast<size_t>(s) * particles + j;
+            const cx<R> v = x[m * block + e];
+            sr = __dadd_rn(sr, __dmul_rn(w[m], static_cast<double>(v.x)));
+            si = __dadd_rn(si, __dmul_rn(w[m], static_cast<double>(v.y)));
+        }
+        out[2 * (static_cast<size_t>(s) * block + e)] = sr;
+        out[2 * (static_cast<size_t>(s) * block + e) + 1] = si;
+    }
+}
+
+// Weights of the segments that were resampled back to 1/particles (filter.cpp:117).
+__global__ void pf_reset_resampled(double *weights, const PfRecord *rec, int members, int particles) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < members; m += gridDim.x * blockDim.x)
+        if (rec[m / particles].resampled)
+            weights[m] = 1.0 / static_cast<double>(particles);
+}
+
+// dst[i] = src[anc[i]] for the members of resampled segments only (grid.y = members), then
+// pf_commit_resampled copies them back: the members of other segments move nowhere.
+template <typename R>
+__global__ void pf_gather_resampled(const cx<R> *src, cx<R> *dst, const unsigned *anc,
+                                    const PfRecord *rec, int particles, long long block) {
+    const int i = blockIdx.y;
+    if (!rec[i / particles].resampled)
+        return;
+    const cx<R> *s = src + static_cast<size_t>(anc[i]) * block;
+    cx<R> *d = dst + static_cast<size_t>(i) * block;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x)
+        d[e] = s[e];
+}
+template <typename R>
+__global__ void pf_commit_resampled(const cx<R> *src, cx<R> *dst, const PfRecord *rec, int particles,
+                                    long long block) {
+    const int i = blockIdx.y;
+    if (!rec[i / particles].resampled)
+        return;
+    const cx<R> *s = src + static_cast<size_t>(i) * block;
+    cx<R> *d = dst + static_cast<size_t>(i) * block;
+    for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < block;
+         e += static_cast<long long>(gridDim.x) * blockDim.x)
+        d[e] = s[e];
 }
 
 // dst[i] = src[ancestor[i]] for member blocks of `block` complex entries.

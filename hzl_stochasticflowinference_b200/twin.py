@@ -23,7 +23,7 @@ from dataclasses import asdict, dataclass
 
 import numpy as np
 
-from . import (Config, Ensemble, full_to_compact, grf_spectrum, kolmogorov_forcing, pf_weights,
+from . import (Config, Ensemble, full_to_compact, grf_spectrum, kolmogorov_forcing,
                retained_k)
 
 TRUTH_ID = 1_000_000
@@ -133,24 +133,23 @@ def run_pf(tc: FilterTwinConfig, truth, log=None) -> dict:
     e = _ensemble(tc, M, PF_BASE)
     xs, ys = observation_grid(tc)
     sd = np.full(len(xs), tc.obs_sd)
+    if tc.resample_fraction != 0.5:
+        raise ValueError("the device filter resamples when ESS < particles / 2 (filter.cpp:102)")
     rng = np.random.default_rng(tc.seed + 9)
-    logw = np.full(M, -np.log(M))
+    e.pf_reset(M)
+    pending = None   # the next resampling uniform, drawn ahead and kept until used
     prior = field_rmse(e.mean_compact(), states[0], tc.n)
     rmse, ess_hist, loglik, resampled, seconds = [], [], [], [], []
     for c in range(tc.cycles):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e.step(tc.dt, tc.obs_every)
-        logw = e.pf_loglik(xs, ys, obs[c], sd, logw)
-        w, inc, ess, _ = pf_weights(logw)
-        mean = e.weighted_mean_compact(w)
-        did = ess < tc.resample_fraction * M
+        if pending is None:
+            pending = float(rng.random())
+        r = e.pf_assimilate(xs, ys, obs[c], sd, u=[pending], weighted_mean=True)
+        did, ess, inc, mean = bool(r["resampled"][0]), r["ess"][0], r["increment"][0], r["mean"][0]
         if did:
-            anc = e.resample(w, float(rng.random()))
-            e.gather(anc)
-            logw = np.full(M, -np.log(M))
-        else:
-            logw = np.log(np.maximum(w, 1e-300))
+            pending = None
         e.synchronize()
         seconds.append(time.perf_counter() - t0)
         rmse.append(field_rmse(mean, states[c + 1], tc.n))

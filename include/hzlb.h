@@ -159,19 +159,59 @@ HZLB_API int hzlb_physical(hzlb_ensemble *h, double *out);
 /* Physical vorticity at p grid points (x[o], y[o]) of every member: out[m*p + o]. */
 HZLB_API int hzlb_observe(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, size_t p, double *out);
 
-/* ---- particle filter (filter.cpp:66-120) ------------------------------------------- */
+/* ---- particle filter (filter.cpp:65-120) ------------------------------------------- */
+/* Every step below runs on the device in FP64, in the reference's order of operations. */
 /* Adds the Gaussian observation log-likelihood of every member to log_weights[m] (the
- * residual (field - value)/sd with the log sd + log(2 pi)/2 constants, filter.cpp:66-75). */
+ * residual (field - value)/sd with the log sd + log(2 pi)/2 constants, filter.cpp:66-75);
+ * log_weights is a host array of members doubles, read and written. */
 HZLB_API int hzlb_pf_loglik(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y, const double *values,
                    const double *sd, size_t p, double *log_weights);
-/* Log-sum-exp increment, normalised weights, ESS = 1/sum w^2, max weight (filter.cpp:76-92). */
-HZLB_API int hzlb_pf_weights(const double *log_weights, size_t count, double *weights, double *increment,
-                    double *ess, double *max_weight);
-/* Systematic resampling: start = u/M, positions start + i/M walked against the sequential
- * cumulative sum of the weights (filter.cpp:102-112).  Bit-exact with the reference given
- * identical weights and u.  Runs on the device when h is non-NULL, else on the host. */
+/* Log-sum-exp increment, normalised weights, ESS = 1/sum w^2, max weight of `count` host
+ * log-weights (filter.cpp:76-92), computed on h's device.  HZLB_ERUNTIME if the largest
+ * log-weight is not finite. */
+HZLB_API int hzlb_pf_weights(hzlb_ensemble *h, const double *log_weights, size_t count, double *weights,
+                    double *increment, double *ess, double *max_weight);
+/* Systematic resampling on h's device: start = u/M, positions start + i/M walked against the
+ * sequential cumulative sum of the weights (filter.cpp:102-112).  Bit-exact with the
+ * reference given identical weights and u.  h must not be NULL. */
 HZLB_API int hzlb_systematic_resample(hzlb_ensemble *h, const double *weights, size_t count, double u,
                              uint32_t *ancestors);
+
+/* Outcome of one observation time of one particle filter (filter.cpp:76-101). */
+typedef struct {
+    double increment;   /* log-likelihood increment: max + log sum_j exp(l_j - max) */
+    double ess;         /* effective sample size 1 / sum_j w_j^2 */
+    double max_weight;  /* largest normalised weight */
+    int32_t resampled;  /* 1: systematic resampling ran and the members were replaced */
+    int32_t collapsed;  /* 1: the largest log-weight was not finite; nothing was changed */
+} hzlb_pf_record;
+/* The ensemble as members / particles independent bootstrap filters (segments) of
+ * `particles` consecutive members each, their weights on the device reset to 1/particles
+ * (bootstrap_filter's initial weights, filter.cpp:52).  members must be a multiple of
+ * particles, particles >= 2.  Until the first call the whole ensemble is one segment. */
+HZLB_API int hzlb_pf_reset(hzlb_ensemble *h, int particles);
+/* One observation time of every segment's bootstrap filter, weights resident on the device
+ * (filter.cpp:65-120): the observation operator, log w_j = log(w_j) - sum_o [0.5 r^2 + log sd_o
+ * + log(2 pi)/2], the increment, normalised weights, ESS and max weight; then, for a segment
+ * whose ESS is below particles/2 and whose u[s] lies in [0, 1), systematic resampling with
+ * start u[s]/particles, the members replaced by their ancestors (and their forcing when it is
+ * per member) and the weights reset to 1/particles -- all without a host round trip.
+ *   u:       segments uniforms, or NULL; u[s] < 0 forbids resampling of segment s (the
+ *            reference's last observation time).  The reference draws the uniform only when
+ *            it resamples, so a caller that draws its u[s] ahead and reuses it until a call
+ *            reports the segment resampled consumes the reference's sequence of uniforms.
+ *   active:  segments flags, or NULL for all; a segment with flag 0 is left untouched.
+ *   records: segments hzlb_pf_record (out).
+ *   ancestors:     members entries (out, may be NULL): member i's ancestor (i if unchanged).
+ *   weighted_mean: segments x hzlb_compact_size complex entries as interleaved doubles (out,
+ *            may be NULL): sum over the segment's members of w_j x_j with the normalised
+ *            weights of this time, before any resampling (filter.cpp:113-120). */
+HZLB_API int hzlb_pf_assimilate(hzlb_ensemble *h, const uint32_t *x, const uint32_t *y,
+                                const double *values, const double *sd, size_t p, const double *u,
+                                const uint8_t *active, hzlb_pf_record *records,
+                                uint32_t *ancestors, double *weighted_mean);
+/* The device weights of hzlb_pf_reset / hzlb_pf_assimilate (members doubles). */
+HZLB_API int hzlb_pf_get_weights(hzlb_ensemble *h, double *weights);
 /* Replace member i's state with member ancestors[i]'s (and its forcing if per member). */
 HZLB_API int hzlb_gather_members(hzlb_ensemble *h, const uint32_t *ancestors);
 

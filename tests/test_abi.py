@@ -1,6 +1,6 @@
 """CPU checks of the C ABI: the library loads, exports every symbol include/hzlb.h declares,
-its host-only entry points agree with the oracle, and device entry points fail loudly (no
-CPU fallback) when no GPU is present."""
+its host-only entry points (random fields, forcing, layouts) agree with the oracle, and device
+entry points fail loudly (no CPU fallback) when no GPU is present."""
 from __future__ import annotations
 
 import re
@@ -43,28 +43,14 @@ def test_kolmogorov_matches_oracle(hzlb, oracle):
     np.testing.assert_array_equal(hzlb.kolmogorov_forcing(64), oracle.kolmogorov(64))
 
 
-def test_pf_weights_match_oracle(hzlb, oracle):
-    rng = np.random.default_rng(3)
-    logs = rng.normal(-50, 10, 257)
-    w, inc, ess, mw = hzlb.pf_weights(logs)
-    w2, inc2, ess2, mw2 = oracle.pf_weights(logs)
-    np.testing.assert_array_equal(w, w2)
-    assert (inc, ess, mw) == (inc2, ess2, mw2)
-
-
-def test_host_resampling_bit_exact(hzlb, oracle):
-    rng = np.random.default_rng(4)
-    for count in (2, 7, 2048):
-        w = rng.random(count) ** 4
-        w /= w.sum()
-        for u in (0.0, 0.37, 0.999999):
-            np.testing.assert_array_equal(hzlb.systematic_resample(w, u),
-                                          oracle.systematic_resample(w, u))
-
-
-def test_invalid_resampling_uniform(hzlb):
-    with pytest.raises(hzlb.HzlbInvalidArgument):
-        hzlb.systematic_resample(np.array([0.5, 0.5]), 1.5)
+def test_resampling_needs_an_ensemble(hzlb):
+    """Systematic resampling has no host path: a NULL handle is rejected."""
+    w = np.array([0.5, 0.5])
+    out = np.zeros(2, np.uint32)
+    lib = hzlb.library()
+    rc = lib.hzlb_systematic_resample(None, w.ctypes.data_as(hzlb._dp), 2, 0.5,
+                                      out.ctypes.data_as(hzlb._u32p))
+    assert rc == hzlb.HZLB_EINVAL
 
 
 def test_compact_layout_round_trip(hzlb, oracle):

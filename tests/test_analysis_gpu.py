@@ -42,6 +42,93 @@ def test_device_resampling_bit_exact(hzlb, oracle):
             np.testing.assert_array_equal(e.resample(w, u), oracle.systematic_resample(w, u))
 
 
+def test_pf_weights_on_device_match_oracle(hzlb, oracle):
+    e, _ = _ensemble(hzlb, 16, 2)
+    rng = np.random.default_rng(3)
+    for count in (2, 257, 4096):
+        logs = rng.normal(-50, 10, count)
+        logs[count // 3] = -np.inf
+        w, inc, ess, mw = e.pf_weights(logs)
+        w2, inc2, ess2, mw2 = oracle.pf_weights(logs)
+        np.testing.assert_allclose(w, w2, rtol=1e-13, atol=0)
+        np.testing.assert_allclose([inc, ess, mw], [inc2, ess2, mw2], rtol=1e-13)
+    with pytest.raises(hzlb.HzlbError) as err:
+        e.pf_weights(np.array([-np.inf, -np.inf]))
+    assert err.value.code == hzlb.HZLB_ERUNTIME
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        e.resample(np.array([0.5, 0.5]), 1.5)
+
+
+def _pf_reference(oracle, phys, xs, ys, vals, sd, prior):
+    """Log-weights in the reference's order (filter.cpp:65-75) from host physical fields."""
+    logs = np.where(prior > 0, np.log(np.where(prior > 0, prior, 1)), -np.inf)
+    half = 0.5 * np.log(2 * np.pi)
+    for o in range(len(xs)):
+        r = (phys[:, ys[o], xs[o]] - vals[o]) / sd[o]
+        logs = logs - (0.5 * r * r + np.log(sd[o]) + half)
+    return logs
+
+
+@pytest.mark.parametrize("precision", [8, 4])
+def test_pf_assimilate_matches_oracle(hzlb, oracle, precision):
+    """Device weights, records, resampling and gather of two 24-particle filters against the
+    reference's formulas (weights rtol 1e-12; ancestors bit-exact given the device weights)."""
+    n, P, S = 32, 24, 2
+    M = P * S
+    e, w = _ensemble(hzlb, n, M, precision)
+    phys = e.physical()
+    xs, ys = np.array([1, 7, 30, 12]), np.array([3, 4, 0, 29])
+    vals, sd = np.array([0.1, -0.2, 0.05, 0.3]), np.array([0.05, 0.08, 0.1, 0.02])
+    e.pf_reset(P)
+    before = e.get_state_compact()
+    r = e.pf_assimilate(xs, ys, vals, sd, weighted_mean=True)   # no resampling
+    logs = _pf_reference(oracle, phys, xs, ys, vals, sd, np.full(M, 1 / P))
+    got_w = e.pf_get_weights()
+    for s in range(S):
+        w2, inc2, ess2, mw2 = oracle.pf_weights(logs[s * P:(s + 1) * P])
+        np.testing.assert_allclose(got_w[s * P:(s + 1) * P], w2, rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose([r["increment"][s], r["ess"][s], r["max_weight"][s]],
+                                   [inc2, ess2, mw2], rtol=1e-12)
+        mean = (got_w[s * P:(s + 1) * P, None] * before[s * P:(s + 1) * P]).sum(axis=0)
+        np.testing.assert_allclose(r["mean"][s], mean, rtol=1e-12, atol=1e-14 * np.abs(mean).max())
+    assert not r["resampled"].any() and not r["collapsed"].any()
+    np.testing.assert_array_equal(r["ancestors"], np.arange(M))
+    np.testing.assert_array_equal(e.get_state_compact(), before)
+    # the same time again from the same state and weights, now allowed to resample segment 0
+    # only: the kernels are deterministic, so the weights equal those above bit for bit
+    e.set_state(w)
+    e.pf_reset(P)
+    u = np.array([0.37, -1.0])
+    r2 = e.pf_assimilate(xs, ys, vals, sd, u=u)
+    np.testing.assert_array_equal(r2["increment"], r["increment"])
+    resampled = r2["ess"] < P / 2
+    assert resampled[0], "the test observations must collapse the weights of segment 0"
+    np.testing.assert_array_equal(r2["resampled"], [1, 0])
+    anc = r2["ancestors"]
+    np.testing.assert_array_equal(anc[:P], oracle.systematic_resample(got_w[:P], 0.37))
+    np.testing.assert_array_equal(anc[P:], np.arange(P, M))
+    np.testing.assert_array_equal(e.get_state_compact(), before[anc])
+    np.testing.assert_array_equal(e.pf_get_weights()[:P], np.full(P, 1 / P))
+    np.testing.assert_array_equal(e.pf_get_weights()[P:], got_w[P:])
+    # an inactive segment is left alone; the other carries its weights into the next time
+    r3 = e.pf_assimilate(xs, ys, vals, sd, u=np.array([-1.0, -1.0]), active=[0, 1])
+    np.testing.assert_array_equal(e.pf_get_weights()[:P], np.full(P, 1 / P))
+    logs3 = _pf_reference(oracle, phys, xs, ys, vals, sd, got_w)[P:]
+    _, inc3, ess3, _ = oracle.pf_weights(logs3)
+    np.testing.assert_allclose([r3["increment"][1], r3["ess"][1]], [inc3, ess3], rtol=1e-12)
+
+
+def test_pf_assimilate_collapse(hzlb):
+    e, _ = _ensemble(hzlb, 16, 4)
+    e.pf_reset(2)
+    before = e.get_state_compact()
+    # an observation no member can explain makes every log-weight -inf in FP64
+    r = e.pf_assimilate([0], [0], [1e300], [1e-300], u=[0.5, 0.5])
+    assert r["collapsed"].all() and not r["resampled"].any()
+    assert np.isneginf(r["increment"]).all()
+    np.testing.assert_array_equal(e.get_state_compact(), before)
+
+
 def test_gather_members(hzlb):
     n, members = 16, 5
     e, w = _ensemble(hzlb, n, members)

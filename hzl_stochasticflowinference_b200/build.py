@@ -48,7 +48,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as pool:
         objs = list(pool.map(compile_one, sources()))
     tmp = LIB.with_suffix(".so.tmp")
-    subprocess.run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart", "-lcublas"],
+    subprocess.run([nvcc, *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"],
                    check=True)
     os.replace(tmp, LIB)
     return LIB

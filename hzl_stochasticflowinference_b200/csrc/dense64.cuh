@@ -1,21 +1,21 @@
 // FP64 dense linear algebra for the EnKF innovation system (p x p, p up to a few thousand):
-// GEMMs with arbitrary operand strides (cuBLAS DGEMM for the plain products, a tiled SIMT
-// kernel for the in-place panel update and strides cuBLAS cannot express), a blocked
-// right-looking Cholesky whose diagonal blocks are factored and inverted in shared memory, and
-// blocked forward substitution for many right-hand sides built from the same GEMM.  FP64 stays
-// here on purpose: the innovation Cholesky and solve are the one place the analysis needs it.
+// a GEMM with arbitrary operand strides on the FP64 tensor cores (mma.sync m8n8k4 f64 tiles;
+// tcgen05 has no FP64 kind), a blocked right-looking Cholesky whose diagonal blocks are
+// factored and inverted in shared memory, and blocked forward substitution for many
+// right-hand sides built from the same GEMM.  FP64 stays here on purpose: the innovation
+// Cholesky and solve are the one place the analysis needs it.
 #pragma once
 #include "common.cuh"
 
-#include <algorithm>
 #include <cstdint>
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 namespace hzlb {
 namespace d64 {
 
-constexpr int BM = 64, BN = 64, BK = 16;   // GEMM tile; 256 threads, 4 x 4 outputs each
+constexpr int BM = 64, BN = 64, BK = 16;   // GEMM tile; 4 warps of 32 x 32, 16 MMA tiles each
+constexpr int GEMM_THREADS = 128;
+constexpr int LDS = BM + 4;                 // shared row pitch: conflict-free fragment loads
 constexpr int NB = 64;                      // Cholesky / substitution block
 
 // C[m][n] = alpha sum_k A(m,k) B(k,n) + beta C[m][n],  A(m,k) = A[m*sam + k*sak],
@@ -31,23 +31,38 @@ struct GemmArgs {
     long long ldc;
 };
 
+// D (8 x 8) += A (8 x 4, row) B (4 x 8, col) on the FP64 tensor cores.  Lane l = 4g + t holds
+// A[g][t], B[t][g] and D[g][2t], D[g][2t + 1].
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// One 64 x 64 tile of C per block.  Warp w owns rows 32 (w / 2) .. +32 and columns
+// 32 (w % 2) .. +32 as 4 x 4 tiles of 8 x 8.  K advances in slabs of 16 staged through shared
+// memory as [k][m] and [k][n] (any operand strides: the loads are coalesced along whichever
+// index is contiguous); the next slab is read into registers while the tensor cores work on
+// the current one.  Shared rows are LDS = 68 doubles apart, so the fragment loads of a half
+// warp (k = t, m = g + 0..3 or 4..7) fall in 16 distinct 8-byte bank pairs.
 // LOWER: skip tiles strictly above the diagonal (only C[m][n], n <= m, is wanted).  A block
 // reads all of its A rows before it writes C, so C may alias the A rows of its own tile when
-// N <= BN (one tile column).  The k-tiles are double-buffered: the next tile is loaded into
-// registers while the current one is multiplied from shared memory.
-template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const GemmArgs g) {
+// N <= BN (one tile column).
+template <bool LOWER> __global__ void __launch_bounds__(GEMM_THREADS) gemm_kernel(const GemmArgs g) {
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     if (LOWER && n0 > m0 + BM - 1)
         return;
-    __shared__ double As[2][BK][BM + 1], Bs[2][BK][BN + 1];
-    const int tid = threadIdx.x, tx = tid % 16, ty = tid / 16;
-    double acc[4][4] = {};
+    __shared__ double As[2][BK][LDS], Bs[2][BK][LDS];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32, lg = lane >> 2, lt = lane & 3;
+    constexpr int PER = BM * BK / GEMM_THREADS;   // staged elements per thread and operand
+    double acc[4][4][2] = {};
     const bool a_k = g.sak == 1, b_k = g.sbk == 1;
-    double ra[4], rb[4];
+    double ra[PER], rb[PER];
     auto fetch = [&](int k0) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int q = tid + 256 * r;
+        for (int r = 0; r < PER; ++r) {
+            const int q = tid + GEMM_THREADS * r;
             const int mk_m = a_k ? q / BK : q % BM, mk_k = a_k ? q % BK : q / BM;
             const int gm = m0 + mk_m, gk = k0 + mk_k;
             ra[r] = (gm < g.M && gk < g.K) ? g.A[gm * g.sam + gk * g.sak] : 0.0;
@@ -58,8 +73,8 @@ template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const G
     };
     auto stash = [&](int buf) {
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int q = tid + 256 * r;
+        for (int r = 0; r < PER; ++r) {
+            const int q = tid + GEMM_THREADS * r;
             const int mk_m = a_k ? q / BK : q % BM, mk_k = a_k ? q % BK : q / BM;
             As[buf][mk_k][mk_m] = ra[r];
             const int kn_n = b_k ? q / BK : q % BN, kn_k = b_k ? q % BK : q / BN;
@@ -75,18 +90,18 @@ template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const G
         if (more)
             fetch(k0 + BK);   // global loads in flight during the products below
 #pragma unroll
-        for (int k = 0; k < BK; ++k) {
+        for (int kk = 0; kk < BK; kk += 4) {
             double a[4], b[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                a[i] = As[buf][k][ty + 16 * i];
-                b[i] = Bs[buf][k][tx + 16 * i];
+                a[i] = As[buf][kk + lt][wm + 8 * i + lg];
+                b[i] = Bs[buf][kk + lt][wn + 8 * i + lg];
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                    dmma_8x8x4(acc[i][j], a[i], b[j]);
         }
         if (more) {
             stash(buf ^ 1);
@@ -96,113 +111,31 @@ template <bool LOWER> __global__ void __launch_bounds__(256) gemm_kernel(const G
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int m = m0 + ty + 16 * i;
+        const int m = m0 + wm + 8 * i + lg;
         if (m >= g.M)
             continue;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = n0 + tx + 16 * j;
-            if (n >= g.N)
-                continue;
-            double *c = g.C + m * g.ldc + n;
-            *c = g.beta == 0.0 ? g.alpha * acc[i][j] : fma(g.alpha, acc[i][j], g.beta * *c);
-        }
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int n = n0 + wn + 8 * j + 2 * lt + h;
+                if (n >= g.N)
+                    continue;
+                double *c = g.C + m * g.ldc + n;
+                *c = g.beta == 0.0 ? g.alpha * acc[i][j][h] : fma(g.alpha, acc[i][j][h], g.beta * *c);
+            }
     }
 }
 
-// A strided operand as a row-major block: rows x cols with leading dimension ld (ld 0 if the
-// strides are not of that form).
-struct Block {
-    const double *p;
-    long long rows, cols, ld;
-};
-inline Block a_block(const GemmArgs &g) {
-    if (g.sak == 1)
-        return {g.A, g.M, g.K, g.sam};
-    if (g.sam == 1)
-        return {g.A, g.K, g.M, g.sak};
-    return {g.A, g.M, g.K, 0};
-}
-inline Block b_block(const GemmArgs &g) {
-    if (g.sbn == 1)
-        return {g.B, g.K, g.N, g.sbk};
-    if (g.sbk == 1)
-        return {g.B, g.N, g.K, g.sbn};
-    return {g.B, g.K, g.N, 0};
-}
-// Whether two blocks may share an element: exact for blocks of one leading dimension (both
-// no wider than it), else by address extent.
-inline bool may_overlap(const Block &x, const Block &y) {
-    const auto lo = [](const Block &b) { return reinterpret_cast<std::uintptr_t>(b.p); };
-    const auto hi = [](const Block &b) {
-        return reinterpret_cast<std::uintptr_t>(b.p) +
-               sizeof(double) * static_cast<std::uintptr_t>((b.rows - 1) * b.ld + b.cols);
-    };
-    if (x.ld == 0 || y.ld == 0 || x.ld != y.ld || x.cols > x.ld || y.cols > y.ld)
-        return !(hi(x) <= lo(y) || hi(y) <= lo(x)) || x.ld == 0 || y.ld == 0;
-    const long long L = x.ld;
-    const long long d = (static_cast<long long>(lo(x)) - static_cast<long long>(lo(y))) /
-                        static_cast<long long>(sizeof(double));
-    long long q = d / L, r = d % L;
-    if (r < 0) {
-        r += L;
-        --q;
-    }
-    const auto meet = [](long long a0, long long a1, long long b0, long long b1) {
-        return a0 < b1 && b0 < a1;
-    };
-    // x's columns [r, r + cols) in y's rows q..; the part past the edge wraps to the next row
-    const long long first = std::min(x.cols, L - r);
-    if (meet(q, q + x.rows, 0, y.rows) && meet(r, r + first, 0, y.cols))
-        return true;
-    if (x.cols > first && meet(q + 1, q + 1 + x.rows, 0, y.rows) && meet(0, x.cols - first, 0, y.cols))
-        return true;
-    return false;
-}
-
-// One cuBLAS handle per device and host thread (kept until exit).
-inline cublasHandle_t cublas_handle() {
-    thread_local cublasHandle_t handles[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
-        return nullptr;
-    if (!handles[dev] && cublasCreate(&handles[dev]) != CUBLAS_STATUS_SUCCESS)
-        handles[dev] = nullptr;
-    return handles[dev];
-}
-
-// The row-major product through column-major DGEMM: C^T = alpha B^T A^T + beta C^T.  Returns
-// false (nothing done) when the operands do not fit (non-unit strides, or an operand sharing
-// an element with C, which DGEMM forbids).
-inline bool gemm_cublas(const GemmArgs &g, cudaStream_t s) {
-    const Block a = a_block(g), b = b_block(g), c{g.C, g.M, g.N, g.ldc};
-    if (a.ld == 0 || b.ld == 0 || g.K <= 0 || g.ldc < g.N || may_overlap(a, c) || may_overlap(b, c))
-        return false;
-    cublasHandle_t h = cublas_handle();
-    if (!h || cublasSetStream(h, s) != CUBLAS_STATUS_SUCCESS)
-        return false;
-    // op(X) = B^T (N x K), op(Y) = A^T (K x M)
-    const cublasOperation_t ox = g.sbn == 1 ? CUBLAS_OP_N : CUBLAS_OP_T;
-    const cublasOperation_t oy = g.sak == 1 ? CUBLAS_OP_N : CUBLAS_OP_T;
-    const long long ldx = g.sbn == 1 ? g.sbk : g.sbn, ldy = g.sak == 1 ? g.sam : g.sak;
-    if (ldx > INT32_MAX || ldy > INT32_MAX || g.ldc > INT32_MAX)
-        return false;
-    return cublasDgemm(h, ox, oy, g.N, g.M, g.K, &g.alpha, g.B, static_cast<int>(ldx), g.A,
-                       static_cast<int>(ldy), &g.beta, g.C, static_cast<int>(g.ldc)) ==
-           CUBLAS_STATUS_SUCCESS;
-}
-
-// lower: only C[m][n], n <= m, is wanted (the cuBLAS path writes the whole of C).
+// lower: only C[m][n], n <= m, is wanted.
 inline cudaError_t gemm(const GemmArgs &g, cudaStream_t s, bool lower = false) {
     if (g.M <= 0 || g.N <= 0)
         return cudaSuccess;
-    if (gemm_cublas(g, s))
-        return cudaSuccess;
     const dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
     if (lower)
-        gemm_kernel<true><<<grid, 256, 0, s>>>(g);
+        gemm_kernel<true><<<grid, GEMM_THREADS, 0, s>>>(g);
     else
-        gemm_kernel<false><<<grid, 256, 0, s>>>(g);
+        gemm_kernel<false><<<grid, GEMM_THREADS, 0, s>>>(g);
     return cudaGetLastError();
 }
 

@@ -1123,27 +1123,27 @@ template <typename R> class EngineT final : public Engine {
                                    stream_>>>(x, mf, n, M_, ahi, alo);
             split_tf32_t<<<dim3((M_ + 31) / 32, (M_ + 31) / 32), tb, 0, stream_>>>(W, M_, whi, wlo);
             cuda_check(cudaGetLastError(), "launch 3xTF32 split");
-            const float *wa[3] = {whi, whi, wlo};
-            const float *aa[3] = {ahi, alo, ahi};
-            for (int i = 0; i < 3; ++i) {
-                tc::GemmArgs g{};
-                g.M = M_;
-                g.N = static_cast<int>(n);
-                g.K = M_;
-                g.A = wa[i];           // opA[m][a] = W[a][m], stored transposed
-                g.lda = M_;
-                g.a_kcontig = 1;
-                g.B = aa[i];           // opB[e][a] = A[a][e], stored transposed
-                g.ldb = M_;
-                g.b_kcontig = 1;
-                g.C = x;
-                g.ldc = n;
-                g.alpha = 1.0f;
-                g.beta = 1.0f;
-                g.epilogue = tc::EPI_NONE;
-                g.status = &ctl_.as<StepControl>()->status;
-                cuda_check(gemm(g, 4, stream_), "launch tensor-core EnKF update");
-            }
+            // one product with K = 3M: (whi, whi, wlo) against (ahi, alo, ahi)
+            tc::GemmArgs g{};
+            g.M = M_;
+            g.N = static_cast<int>(n);
+            g.K = 3 * M_;
+            g.split3 = M_;
+            g.A = whi;             // opA[m][a] = W[a][m], stored transposed
+            g.A2 = wlo;
+            g.lda = M_;
+            g.a_kcontig = 1;
+            g.B = ahi;             // opB[e][a] = A[a][e], stored transposed
+            g.B2 = alo;
+            g.ldb = M_;
+            g.b_kcontig = 1;
+            g.C = x;
+            g.ldc = n;
+            g.alpha = 1.0f;
+            g.beta = 1.0f;
+            g.epilogue = tc::EPI_NONE;
+            g.status = &ctl_.as<StepControl>()->status;
+            cuda_check(gemm(g, 4, stream_), "launch tensor-core EnKF update");
         } else {
             // FP64 path: X_a = X + (X - mean) W with FP64 accumulation
             const dim3 ug(static_cast<unsigned>((compact_ + 63) / 64), (M_ + 15) / 16);

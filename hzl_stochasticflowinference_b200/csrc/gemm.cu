@@ -65,9 +65,15 @@ bool make_map(CUtensorMap *map, const void *ptr, int rows, int K, long long ld, 
 template <typename TIn, int BN, int ST> cudaError_t launch_tma(const tc::GemmArgs &g, cudaStream_t s,
                                                                bool &used) {
     used = false;
-    CUtensorMap ma, mb;
-    if (!make_map<TIn>(&ma, g.A, g.M, g.K, g.lda, tc::BM) ||
-        !make_map<TIn>(&mb, g.B, g.N, g.K, g.ldb, BN))
+    CUtensorMap ma, mb, ma2, mb2;
+    const int kext = g.split3 > 0 ? g.split3 : g.K;
+    if (!make_map<TIn>(&ma, g.A, g.M, kext, g.lda, tc::BM) ||
+        !make_map<TIn>(&mb, g.B, g.N, kext, g.ldb, BN))
+        return cudaSuccess;
+    ma2 = ma;
+    mb2 = mb;
+    if (g.split3 > 0 && (!make_map<TIn>(&ma2, g.A2, g.M, kext, g.lda, tc::BM) ||
+                         !make_map<TIn>(&mb2, g.B2, g.N, kext, g.ldb, BN)))
         return cudaSuccess;
     constexpr size_t smem = tc::tma_smem<BN, ST>();
     static bool configured[64] = {};
@@ -82,11 +88,31 @@ template <typename TIn, int BN, int ST> cudaError_t launch_tma(const tc::GemmArg
         configured[dev] = true;
     }
     const dim3 grid((g.N + BN - 1) / BN, (g.M + tc::BM - 1) / tc::BM, g.splits > 1 ? g.splits : 1);
-    tc::umma_tma_kernel<TIn, BN, ST><<<grid, 128, smem, s>>>(ma, mb, g);
+    tc::umma_tma_kernel<TIn, BN, ST><<<grid, 128, smem, s>>>(ma, mb, ma2, mb2, g);
     used = true;
     return cudaGetLastError();
 }
+template <typename TIn> cudaError_t launch_any(const tc::GemmArgs &g, cudaStream_t s);
+// A split3 product whose operands the TMA path cannot map: the three terms one after another.
+template <typename TIn> cudaError_t launch_split3_terms(const tc::GemmArgs &g, cudaStream_t s) {
+    const void *as[3] = {g.A, g.A, g.A2}, *bs[3] = {g.B, g.B2, g.B};
+    for (int i = 0; i < 3; ++i) {
+        tc::GemmArgs t = g;
+        t.split3 = 0;
+        t.K = g.split3;
+        t.A = as[i];
+        t.B = bs[i];
+        if (i > 0)
+            t.beta = 1.0f;
+        const cudaError_t e = launch_any<TIn>(t, s);
+        if (e != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
 template <typename TIn> cudaError_t launch_any(const tc::GemmArgs &g, cudaStream_t s) {
+    if (g.split3 > 0 && (!g.a_kcontig || !g.b_kcontig || g.splits > 1 || g.epilogue != tc::EPI_NONE))
+        return launch_split3_terms<TIn>(g, s);
     if (g.a_kcontig && g.b_kcontig) {
         bool used = false;
         cudaError_t e;
@@ -98,6 +124,8 @@ template <typename TIn> cudaError_t launch_any(const tc::GemmArgs &g, cudaStream
             e = launch_tma<TIn, 32, 4>(g, s, used);
         if (e != cudaSuccess || used)
             return e;
+        if (g.split3 > 0)
+            return launch_split3_terms<TIn>(g, s);
     }
     if (g.N >= 128)
         return launch<TIn, 128>(g, s);

@@ -118,6 +118,12 @@ struct GemmArgs {
     int splits;
     int kchunk;
     float *partial;
+    // 3xTF32 in one product (TMA path): with split3 > 0, K = 3 split3 and the K range is three
+    // segments of split3 elements whose A operands are (A, A, A2) and B operands (B, B2, B),
+    // so one accumulator sums A B + A B2 + A2 B -- hi hi + hi lo + lo hi of split operands --
+    // and C is read and written once.  A2 and B2 have the layouts of A and B.
+    const void *A2, *B2;
+    int split3;
 };
 
 constexpr int BM = 128;

@@ -47,9 +47,12 @@ template <int BN, int ST> constexpr size_t tma_smem() {
     return static_cast<size_t>(ST) * (BM + BN) * SLAB + 1024;
 }
 
+// ta2 / tb2 map g.A2 / g.B2 when g.split3 > 0 (otherwise they repeat ta / tb, unused).
 template <typename TIn, int BN, int ST>
 __global__ void __launch_bounds__(128) umma_tma_kernel(const __grid_constant__ CUtensorMap ta,
                                                        const __grid_constant__ CUtensorMap tb,
+                                                       const __grid_constant__ CUtensorMap ta2,
+                                                       const __grid_constant__ CUtensorMap tb2,
                                                        const GemmArgs g) {
     static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M = 128");
     constexpr bool TF32 = sizeof(TIn) == 4;
@@ -72,7 +75,9 @@ __global__ void __launch_bounds__(128) umma_tma_kernel(const __grid_constant__ C
         kb = blockIdx.z * g.kchunk;
         K = g.K - kb < g.kchunk ? g.K - kb : g.kchunk;
     }
-    const int slabs = (K + EPS - 1) / EPS;
+    // split3: slabs per K segment (each segment's tail is zero-filled by its map's extent)
+    const int sps = g.split3 > 0 ? (g.split3 + EPS - 1) / EPS : 0;
+    const int slabs = g.split3 > 0 ? 3 * sps : (K + EPS - 1) / EPS;
     if (warp == 0)
         tmem_alloc(&tmem_base, NCOLS);
     if (threadIdx.x == 32) {
@@ -99,9 +104,19 @@ __global__ void __launch_bounds__(128) umma_tma_kernel(const __grid_constant__ C
                 atomicExch(&err, 1);
                 break;
             }
+            const CUtensorMap *mapa = &ta, *mapb = &tb;
+            int kk = kb + s * EPS;
+            if (sps > 0) {
+                const int seg = s / sps;
+                kk = (s - seg * sps) * EPS;
+                if (seg == 2)
+                    mapa = &ta2;
+                if (seg == 1)
+                    mapb = &tb2;
+            }
             mbar_arrive_expect(&full[b], A_BYTES + B_BYTES);
-            tma_load_2d(sa + b * A_BYTES, &ta, kb + s * EPS, m0, &full[b]);
-            tma_load_2d(sb + b * B_BYTES, &tb, kb + s * EPS, n0, &full[b]);
+            tma_load_2d(sa + b * A_BYTES, mapa, kk, m0, &full[b]);
+            tma_load_2d(sb + b * B_BYTES, mapb, kk, n0, &full[b]);
             issued = s + 1;
         }
         issued_sh = issued;

@@ -12,13 +12,16 @@ Legs:
                state read from pinned host memory and written back every step, the
                copies of each member chunk overlapping the stepping of the others
   roofline     dominant kernel: algorithmic bytes per launch / mean launch duration
-  cpu_baseline the reference's own CPU solver (oracle/_ref, hzl::ensemble on all host
-               threads) on a bounded sample of the same grid size
+  cpu_baseline the reference's own CPU solver (oracle/_ref, its Solver API driven with this
+               workload's forcing, noise and fields on all host threads, FP64) on a bounded
+               sample of the same workload
+  fp64         the same workload, members and steps in FP64 (the reference's precision), with
+               its own roofline and e2e: the like-for-like comparison with the reference arm
   gpu_reference the reference's own GPU path (src/cuda_solver.cu: cuFFT Z2Z, FP64, one solver
                instance per member launched in sequence, host OU forcing), built for sm_100a by
                oracle/Makefile, through its hzl-cuda-ensemble-benchmark driver at 256^2
-  fp64         this path's FP64 variant at 256^2 (512 members), device-timed, for a like-for-like
-               precision comparison with gpu_reference
+  config1      (1 GPU) 256 members at 128^2, nu = dt = 5e-4, 2000 steps in FP32 and FP64 from
+               identical inputs: per-member relative L2 and enstrophy drift of FP32 against FP64
 
   filters      (1 GPU) the 128^2 filtering twin experiment: EnKF 512 members (inflation 1.05) and
                bootstrap PF 2048 particles, 16x16 observations (sigma 0.1) every 50 steps, 40
@@ -33,7 +36,8 @@ Legs:
                0.1) every 20 steps for 40 cycles; analysis RMSE and wall-clock per cycle of
                the spectral, learned, hybrid and no-network forecasts (--no-learned skips it)
 
-`--impl reference` times only the reference CPU path (rank 0; other ranks exit 0).
+`--impl reference` times only the reference CPU solver on this workload (rank 0; other ranks
+exit 0).
 `--case gemm|enkf|learned` times one isolated workload (1 GPU) and prints its own JSON line:
 the tcgen05 GEMM at 4096^3 (TF32 and BF16), one EnKF analysis at 1024 members x 1024
 observations at 256^2, one learned forecast window at 1024 members x 256^2.
@@ -147,24 +151,27 @@ def dist_env():
 
 
 def cpu_reference_sample(n: int, seconds_target: float = 15.0):
-    """Times the reference's own CPU path (hzl::ensemble: Solver::step per member on
-    std::jthread workers, src/inference.cpp:555-590) on all host threads; bounded sample."""
-    from oracle.oracle import Reference, host_cores, params6
+    """Times the reference's own CPU solver on this benchmark's workload: the seeded-synthetic
+    physics (Kolmogorov forcing, Euler-Maruyama noise, random initial fields) driven through
+    the reference's Solver API -- update_latent_state, then Solver::step with its validate_step
+    -- one member per std::jthread worker on all host threads (ref_synthetic_ensemble, as
+    hzl::ensemble shares members out, src/inference.cpp:555-590); FP64, its only precision.
+    A bounded sample: every thread's member for as many steps as fill ~seconds_target."""
+    from oracle.oracle import Reference, host_cores
     ref = Reference()
     threads = host_cores()
-    p = params6(NU, 0.1, 0.2, 0.5, 2, 3)   # reference physics (OU forcing); same FFT cost
     # calibrate with one member-step per thread, then size the sample to ~seconds_target
     t0 = time.perf_counter()
-    ref.ensemble(n, p, DT, 1, threads, threads, SEED)
+    ref.synthetic_ensemble(n, NU, DT, 1, threads, threads, SEED, SIGMA, 4, keep=False)
     one = time.perf_counter() - t0
-    steps = max(1, int(seconds_target / max(one, 1e-3)))
+    steps = max(2, int(seconds_target / max(one, 1e-3)))
     t0 = time.perf_counter()
-    ref.ensemble(n, p, DT, steps, threads, threads, SEED)
+    ref.synthetic_ensemble(n, NU, DT, steps, threads, threads, SEED, SIGMA, 4, keep=False)
     el = time.perf_counter() - t0
     value = threads * steps / el
-    sample = (f"hzl::ensemble (reference CPU build, -O2) at {n}^2: {threads} members x {steps} "
-              f"steps on {threads} threads, {el:.1f} s, includes the reference's per-step "
-              f"validate_step diagnostics")
+    sample = (f"reference Solver (its CPU build, -O2, FP64) on this workload through its API "
+              f"(update_latent_state + step, validate_step included) at {n}^2: {threads} members "
+              f"x {steps} steps on {threads} threads, {el:.1f} s including set-up")
     return value, threads, sample
 
 
@@ -216,8 +223,9 @@ def filter_experiment(cpu: bool) -> dict:
 
 def arm_config(members: int, world: int) -> dict:
     """The workload both arms report (the reference arm times a bounded sample of it)."""
-    return {"workload": f"{N}^2 FP32 ensemble RK4 step, {members} members per GPU "
-                        "(Kolmogorov forcing + Philox EM noise, GRF initial fields)",
+    return {"workload": f"{N}^2 ensemble RK4 step, {members} members per GPU: nu {NU}, dt {DT}, "
+                        f"Kolmogorov forcing 0.1 sin(4y), Euler-Maruyama noise sigma {SIGMA} on "
+                        "1<=|k|<=4 (Philox keyed by seed and member), seeded random initial fields",
             "n": N, "members_per_gpu": members, "nu": NU, "dt": DT,
             "l2": "inputs larger than L2 (state + stage buffers ~2.5 GB per GPU)",
             "parallelism": f"member shards x{world}"}
@@ -227,8 +235,6 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     value, threads, sample = cpu_reference_sample(N, seconds_target=max(5.0, 3.0 * args.steps))
-    sample += ("; its member-step cost does not depend on the forcing kind, so it stands for "
-               "this workload's member-steps")
     out = {
         "metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * threads / value,
@@ -267,30 +273,155 @@ def reference_gpu_sample(n: int, steps: int = 20, members: int = 64) -> dict:
             "evolution_seconds": res["gpu_evolution_seconds"]}
 
 
-def fp64_sample(hz, torch, n: int, members: int = 512, steps: int = 10) -> dict:
-    """This path in FP64 at n^2: device-timed member-steps/s."""
-    cfg = hz.Config(n=n, members=members, precision=8, nu=NU, alpha=0.0, forcing_kmax=0,
-                    noise_sigma=SIGMA, noise_kmax=4, seed=SEED)
-    e = hz.Ensemble(cfg)
-    init = np.zeros((members, e.compact_size), np.complex128)
-    for m in range(members):
-        init[m] = hz.full_to_compact(hz.grf_spectrum(n, SEED, m), n)[0]
-    e.set_state_compact(init)
-    e.set_forcing(hz.kolmogorov_forcing(n)[None])
-    stream = torch.cuda.ExternalStream(e.stream)
-    for _ in range(3):
-        e.step(DT, 1)
-    e.synchronize()
+def build_ensemble(hz, precision: int, M: int, member_base: int, device: int):
+    """The benchmark ensemble: M members at N^2 of the given precision (4 or 8), the seeded
+    random fields of members member_base.., Kolmogorov forcing, Philox noise."""
+    cfg = hz.Config(n=N, members=M, precision=precision, nu=NU, alpha=0.0, forcing_kmax=0,
+                    noise_sigma=SIGMA, noise_kmax=4, seed=SEED, member_base=member_base,
+                    device=device)
+    ens = hz.Ensemble(cfg)
+    dtype = np.complex64 if precision == 4 else np.complex128
+    init = np.zeros((M, ens.compact_size), dtype)
+    for m in range(M):
+        init[m] = hz.full_to_compact(hz.grf_spectrum(N, SEED, member_base + m), N)[0]
+    ens.set_state_compact(init)
+    ens.set_forcing(hz.kolmogorov_forcing(N)[None])
+    ens.set_time(0.0, 0)
+    return ens
+
+
+def measure(hz, torch, ens, precision: int, steps: int, warmup: int, world: int, barrier,
+            max_over_ranks, clocks=None) -> dict:
+    """value (device-resident member-steps/s, CUDA events on the library stream around
+    `steps` steps, max over ranks), roofline of the dominant kernel (this design's algorithmic
+    bytes per launch over the launch's mean CUDA-event duration) and e2e (the same step through
+    hzlb_step_host with the whole state copied from pinned host memory and back every step)."""
+    M = ens.members
+    stream = torch.cuda.ExternalStream(ens.stream)
+    for _ in range(warmup):
+        ens.step(DT, 1)
+    ens.synchronize()
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if clocks is not None:
+        clocks.__enter__()
+    start.record(stream)
+    for _ in range(steps):
+        ens.step(DT, 1)
+    stop.record(stream)
+    ens.synchronize()
+    barrier()
+    if clocks is not None:
+        clocks.__exit__(None, None, None)
+    ms = max_over_ranks(start.elapsed_time(stop))
+    status = ens.status()
+    value = world * M * steps / (ms / 1e3)
+
+    # roofline: per-launch events on the library stream
+    row_ms, col_ms = ens.step_profiled(DT, max(2, steps // 4))
+    K = (N - 1) // 3
+    C, LD = K + 1, 2 * K + 1
+    cb = 8 if precision == 4 else 16   # complex bytes
+    # per launch: the row kernel reads the 2 velocity column fields and writes the 2 product
+    # fields; the column kernel reads the 2 product fields, writes the 2 velocity fields and
+    # reads/writes the compact state, stage input and accumulator (3, 5, 5, 4 entries per mode
+    # on stages 1-4: 4.25 on average)
+    row_bytes = M * (2 * C * N + 2 * C * N) * cb
+    col_bytes = int(M * (2 * C * N + 2 * C * N + 4.25 * C * LD) * cb)
+    row_gbs = row_bytes / (row_ms * 1e-3) / 1e9
+    col_gbs = col_bytes / (col_ms * 1e-3) / 1e9
+    peak, peak_kind = peaks()
+    dom = ("column_kernel", col_gbs, col_bytes, col_ms) if col_ms >= row_ms else \
+        ("row_kernel", row_gbs, row_bytes, row_ms)
+    traffic = NCU_TRAFFIC_PER_MEMBER[dom[0]] * M if precision == 4 else None
+    model_bytes = (32 * 8 * N * (N // 2 + 1) + 16 * 8 * N * N) * (1 if precision == 4 else 2)
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": dom[1], "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": dom[1] / peak,
+                "traffic": traffic, "algorithmic_bytes": dom[2], "launch_ms": dom[3],
+                "row_kernel": {"ms": row_ms, "gbs": row_gbs, "frac": row_gbs / peak},
+                "column_kernel": {"ms": col_ms, "gbs": col_gbs, "frac": col_gbs / peak},
+                # the whole-step byte model of a schedule that moves five real fields per stage
+                # (B32 = 32 S + 16 P, S = 8 N (N/2+1), P = 8 N^2 bytes; twice that in FP64);
+                # this design moves fewer bytes, so this fraction exceeds 1
+                "step_model": {"bytes_per_member_step": model_bytes,
+                               "achieved": value * model_bytes / 1e9,
+                               "frac": value * model_bytes / 1e9 / peak}}
+
+    # e2e: host state in and out around every step
+    state_bytes = M * ens.compact_size * cb
+    view = np.float32 if precision == 4 else np.float64
+    host_in = torch.from_numpy(ens.get_state_compact().view(view)).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    e2e_steps = max(3, steps // 2)
+    for _ in range(2):
+        ens.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), DT, 1)
+    barrier()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
-    for _ in range(steps):
-        e.step(DT, 1)
+    for _ in range(e2e_steps):
+        ens.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), DT, 1)
     t1.record(stream)
-    e.synchronize()
-    ms = t0.elapsed_time(t1)
-    e.close()
-    return {"value": members * steps / (ms / 1e3), "unit": "member-steps/s", "members": members,
-            "steps": steps, "dtype": "f64"}
+    ens.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1))
+    e2e = {"value": world * M * e2e_steps / (e2e_ms / 1e3), "unit": "member-steps/s",
+           "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+           "steps": e2e_steps}
+    return {"value": value, "ms_per_step": ms / steps, "status": status, "roofline": roofline,
+            "e2e": e2e, "members": M, "steps": steps, "dtype": "f32" if precision == 4 else "f64",
+            "gpu_launches": 8 * steps}
+
+
+def config1_experiment(hz) -> dict:
+    """Config 1 at its own size: 256 members at 128^2, nu = dt = 5e-4, 2000 steps, from the
+    same random fields and the same Philox noise in FP32 (complex64 spectra) and FP64.  Every
+    250 steps, per member: the relative L2 error of the FP32 vorticity spectrum against the FP64
+    one and the FP32 enstrophy drift |Z32 / Z64 - 1| (Z = A/2 sum |w_k|^2 over the whole
+    spectrum; the compact half-spectrum's kx > 0 columns count twice).  The FP64 path itself
+    equals the reference CPU solver to 1e-12 over these 2000 steps (tests/test_step_gpu.py)."""
+    try:
+        n, M, steps, every, dt, nu = 128, 256, 2000, 250, 5e-4, 5e-4
+        ens = {}
+        for prec in (4, 8):
+            cfg = hz.Config(n=n, members=M, precision=prec, nu=nu, alpha=0.0, forcing_kmax=0,
+                            noise_sigma=SIGMA, noise_kmax=4, seed=SEED)
+            e = hz.Ensemble(cfg)
+            init = np.array([hz.full_to_compact(hz.grf_spectrum(n, SEED, m), n)[0]
+                             for m in range(M)])
+            e.set_state_compact(init.astype(np.complex64 if prec == 4 else np.complex128))
+            e.set_forcing(hz.kolmogorov_forcing(n)[None])
+            e.set_time(0.0, 0)
+            ens[prec] = e
+        K = (n - 1) // 3
+        w = np.full(ens[8].compact_size, 2.0)
+        w[:2 * K + 1] = 1.0   # the kx = 0 column holds both signs of ky
+        series, seconds = [], {4: 0.0, 8: 0.0}
+        for done in range(every, steps + 1, every):
+            for prec in (4, 8):
+                t0 = time.perf_counter()
+                ens[prec].step(dt, every)
+                ens[prec].synchronize()
+                seconds[prec] += time.perf_counter() - t0
+            a = ens[4].get_state_compact().astype(np.complex128)
+            b = ens[8].get_state_compact()
+            za, zb = (w * np.abs(a) ** 2).sum(axis=1), (w * np.abs(b) ** 2).sum(axis=1)
+            err = np.sqrt((w * np.abs(a - b) ** 2).sum(axis=1) / zb)
+            drift = np.abs(za / zb - 1)
+            series.append({"step": done, "l2_max": float(err.max()),
+                           "l2_median": float(np.median(err)),
+                           "l2_p90": float(np.percentile(err, 90)),
+                           "enstrophy_drift_max": float(drift.max()),
+                           "enstrophy_drift_median": float(np.median(drift))})
+        status = {"f32": ens[4].status(), "f64": ens[8].status()}
+        for e in ens.values():
+            e.close()
+        return {"workload": f"{M} members at {n}^2, nu {nu}, dt {dt}, {steps} steps, Kolmogorov "
+                            f"forcing + sigma {SIGMA} Philox noise, seeded random fields; FP32 "
+                            "against FP64 from identical inputs",
+                "final": series[-1], "series": series, "status": status,
+                "wall_seconds": {"f32": seconds[4], "f64": seconds[8]}}
+    except Exception as exc:   # report, never lose the main line
+        return {"error": f"{type(exc).__name__}: {exc}"}
 
 
 def mixed_experiment() -> dict:
@@ -578,17 +709,6 @@ def main():
         pg = dist
 
     M = args.members
-    cfg = hz.Config(n=N, members=M, precision=4, nu=NU, alpha=0.0, forcing_kmax=0,
-                    noise_sigma=SIGMA, noise_kmax=4, seed=SEED, member_base=rank * M, device=local)
-    ens = hz.Ensemble(cfg)
-    # seeded initial fields (host FP64 generator, compact layout)
-    init = np.zeros((M, ens.compact_size), np.complex64)
-    for m in range(M):
-        init[m] = hz.full_to_compact(hz.grf_spectrum(N, SEED, rank * M + m), N)[0]
-    ens.set_state_compact(init)
-    ens.set_forcing(hz.kolmogorov_forcing(N)[None])
-    ens.set_time(0.0, 0)
-    stream = torch.cuda.ExternalStream(ens.stream)
 
     def barrier():
         torch.cuda.synchronize()
@@ -602,63 +722,16 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
-    # ---- value: device-resident steps ---------------------------------------------
-    for _ in range(args.warmup):
-        ens.step(DT, 1)
-    ens.synchronize()
-    barrier()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
-            ens.step(DT, 1)
-        stop.record(stream)
-        ens.synchronize()
-        barrier()
-    ms = start.elapsed_time(stop)
-    ms = max_over_ranks(ms)
-    status = ens.status()
-    value = world * M * args.steps / (ms / 1e3)
-    ms_per_step = ms / args.steps
-
-    # ---- roofline: per-launch events on the library stream -----------------------
-    row_ms, col_ms = ens.step_profiled(DT, max(2, args.steps // 4))
-    K = (N - 1) // 3
-    C, LD = K + 1, 2 * K + 1
-    cb = 8  # complex64 bytes
-    # per launch: row kernel reads the 2 velocity column fields and writes the 2 product fields;
-    # column kernel reads the 2 product fields, writes the 2 velocity fields and reads/writes
-    # the compact state, stage input and accumulator (3, 5, 5, 4 entries per mode on stages
-    # 1-4: 4.25 on average)
-    row_bytes = M * (2 * C * N + 2 * C * N) * cb
-    col_bytes = int(M * (2 * C * N + 2 * C * N + 4.25 * C * LD) * cb)
-    row_gbs = row_bytes / (row_ms * 1e-3) / 1e9
-    col_gbs = col_bytes / (col_ms * 1e-3) / 1e9
-    peak, peak_kind = peaks()
-    dom = ("column_kernel", col_gbs, col_bytes, col_ms) if col_ms >= row_ms else \
-        ("row_kernel", row_gbs, row_bytes, row_ms)
-    traffic = NCU_TRAFFIC_PER_MEMBER[dom[0]] * M
-
-    # ---- e2e: host state in/out around every step ---------------------------------
-    state_bytes = M * ens.compact_size * cb
-    host_in = torch.from_numpy(ens.get_state_compact().view(np.float32)).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    e2e_steps = max(3, args.steps // 2)
-    # every step reads the whole state from pinned host memory and writes the result back
-    # (hzlb_step_host: member chunks whose copies overlap the stepping of the others)
-    for _ in range(2):
-        ens.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), DT, 1)
-    barrier()
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for _ in range(e2e_steps):
-        ens.step_host_ptr(host_in.data_ptr(), host_out.data_ptr(), DT, 1)
-    t1.record(stream)
-    ens.synchronize()
-    barrier()
-    e2e_ms = max_over_ranks(t0.elapsed_time(t1))
-    e2e_value = world * M * e2e_steps / (e2e_ms / 1e3)
+    # ---- the headline: FP32 at 256^2 --------------------------------------------------
+    ens = build_ensemble(hz, 4, M, rank * M, local)
+    clocks = ClockSampler(local)
+    main_leg = measure(hz, torch, ens, 4, args.steps, args.warmup, world, barrier, max_over_ranks,
+                       clocks)
+    ens.close()
+    # ---- the same workload in FP64 (the reference's precision), same members and steps ----
+    ens = build_ensemble(hz, 8, M, rank * M, local)
+    fp64 = measure(hz, torch, ens, 8, args.steps, args.warmup, world, barrier, max_over_ranks)
+    ens.close()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -669,13 +742,15 @@ def main():
         except Exception as exc:   # the reference library is test infrastructure; report why
             cpu = {"value": None, "unit": "member-steps/s", "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
+    if cpu and cpu.get("value"):
+        fp64["vs_cpu_reference"] = fp64["value"] / cpu["value"]
+        fp64["e2e"]["vs_cpu_reference"] = fp64["e2e"]["value"] / cpu["value"]
 
-    ens.close()
-    learned = gpu_ref = fp64 = filters = mixed = likelihood = tangent = None
+    learned = gpu_ref = filters = mixed = likelihood = tangent = config1 = None
     if rank == 0 and world == 1:
-        fp64 = fp64_sample(hz, torch, N)
         if not args.no_cpu_baseline:
             gpu_ref = reference_gpu_sample(N)
+        config1 = config1_experiment(hz)
         if not args.no_learned:
             learned = learned_experiment()
             filters = filter_experiment(not args.no_cpu_baseline)
@@ -683,34 +758,24 @@ def main():
             likelihood = likelihood_experiment(not args.no_cpu_baseline)
             tangent = tangent_experiment(not args.no_cpu_baseline)
 
-    model_bytes = 32 * 8 * N * (N // 2 + 1) + 16 * 8 * N * N
     if rank == 0:
         out = {
-            "metric": METRIC, "value": value, "unit": "member-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
+            "metric": METRIC, "value": main_leg["value"], "unit": "member-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": main_leg["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": arm_config(M, world),
-            "roofline": {"bound": "hbm", "kernel": dom[0], "achieved": dom[1], "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": dom[1] / peak,
-                         "traffic": traffic, "algorithmic_bytes": dom[2],
-                         "launch_ms": dom[3],
-                         "row_kernel": {"ms": row_ms, "gbs": row_gbs},
-                         "column_kernel": {"ms": col_ms, "gbs": col_gbs},
-                         # the whole-step byte model B32(N) = 32 S + 16 P of a schedule that
-                         # moves five real fields per stage (S = 8 N (N/2+1), P = 8 N^2 bytes);
-                         # this design moves fewer bytes, so this fraction exceeds 1
-                         "step_model": {"bytes_per_member_step": model_bytes,
-                                        "achieved": value * model_bytes / 1e9,
-                                        "frac": value * model_bytes / 1e9 / peak}},
-            "cpu_baseline": cpu,
-            "gpu_reference": gpu_ref,
-            "fp64": fp64,
-            "e2e": {"value": e2e_value, "unit": "member-steps/s",
-                    "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes},
-            "gpu_launches": 8 * args.steps,
+            "roofline": main_leg["roofline"],
+            "e2e": main_leg["e2e"],
+            "gpu_launches": main_leg["gpu_launches"],
             "clocks": clocks.summary(),
-            "status": status,
+            "status": main_leg["status"],
+            "cpu_baseline": cpu,
+            # the same workload in FP64, the reference's precision: like-for-like with the
+            # reference arm and with gpu_reference
+            "fp64": fp64,
+            "gpu_reference": gpu_ref,
+            "config1": config1,
             "learned": learned,
             "filters": filters,
             "mixed": mixed,

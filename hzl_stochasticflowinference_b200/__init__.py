@@ -129,6 +129,7 @@ def library() -> C.CDLL:
         "hzlb_compact_size": (C.c_size_t, [vp]),
         "hzlb_set_forcing": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
         "hzlb_step": (C.c_int, [vp, C.c_double, C.c_uint64]),
+        "hzlb_step_checked": (C.c_int, [vp, C.c_double]),
         "hzlb_step_host": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, C.c_int]),
         "hzlb_status": (C.c_int, [vp, _u32p]),
         "hzlb_synchronize": (C.c_int, [vp]),
@@ -404,6 +405,10 @@ class Ensemble:
     def step(self, dt: float, steps: int = 1):
         _check(self._lib.hzlb_step(self._h, dt, steps))
 
+    def step_checked(self, dt: float):
+        """One step that is undone when its stage-1 CFL check fails (hzlb_step_checked);
+        raises HzlbError (HZLB_ERUNTIME) in that case."""
+        _check(self._lib.hzlb_step_checked(self._h, dt))
     def step_profiled(self, dt: float, steps: int):
         """Steps with per-launch CUDA events; returns mean (row_ms, column_ms) per launch."""
         r, c = C.c_double(), C.c_double()

@@ -94,6 +94,9 @@ int hzlb_set_forcing(hzlb_ensemble *h, const double *spectra, int first, int cou
 int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps) {
     return guarded([&] { engine(h).step(dt, nsteps); });
 }
+int hzlb_step_checked(hzlb_ensemble *h, double dt) {
+    return guarded([&] { engine(h).step_checked(dt); });
+}
 int hzlb_step_host(hzlb_ensemble *h, const void *state_in, void *state_out, double dt,
                    uint64_t nsteps, int chunk_members) {
     return guarded([&] { engine(h).step_host(state_in, state_out, dt, nsteps, chunk_members); });

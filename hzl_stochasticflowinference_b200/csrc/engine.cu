@@ -77,12 +77,7 @@ template <typename R> class EngineT final : public Engine {
         if (fcount_)
             cuda_check(cudaMemsetAsync(forcing_.ptr, 0, forcing_.bytes, stream_), "clear forcing");
         cuda_check(cudaMemsetAsync(ctl_.ptr, 0, sizeof(StepControl), stream_), "clear control");
-        // W_N^k = exp(-2 pi i k / N), the construction of the reference's roots (fft.cpp:25-27)
-        std::vector<cx<R>> tw(n_);
-        for (int k = 0; k < n_; ++k) {
-            const double theta = -2.0 * kPi * static_cast<double>(k) / static_cast<double>(n_);
-            tw[k] = mk<R>(static_cast<R>(std::cos(theta)), static_cast<R>(std::sin(theta)));
-        }
+        const std::vector<cx<R>> tw = host_twiddles<R>(n_);
         cuda_check(cudaMemcpyAsync(tw_.ptr, tw.data(), cb * n_, cudaMemcpyHostToDevice, stream_),
                    "upload twiddles");
         cuda_check(cudaStreamSynchronize(stream_), "initialise ensemble");
@@ -501,6 +496,44 @@ template <typename R> class EngineT final : public Engine {
         w_valid_ = true;
         time += dt * static_cast<double>(nsteps);
         step_index += nsteps;
+    }
+    // One step with the reference CudaSolver's failure semantics (cuda_solver.cu:106-117,
+    // 203-215): its stage-1 CFL check throws before the state changes.  Here the step runs
+    // and, when its stage-1 row pass flagged the CFL limit, the state, forcing, control word,
+    // clock and step counter are put back from a device copy taken before it.
+    void step_checked(double dt) override {
+        const size_t sb = sizeof(cx<R>) * compact_ * M_;
+        const size_t fb = fcount_ ? sizeof(cx<R>) * static_cast<size_t>(fcols_) * LD_ * fcount_ : 0;
+        backup_.ensure(sb + fb + sizeof(StepControl) + 64, "allocate step backup");
+        unsigned char *bk = backup_.as<unsigned char>();
+        cuda_check(cudaMemcpyAsync(bk, omega_.ptr, sb, cudaMemcpyDeviceToDevice, stream_), "back up state");
+        if (fb)
+            cuda_check(cudaMemcpyAsync(bk + sb, forcing_.ptr, fb, cudaMemcpyDeviceToDevice, stream_),
+                       "back up forcing");
+        cuda_check(cudaMemcpyAsync(bk + sb + fb, ctl_.ptr, sizeof(StepControl),
+                                   cudaMemcpyDeviceToDevice, stream_),
+                   "back up step control");
+        const double t0 = time;
+        const uint64_t s0 = step_index;
+        step(dt, 1);
+        StepControl c{};
+        cuda_check(cudaMemcpyAsync(&c, ctl_.ptr, sizeof c, cudaMemcpyDeviceToHost, stream_),
+                   "read status");
+        cuda_check(cudaStreamSynchronize(stream_), "checked step");
+        if (!(c.status & STATUS_CFL))
+            return;
+        cuda_check(cudaMemcpyAsync(omega_.ptr, bk, sb, cudaMemcpyDeviceToDevice, stream_), "restore state");
+        if (fb)
+            cuda_check(cudaMemcpyAsync(forcing_.ptr, bk + sb, fb, cudaMemcpyDeviceToDevice, stream_),
+                       "restore forcing");
+        cuda_check(cudaMemcpyAsync(ctl_.ptr, bk + sb + fb, sizeof(StepControl),
+                                   cudaMemcpyDeviceToDevice, stream_),
+                   "restore step control");
+        cuda_check(cudaStreamSynchronize(stream_), "restore state");
+        time = t0;
+        step_index = s0;
+        w_valid_ = false;
+        raise(HZLB_ERUNTIME, "GPU CFL limit exceeded");
     }
     // Steps the ensemble whose state lives on the host: members [f, f+k) of each chunk are
     // copied in, stepped and copied out, the copies of one chunk overlapping the stepping of
@@ -1174,7 +1207,7 @@ template <typename R> class EngineT final : public Engine {
     size_t compact_ = 0;
     cudaStream_t stream_ = nullptr;
     DeviceBuffer omega_, ystage_, acc_, w_, nl_, forcing_, ctl_, tw_, phys_, scratch_d_, vbits_,
-        obs_xy_, obs_, anc_, enkf_, aux_, split_, pfw_, pfrec_, pfctl_, pfobs_, pfone_;
+        obs_xy_, obs_, anc_, enkf_, aux_, split_, pfw_, pfrec_, pfctl_, pfobs_, pfone_, backup_;
     int pf_particles_ = 0;
     PinnedBuffer staging_, fstage_[2];
     cudaEvent_t fevent_[2] = {nullptr, nullptr};

@@ -90,6 +90,8 @@ class Engine {
     virtual void get_state_compact(void *data, int first, int count) = 0;
     virtual void set_forcing(const double *spectra, int first, int count) = 0;
     virtual void step(double dt, uint64_t nsteps) = 0;
+    // one step, undone (state, forcing, clock, counter) when its stage-1 CFL check fails
+    virtual void step_checked(double dt) = 0;
     // nsteps steps of a host-resident state (compact layout): copied in, stepped and copied
     // out in member chunks that overlap copies with stepping
     virtual void step_host(const void *in, void *out, double dt, uint64_t nsteps, int chunk) = 0;

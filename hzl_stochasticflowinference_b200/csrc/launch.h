@@ -2,6 +2,9 @@
 #pragma once
 #include "spectral_step.cuh"
 
+#include <cmath>
+#include <vector>
+
 namespace hzlb {
 
 struct KernelShape {
@@ -10,6 +13,18 @@ struct KernelShape {
     size_t col_smem, row_smem;
     int elements_per_thread, rows_per_block;
 };
+
+// The transform's twiddle table W_N^k = exp(-2 pi i k / N), k < N, built on the host in double
+// precision as the reference builds its roots (std::polar, fft.cpp:25-27), then rounded to R.
+template <typename R> std::vector<cx<R>> host_twiddles(int n) {
+    std::vector<cx<R>> tw(n);
+    for (int k = 0; k < n; ++k) {
+        const double theta = -2.0 * 3.141592653589793238462643383279502884 * static_cast<double>(k) /
+                             static_cast<double>(n);
+        tw[k] = mk<R>(static_cast<R>(std::cos(theta)), static_cast<R>(std::sin(theta)));
+    }
+    return tw;
+}
 
 template <typename R> cudaError_t prepare_kernels(int n);
 // cap > 0 limits the persistent grid to cap blocks (default: all resident blocks of the device)

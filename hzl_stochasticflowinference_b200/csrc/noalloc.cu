@@ -6,7 +6,7 @@
 // allocates the stage buffers with cudaMalloc, so those callers use this entry point instead.
 // It runs the same row and column kernels as hzlb_step, but every scratch buffer they need
 // (the stage input, the RK accumulator, the velocity rows, the product columns, the step
-// control word, the twiddle table and a padded working copy of the state) is carved out of
+// control word, the twiddle tables and a padded working copy of the state) is carved out of
 // one file-scope device array of HZLB_NOALLOC_SCRATCH_BYTES.  The caller passes the state
 // (in/out) and the forcing; nothing here calls cudaMalloc, cudaFree or any allocating routine.
 //
@@ -16,16 +16,24 @@
 // whose work overlaps on the GPU (different streams, or different host threads on the same
 // device) race on the array, so serialise them.
 //
-// The first call on each device does a one-time set-up with that device current: it resolves
-// the array's device address with cudaGetSymbolAddress (in host code the array's name is only
-// a host-side stand-in, not a device address) and configures the kernels.  Make that first
-// call before any stream capture on the device.
+// The first call on each device, and the first for each (precision, grid) on it, does a
+// one-time set-up with that device current: it resolves the array's device address with
+// cudaGetSymbolAddress (in host code the array's name is only a host-side stand-in, not a
+// device address), configures the kernels, and writes the twiddle table of that grid -- the
+// host FP64 table hzlb_ensemble_create builds, so both entry points give identical results --
+// into a region of the array reserved for it.  Make those first calls before any stream
+// capture on the device.
+//
+// Array layout: [twiddle tables of every grid 8..512, FP32 then FP64 | step control word |
+// state copy | stage input | RK accumulator | velocity rows | product columns], each piece
+// rounded up to 256 bytes (layout() below).
 #include "engine.h"
 
 #include <algorithm>
 #include <cmath>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace hzlb {
 namespace {
@@ -40,34 +48,32 @@ struct DeviceSetup {
 std::mutex g_setup_mutex;
 DeviceSetup g_setup[kMaxDevices];
 
-template <typename R> __global__ void noalloc_init(StepControl *ctl, cx<R> *tw, int n,
-                                                  unsigned long long first_step) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        ctl->step = first_step;
-        ctl->arrivals = 0;
-        ctl->status = 0;
-    }
-    // W_N^k = exp(-2 pi i k / N)
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const double theta = -2.0 * 3.141592653589793238462643383279502884 * k / n;
-        double s, c;
-        sincos(theta, &s, &c);
-        tw[k] = mk<R>(static_cast<R>(c), static_cast<R>(s));
-    }
+__global__ void noalloc_init(StepControl *ctl, unsigned long long first_step) {
+    ctl->step = first_step;
+    ctl->arrivals = 0;
+    ctl->status = 0;
 }
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
+// Twiddle tables of every grid 8, 16, .., 512, one after another: FP32 ones (8 bytes an entry)
+// from offset 0, FP64 ones (16 bytes) from kTwDouble.
+constexpr size_t kTwEntries = 8 + 16 + 32 + 64 + 128 + 256 + 512;
+constexpr size_t kTwDouble = (kTwEntries * 8 + 255) / 256 * 256;
+constexpr size_t kTwRegion = kTwDouble + (kTwEntries * 16 + 255) / 256 * 256;
+template <typename R> size_t twiddle_offset(int n) {
+    return (sizeof(R) == 4 ? 0 : kTwDouble) + sizeof(cx<R>) * static_cast<size_t>(n - 8);
+}
+
 struct Layout {
-    size_t ctl, tw, omega, ystage, acc, w, nl, total;
+    size_t ctl, omega, ystage, acc, w, nl, total;
 };
 template <typename R> Layout layout(int n, int members) {
     const size_t K = (n - 1) / 3, C = K + 1, LD = 2 * K + 1, cb = sizeof(cx<R>);
     const size_t state = align256(cb * C * LD * members + 16);   // +16: bulk-copy slack
     Layout l{};
-    l.ctl = 0;
-    l.tw = align256(sizeof(StepControl));
-    l.omega = l.tw + align256(cb * n);
+    l.ctl = kTwRegion;
+    l.omega = l.ctl + align256(sizeof(StepControl));
     l.ystage = l.omega + state;
     l.acc = l.ystage + state;
     l.w = l.acc + state;
@@ -76,11 +82,9 @@ template <typename R> Layout layout(int n, int members) {
     return l;
 }
 
-// One-time set-up of `device` (current while this runs): the scratch array's device address
-// and the kernel configuration for (precision, n).
+// One-time set-up of `device` (current while this runs): the scratch array's device address,
+// and for (precision, n) the kernel configuration and the twiddle table.
 template <typename R> unsigned char *setup_device(int device, int n) {
-    if (device < 0 || device >= kMaxDevices)
-        raise(HZLB_EINVAL, "invalid CUDA device ordinal");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
     DeviceSetup &d = g_setup[device];
     if (!d.scratch) {
@@ -94,6 +98,10 @@ template <typename R> unsigned char *setup_device(int device, int n) {
     const uint32_t bit = 1u << ((sizeof(R) == 4 ? 0 : 8) + lg);
     if (!(d.prepared & bit)) {
         cuda_check(prepare_kernels<R>(n), "configure kernels");
+        const std::vector<cx<R>> tw = host_twiddles<R>(n);
+        cuda_check(cudaMemcpy(d.scratch + twiddle_offset<R>(n), tw.data(), sizeof(cx<R>) * n,
+                              cudaMemcpyHostToDevice),
+                   "write no-alloc twiddle table");
         d.prepared |= bit;
     }
     return d.scratch;
@@ -113,10 +121,10 @@ void step_noalloc(const hzlb_config &c, double dt, uint64_t nsteps, uint64_t fir
     const int K = (n - 1) / 3, C = K + 1, LD = 2 * K + 1;
     const size_t state_bytes = sizeof(cx<R>) * static_cast<size_t>(C) * LD * M;
     StepControl *ctl = reinterpret_cast<StepControl *>(base + l.ctl);
-    cx<R> *tw = reinterpret_cast<cx<R> *>(base + l.tw);
+    const cx<R> *tw = reinterpret_cast<const cx<R> *>(base + twiddle_offset<R>(n));
     cx<R> *omega = reinterpret_cast<cx<R> *>(base + l.omega);
 
-    noalloc_init<R><<<1, 256, 0, stream>>>(ctl, tw, n, first_step);
+    noalloc_init<<<1, 1, 0, stream>>>(ctl, first_step);
     cuda_check(cudaGetLastError(), "launch no-alloc set-up");
     cuda_check(cudaMemcpyAsync(omega, state, state_bytes, cudaMemcpyDeviceToDevice, stream),
                "copy state into scratch");
@@ -196,6 +204,10 @@ extern "C" HZLB_API int hzlb_step_noalloc(const hzlb_config *config, double dt, 
         const int largest = (c.n - 1) / 3;
         if (!std::isfinite(dt) || dt <= 0 || dt * (2 * c.nu * largest * largest + c.alpha) > 2.5)
             raise(HZLB_EINVAL, "invalid GPU time step or diffusion stability limit exceeded");
+        int devices = 0;
+        cuda_check(cudaGetDeviceCount(&devices), "query CUDA devices");
+        if (c.device < 0 || c.device >= std::min(devices, kMaxDevices))
+            raise(HZLB_EINVAL, "invalid CUDA device ordinal");
         cuda_check(cudaGetDevice(&previous), "query current device");
         cuda_check(cudaSetDevice(c.device), "select CUDA device");
         const cudaStream_t s = static_cast<cudaStream_t>(stream);

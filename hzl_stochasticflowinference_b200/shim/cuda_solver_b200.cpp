@@ -1,15 +1,18 @@
 // hzl::CudaSolver on the B200 engine: a drop-in replacement for the reference's
 // src/cuda_solver.cu behind its unchanged header include/hzl/cuda_solver.hpp.  Build it in
-// place of src/cuda_solver.cu and link libhzlb.so; every other reference
-// file stays as it is.
+// place of src/cuda_solver.cu and link libhzlb.so; every other reference file stays as it is.
 //
 // Semantics kept from the reference (src/cuda_solver.cu):
 //  * constructor: validates the grid (Fourier2D), the parameters and the initial field size,
 //    rejects nonfinite coefficients, keeps only the 2/3-rule modes (:126-171);
 //  * step(dt): sigma must be 0 (:173-183); step(dt, forcing): forcing of size n*n, finite and
 //    conjugate-symmetric to 1e-12 (:184-202); RK4 with the forcing held over the step;
-//  * std::invalid_argument for bad input, std::runtime_error for CFL violations and CUDA
-//    failures, nonfinite results on download (:222-235).
+//  * std::invalid_argument for bad input and for a time step beyond the diffusion bound
+//    (:205-208); std::runtime_error for CUDA failures;
+//  * a step whose stage-1 velocities violate the CFL limit throws "GPU CFL limit exceeded"
+//    and leaves the state as it was (:106-117); a nonfinite state makes that rate nonfinite,
+//    so every step after a nonfinite result throws the same way;
+//  * nonfinite coefficients throw "nonfinite GPU result" on download (:222-235).
 // The flow state stays on the device between calls; one member per instance.
 #include "hzl/cuda_solver.hpp"
 #include "hzlb.h"
@@ -36,6 +39,7 @@ struct CudaSolver::Implementation {
     std::size_t n = 0;
     Parameters p;
     bool external_forcing = false;
+    bool nonfinite = false;   // the last step left a nonfinite coefficient
     ~Implementation() {
         if (handle)
             hzlb_ensemble_destroy(handle);
@@ -92,13 +96,13 @@ void CudaSolver::step(double dt, const Field &forcing) {
 
 void CudaSolver::advance(double dt) {
     auto &s = *implementation_;
-    throw_on(hzlb_step(s.handle, dt, 1));
+    if (s.nonfinite)   // the reference's stage-1 rate of a nonfinite state is not finite
+        throw std::runtime_error("GPU CFL limit exceeded");
+    throw_on(hzlb_step_checked(s.handle, dt));
     uint32_t status = 0;
     throw_on(hzlb_status(s.handle, &status));
-    if (status & HZLB_STATUS_CFL)
-        throw std::runtime_error("GPU CFL limit exceeded");
     if (status & HZLB_STATUS_NONFINITE)
-        throw std::runtime_error("nonfinite GPU result");
+        s.nonfinite = true;
 }
 
 void CudaSolver::synchronize() { throw_on(hzlb_synchronize(implementation_->handle)); }
@@ -107,6 +111,9 @@ Field CudaSolver::coefficients() const {
     const auto &s = *implementation_;
     Field result(s.n * s.n);
     throw_on(hzlb_get_state(s.handle, reinterpret_cast<double *>(result.data()), 0, 1));
+    for (const auto &z : result)
+        if (!std::isfinite(z.real()) || !std::isfinite(z.imag()))
+            throw std::runtime_error("nonfinite GPU result");
     return result;
 }
 

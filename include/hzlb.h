@@ -126,6 +126,11 @@ HZLB_API int hzlb_get_forcing_compact(hzlb_ensemble *h, double *out, int first, 
  * HZLB_EINVAL for a nonpositive/nonfinite dt or dt * (2 nu K^2 + alpha) > 2.5
  * (cuda_solver.cu:205-208). */
 HZLB_API int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps);
+/* One RK4 step with CudaSolver::advance's failure semantics (cuda_solver.cu:106-117,
+ * 203-215): when the stage-1 velocities of some member violate dt max(|u|+|v|) n/2pi <= 0.5,
+ * the state, forcing, clock and step counter are left as they were before the call and
+ * HZLB_ERUNTIME ("GPU CFL limit exceeded") is returned.  Synchronous. */
+HZLB_API int hzlb_step_checked(hzlb_ensemble *h, double dt);
 /* No counterpart in the reference (its CudaSolver copies each member's state in and out around
  * every step, cuda_solver.cu:173-235).  The ensemble state lives on the host: state_in is read
  * and state_out written (both all members, the compact layout of the configured precision, as
@@ -428,10 +433,14 @@ HZLB_API int hzlb_gemm(int M, int N, int K, int dtype, const void *A, long long 
  * of the configured precision, advanced in place by nsteps steps of dt; forcing: device
  * pointer in the compact forcing layout (columns kx <= forcing_kmax, one field or one per
  * member) or NULL; first_step: noise counter of the first step; stream: a cudaStream_t or
- * NULL; status: if non-NULL, the call waits for the stream and stores the HZLB_STATUS_* bits.
- * Sizes whose scratch exceeds the limit are HZLB_EINVAL.  The first call on a device resolves
- * the array's device address and configures the kernels; make it before any stream capture.
- * Calls share the array, so calls that overlap on the GPU race: serialise them. */
+ * NULL; status: if non-NULL, the call waits for the stream and stores the HZLB_STATUS_* bits;
+ * with status NULL the call does not wait and the step's CFL, nonfinite and timeout bits are
+ * lost (the next call clears them), so a caller that captures the call into a graph has no
+ * error report from it.  Sizes whose scratch exceeds the limit are HZLB_EINVAL (for example
+ * at most 31 members at 256^2 FP32, 15 in FP64).  The first call on a device, and the first
+ * for each (precision, n) on it, resolves the array's device address, configures the kernels
+ * and writes that grid's twiddle table into the array; make those calls before any stream
+ * capture.  Calls share the array, so calls that overlap on the GPU race: serialise them. */
 #define HZLB_NOALLOC_SCRATCH_BYTES (32u << 20)
 HZLB_API int hzlb_step_noalloc(const hzlb_config *config, double dt, uint64_t nsteps,
                                uint64_t first_step, void *state, const void *forcing, void *stream,

@@ -252,6 +252,8 @@ class Reference:
         lib.ref_shell_forcing_midpoint_step.argtypes = [C.c_void_p, C.c_double, _dp]
         lib.ref_shell_forcing_coefficients.argtypes = [C.c_void_p, _dp]
         lib.ref_ensemble.argtypes = [C.c_int, _dp, C.c_double, _u64, _u64, _u64, _u64, _dp]
+        lib.ref_synthetic_ensemble.argtypes = [C.c_int, C.c_double, C.c_double, _u64, _u64, _u64,
+                                               _u64, C.c_double, C.c_int, _dp]
         u64p = C.POINTER(_u64)
         lib.ref_synthetic_observations.argtypes = [C.c_int, C.c_double, _u64, _u64, _dp, C.c_double,
                                                    _u64, _u64, u64p, u64p, _u32p, _u32p, _dp, _dp]
@@ -295,6 +297,16 @@ class Reference:
 
     def solver(self, n: int, p6, seed: int) -> "ReferenceSolver":
         return ReferenceSolver(self, n, p6, seed)
+
+    def synthetic_ensemble(self, n: int, nu: float, dt: float, steps: int, count: int,
+                           workers: int, seed: int, sigma: float = 0.05, noise_kmax: int = 4,
+                           keep: bool = True):
+        """The benchmark's seeded-synthetic workload through the reference's Solver API on
+        `workers` threads (ref_synthetic_ensemble); final spectra (count, n, n) or None."""
+        out = np.zeros((count, n, n), np.complex128) if keep else None
+        self.check(self.lib.ref_synthetic_ensemble(n, nu, dt, steps, count, workers, seed, sigma,
+                                                   noise_kmax, _ptr(out) if keep else None))
+        return out
 
     def solver_load(self, path) -> "ReferenceSolver":
         """Solver::load (src/solver.cpp:453-491)."""

@@ -14,12 +14,18 @@
 #include "hzl/reduced.hpp"
 #include "hzl/solver.hpp"
 
+#include <atomic>
 #include <cstring>
 #include <exception>
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
+
+extern "C" {
+#include "hzl_oracle.h"
+}
 
 namespace {
 thread_local std::string last_error;
@@ -212,6 +218,71 @@ int ref_ensemble(int n, const double *p6, double dt, unsigned long long steps,
             out6xcount[6 * i + 4] = r[i].injection;
             out6xcount[6 * i + 5] = r[i].cfl_rate;
         }
+    });
+}
+
+// ---- the seeded-synthetic workload through the reference's public API ---------------------
+// `count` members of the benchmark physics, each a reference hzl::Solver: OU forcing switched
+// off (sigma 0, tau 1e300: the transition's decay is exactly 1 and its scale 0, so the latent
+// forcing stays as installed, src/solver.cpp:93-105), the Kolmogorov forcing and the member's
+// random initial field installed by Solver::update_latent_state, then per step Solver::step(dt)
+// (RK4 with its validate_step) and the Euler-Maruyama noise of that step (the oracle's Philox
+// draws, keyed by (seed, member)) added through update_latent_state.  Members are shared out
+// over `workers` threads as hzl::ensemble does (src/inference.cpp:555-590).  final_out (may be
+// null) receives the members' final spectra, n*n interleaved complex each.
+int ref_synthetic_ensemble(int n, double nu, double dt, unsigned long long steps,
+                           unsigned long long count, unsigned long long workers,
+                           unsigned long long seed, double sigma, int noise_kmax,
+                           double *final_out) {
+    return guarded([&] {
+        if (n < 16 || count == 0 || workers == 0)
+            throw std::invalid_argument("invalid synthetic ensemble");
+        const std::size_t nn = static_cast<std::size_t>(n) * n;
+        hzl::Parameters p;
+        p.viscosity = nu;
+        p.friction = 0.0;
+        p.forcing_sigma = 0.0;
+        p.forcing_tau = 1e300;
+        p.forcing_min = 4;
+        p.forcing_max = 4;
+        std::vector<double> kolm(2 * nn);
+        if (ho_kolmogorov_forcing(n, 0.1, 4, kolm.data()) != 0)
+            throw std::runtime_error("Kolmogorov forcing");
+        const hzl::Field forcing = to_field(kolm.data(), nn);
+        std::atomic<unsigned long long> next{0};
+        std::vector<std::string> errors(workers);
+        auto work = [&](std::size_t w) {
+            try {
+                std::vector<double> buf(2 * nn);
+                for (unsigned long long m = next++; m < count; m = next++) {
+                    hzl::Solver s(static_cast<std::size_t>(n), p, 0);
+                    if (ho_grf_spectrum(n, seed, static_cast<uint32_t>(m), buf.data()) != 0)
+                        throw std::runtime_error("random field");
+                    s.update_latent_state(to_field(buf.data(), nn), forcing);
+                    for (unsigned long long i = 0; i < steps; ++i) {
+                        s.step(dt);
+                        from_field(s.coefficients(), buf.data());
+                        ho_add_noise(n, buf.data(), sigma, dt, noise_kmax, seed,
+                                     static_cast<uint32_t>(m), i);
+                        // a copy: update_latent_state must not read the forcing it rewrites
+                        const hzl::Field f = s.forcing();
+                        s.update_latent_state(to_field(buf.data(), nn), f);
+                    }
+                    if (final_out)
+                        from_field(s.coefficients(), final_out + 2 * nn * m);
+                }
+            } catch (const std::exception &e) {
+                errors[w] = e.what();
+            }
+        };
+        {
+            std::vector<std::jthread> pool;
+            for (std::size_t w = 0; w < workers; ++w)
+                pool.emplace_back(work, w);
+        }
+        for (const auto &e : errors)
+            if (!e.empty())
+                throw std::runtime_error(e);
     });
 }
 

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <iostream>
 #include <stdexcept>
+#include <string>
 
 int main(int argc, char **argv) {
     try {
@@ -52,11 +53,46 @@ int main(int argc, char **argv) {
         } else {
             threw = true;
         }
+        // CFL semantics (cuda_solver.cu:106-117): a step whose stage-1 velocities violate
+        // dt * rate <= 0.5 throws "GPU CFL limit exceeded" before the state changes; the
+        // instance then steps on normally from the same state
+        hzl::Solver fresh(n, p, 0);
+        fresh.initialize("multimode");
+        hzl::CudaSolver probe(n, p, fresh.coefficients());
+        const auto before = probe.coefficients();
+        const double bad = 0.75 / fresh.diagnostics().cfl_rate;
+        const int largest = static_cast<int>((n - 1) / 3);
+        bool cfl_threw = false, cfl_unchanged = false, cfl_recovered = false;
+        if (bad * (2 * p.viscosity * largest * largest + p.friction) <= 2.5) {
+            const hzl::Field zero(n * n);
+            try {
+                if (p.forcing_sigma > 0)
+                    probe.step(bad, zero);
+                else
+                    probe.step(bad);
+            } catch (const std::runtime_error &e) {
+                cfl_threw = std::string(e.what()) == "GPU CFL limit exceeded";
+            }
+            cfl_unchanged = probe.coefficients() == before;
+            hzl::CudaSolver twin(n, p, fresh.coefficients());
+            if (p.forcing_sigma > 0) {
+                probe.step(dt, zero);
+                twin.step(dt, zero);
+            } else {
+                probe.step(dt);
+                twin.step(dt);
+            }
+            cfl_recovered = probe.coefficients() == twin.coefficients();
+        } else {
+            cfl_threw = cfl_unchanged = cfl_recovered = true;   // diffusion bound first: n/a
+        }
         std::cout.precision(17);
         std::cout << "{\"n\":" << n << ",\"steps\":" << steps << ",\"relative_l2_error\":"
                   << std::sqrt(num / den) << ",\"invalid_argument_on_missing_forcing\":"
-                  << (threw ? "true" : "false") << "}\n";
-        return std::sqrt(num / den) <= 1e-9 && threw ? 0 : 2;
+                  << (threw ? "true" : "false") << ",\"cfl_throws\":" << (cfl_threw ? "true" : "false")
+                  << ",\"cfl_state_unchanged\":" << (cfl_unchanged ? "true" : "false")
+                  << ",\"cfl_steps_on\":" << (cfl_recovered ? "true" : "false") << "}\n";
+        return std::sqrt(num / den) <= 1e-9 && threw && cfl_threw && cfl_unchanged && cfl_recovered ? 0 : 2;
     } catch (const std::exception &e) {
         std::cerr << "error: " << e.what() << '\n';
         return 1;

@@ -104,6 +104,21 @@ def test_config0_golden(oracle):
     np.testing.assert_allclose(series, g["series"], rtol=1e-12)
 
 
+def test_reference_synthetic_driver_matches_oracle(oracle, reference):
+    """The benchmark's seeded-synthetic workload driven through the reference's own Solver
+    (update_latent_state + step, threads as hzl::ensemble) equals the oracle's restatement:
+    the reference arm of bench.py times the workload it reports."""
+    import sys
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent))
+    from helpers import oracle_synthetic_run, rel_l2
+    n, members, steps = 32, 3, 20
+    ref, _ = oracle_synthetic_run(oracle, n, members, steps, 1e-3, 1e-3, 0.05, 42)
+    for workers in (1, 2):
+        got = reference.synthetic_ensemble(n, 1e-3, 1e-3, steps, members, workers, 42)
+        for m in range(members):
+            assert rel_l2(got[m], ref[m]) < 1e-14
+
+
 def test_taylor_green_decay_and_order(oracle):
     """verification.cpp:44-65."""
     p = params6(0.7, 0.6, 0.0, 0.5, 2, 3)

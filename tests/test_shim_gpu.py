@@ -25,3 +25,5 @@ def test_cuda_solver_shim_parity(args):
     result = json.loads(out.stdout.strip().splitlines()[-1])
     assert result["relative_l2_error"] <= 1e-12
     assert result["invalid_argument_on_missing_forcing"]
+    # a CFL violation throws before the state changes, and the instance steps on from it
+    assert result["cfl_throws"] and result["cfl_state_unchanged"] and result["cfl_steps_on"]

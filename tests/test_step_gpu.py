@@ -56,6 +56,81 @@ def test_config0_fp64_1000_steps(hzlb, oracle):
     np.testing.assert_allclose(np.array(got_series), series[99::100], rtol=1e-12)
 
 
+# Config 1 (256 members at 128^2, nu = dt = 5e-4, 2000 steps): the FP32-against-FP64 maxima
+# over the 256 members after 2000 steps measured 1.67e-6 (relative L2) and 1.31e-6 (enstrophy
+# drift) on a B200, growing about linearly in time; the bounds asserted here leave 3x margin.
+CONFIG1_L2_BOUND = 5e-6
+CONFIG1_ENSTROPHY_BOUND = 5e-6
+
+
+def _config1(hzlb, precision, members=256):
+    e = device_synthetic(hzlb, 128, members, precision, 5e-4, 0.05, 42)
+    return e
+
+
+def test_config1_fp64_2000_steps_against_reference(hzlb, reference):
+    """The FP64 path over config 1's 2000 steps equals the reference's own CPU Solver driven
+    with the same forcing, noise and initial fields (its update_latent_state + step) within
+    1e-12 relative L2, for the first four members of the 256-member ensemble."""
+    n, steps, dt, nu = 128, 2000, 5e-4, 5e-4
+    e = _config1(hzlb, 8)
+    e.step(dt, steps)
+    assert e.status() == 0
+    got = e.get_state()
+    e.close()
+    ref = reference.synthetic_ensemble(n, nu, dt, steps, 4, 4, 42)
+    for m in range(4):
+        assert rel_l2(got[m], ref[m]) <= FP64_TOL, (m, rel_l2(got[m], ref[m]))
+
+
+def test_config1_fp32_error_statement(hzlb):
+    """Config 1 in FP32 against the same run in FP64 (identical fields and Philox noise): every
+    member's relative L2 error and enstrophy drift after 2000 steps stay within the stated
+    bounds, and both grow with time (no step leaves a jump)."""
+    steps, every, dt = 2000, 500, 5e-4
+    a, b = _config1(hzlb, 4), _config1(hzlb, 8)
+    K = (128 - 1) // 3
+    w = np.full(b.compact_size, 2.0)
+    w[:2 * K + 1] = 1.0
+    worst = []
+    for _ in range(steps // every):
+        a.step(dt, every)
+        b.step(dt, every)
+        x = a.get_state_compact().astype(np.complex128)
+        y = b.get_state_compact()
+        zx, zy = (w * np.abs(x) ** 2).sum(axis=1), (w * np.abs(y) ** 2).sum(axis=1)
+        err = np.sqrt((w * np.abs(x - y) ** 2).sum(axis=1) / zy)
+        worst.append((err.max(), np.abs(zx / zy - 1).max()))
+    assert a.status() == 0 and b.status() == 0
+    a.close()
+    b.close()
+    print("config1 FP32 vs FP64 (max rel L2, max enstrophy drift) per 500 steps:", worst)
+    assert worst[-1][0] < CONFIG1_L2_BOUND
+    assert worst[-1][1] < CONFIG1_ENSTROPHY_BOUND
+    assert worst[-1][0] >= worst[0][0] * 0.5
+
+
+@pytest.mark.parametrize("precision", [4, 8])
+def test_checked_step_leaves_state_on_cfl_violation(hzlb, precision):
+    """hzlb_step_checked: a step whose stage-1 velocities break the CFL limit is undone
+    (state, clock, noise counter), and the next step equals a fresh ensemble's."""
+    n, members, seed = 64, 3, 5
+    a = device_synthetic(hzlb, n, members, precision, 1e-3, 0.05, seed)
+    b = device_synthetic(hzlb, n, members, precision, 1e-3, 0.05, seed)
+    before = a.get_state_compact()
+    rate = a.diagnostics()[:, 5].max()
+    with pytest.raises(hzlb.HzlbError) as err:
+        a.step_checked(0.75 / rate)
+    assert err.value.code == hzlb.HZLB_ERUNTIME and "CFL" in str(err.value)
+    np.testing.assert_array_equal(a.get_state_compact(), before)
+    assert a.status() == 0
+    a.step_checked(0.1 / rate)
+    b.step(0.1 / rate, 1)
+    np.testing.assert_array_equal(a.get_state_compact(), b.get_state_compact())
+    a.close()
+    b.close()
+
+
 def test_fp32_error_against_fp64_oracle(hzlb, oracle):
     """FP32 path (complex64 spectra): stated error bound against the FP64 oracle."""
     n, members, steps, dt, nu, sigma, seed = 128, 2, 100, 5e-4, 5e-4, 0.05, 11

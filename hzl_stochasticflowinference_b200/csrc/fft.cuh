@@ -91,7 +91,7 @@ template <int N, int E, int NS> struct PassTw {
     }
     static constexpr int total = own + rest();                     // this and later passes
 };
-template <int N, int E> constexpr int pass_twiddle_entries() { return PassTw<N, E, 1>::total; }
+template <int N, int E> __host__ __device__ constexpr int pass_twiddle_entries() { return PassTw<N, E, 1>::total; }
 
 // Fills the per-pass table (cooperatively, all threads of the block) from the base table
 // base[k] = W_N^k = exp(-2 pi i k / N).
@@ -109,10 +109,11 @@ __device__ __forceinline__ void load_pass_twiddles(cx<R> *dst, const cx<R> *base
         load_pass_twiddles<N, E, R, NS * P::RAD>(dst + P::own, base);
 }
 
-// One Stockham pass with stride NS; recursion over the remaining passes.  `tw` points at this
-// pass's entries of the per-pass twiddle table.
-template <int N, int E, int SIGN, typename R, int NS>
-__device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *tw, int t) {
+// One Stockham pass with stride NS; recursion over the remaining passes.  tw(i) returns
+// entry i of this thread's between-pass twiddles: passes after the first in order, within a
+// pass [q][r-1] (the per-pass table's entry i*T + t, or a register copy of it).
+template <int N, int E, int SIGN, typename R, int NS, int TI, class Tw>
+__device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const Tw &tw, int t) {
     constexpr int T = N / E;
     using P = PassTw<N, E, NS>;
     constexpr int RAD = P::RAD;
@@ -129,7 +130,7 @@ __device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *
         if constexpr (NS > 1) {
 #pragma unroll
             for (int r = 1; r < RAD; ++r) {
-                cx<R> w = tw[(q * (RAD - 1) + (r - 1)) * T + t];
+                cx<R> w = tw(TI + q * (RAD - 1) + (r - 1));
                 if constexpr (SIGN > 0)
                     w.y = -w.y;
                 u[r] = cmul(u[r], w);
@@ -153,8 +154,22 @@ __device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *
         for (int r = 0; r < E; ++r)
             v[r] = sm[pad<E>(t + r * T)];
         __syncwarp();
-        fft_pass<N, E, SIGN, R, NS * RAD>(v, sm, tw + P::own, t);
+        fft_pass<N, E, SIGN, R, NS * RAD, TI + P::own / T>(v, sm, tw, t);
     }
+}
+
+// Between-pass twiddles held per thread (a line position t keeps the same entries in every
+// transform): registers in place of shared-memory loads.
+template <int N, int E> __host__ __device__ constexpr int thread_twiddles() {
+    return pass_twiddle_entries<N, E>() / (N / E) > 0 ? pass_twiddle_entries<N, E>() / (N / E) : 1;
+}
+template <int N, int E, typename R>
+__device__ __forceinline__ void load_thread_twiddles(cx<R> (&twr)[thread_twiddles<N, E>()],
+                                                     const cx<R> *tw, int t) {
+    constexpr int T = N / E;
+#pragma unroll
+    for (int i = 0; i < thread_twiddles<N, E>(); ++i)
+        twr[i] = i * T < pass_twiddle_entries<N, E>() ? tw[i * T + t] : mk<R>(1, 0);
 }
 
 // Unnormalised DFT of one line: X[k] = sum_n x[n] exp(SIGN 2 pi i n k / N).
@@ -164,7 +179,16 @@ __device__ __forceinline__ void fft_pass(cx<R> (&v)[E], cx<R> *sm, const cx<R> *
 template <int N, int E, int SIGN, typename R>
 __device__ __forceinline__ void fft_line(cx<R> (&v)[E], cx<R> *sm, const cx<R> *tw, int t) {
     (void)FftShape<N, E>::T;
-    fft_pass<N, E, SIGN, R, 1>(v, sm, tw, t);
+    constexpr int T = N / E;
+    const auto get = [&](int i) { return tw[i * T + t]; };
+    fft_pass<N, E, SIGN, R, 1, 0>(v, sm, get, t);
+}
+// The same with this thread's twiddles in registers (load_thread_twiddles).
+template <int N, int E, int SIGN, typename R>
+__device__ __forceinline__ void fft_line_rt(cx<R> (&v)[E], cx<R> *sm,
+                                            const cx<R> (&twr)[thread_twiddles<N, E>()], int t) {
+    const auto get = [&](int i) { return twr[i]; };
+    fft_pass<N, E, SIGN, R, 1, 0>(v, sm, get, t);
 }
 
 } // namespace hzlb

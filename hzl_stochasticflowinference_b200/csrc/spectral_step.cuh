@@ -181,6 +181,17 @@ __device__ __forceinline__ bool block_wait(uint64_t *bar, uint32_t parity, volat
     return ok;
 }
 
+// A line transform with the between-pass twiddles in registers (FP32) or read from the
+// shared per-pass table (FP64, whose registers the data needs).
+template <int N, int E, int SIGN, typename R>
+__device__ __forceinline__ void transform_line(cx<R> (&x)[E], cx<R> *xsm, const cx<R> *tw,
+                                               const cx<R> (&twr)[thread_twiddles<N, E>()], int t) {
+    if constexpr (sizeof(R) == 4)
+        fft_line_rt<N, E, SIGN, R>(x, xsm, twr, t);
+    else
+        fft_line<N, E, SIGN, R>(x, xsm, tw, t);
+}
+
 // S is the RK stage (0: velocity of the initial state only, 1..3 intermediate, 4 final), a
 // compile-time constant so that each stage's epilogue is straight-line code.
 template <typename R, int N, int S>
@@ -271,6 +282,12 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     };
 
     const int line = threadIdx.x / T, t = threadIdx.x % T;
+    // FP32: this thread's between-pass twiddles in registers for every transform it does
+    // (FP64 keeps reading the shared table: its registers are spent on the data)
+    constexpr bool reg_tw = sizeof(R) == 4;
+    cx<R> twr[thread_twiddles<N, E>()];
+    if constexpr (reg_tw)
+        load_thread_twiddles<N, E, R>(twr, tw, t);
     if (threadIdx.x < 32 && forward && static_cast<int>(blockIdx.x) < items)
         issue_nl(blockIdx.x);
     bool timed_out = false;
@@ -320,7 +337,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                 for (int r = 0; r < E; ++r)
                     v[r] = src[t + r * T];
                 __syncwarp();   // the line's lanes have read the column it exchanges in
-                fft_line<N, E, -1, R>(v, src, tw, t);
+                transform_line<N, E, -1, R>(v, src, tw, twr, t);
                 if (f == 0) {
                     static_for<0, E>([&](auto rc) {
                         constexpr int r = decltype(rc)::value;
@@ -451,7 +468,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
                     const cx<R> psi = y[r];
                     v[r] = f == 0 ? mk<R>(-kyr * psi.y, kyr * psi.x) : mk<R>(kxr * psi.y, -kxr * psi.x);
                 });
-                fft_line<N, E, +1, R>(v, xb, tw, t);
+                transform_line<N, E, +1, R>(v, xb, tw, twr, t);
                 if (f == 1)
                     __syncthreads();   // field 0 is out of the staging rows
 #pragma unroll
@@ -573,6 +590,11 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         issue(blockIdx.x);
 
     const int g = threadIdx.x / T, t = threadIdx.x % T;
+    // FP32: this thread's between-pass twiddles in registers (see column_kernel)
+    constexpr bool reg_tw = sizeof(R) == 4;
+    cx<R> twr[thread_twiddles<N, E>()];
+    if constexpr (reg_tw)
+        load_thread_twiddles<N, E, R>(twr, tw, t);
     const bool active = g < TY;
     const int ty = active ? g : 0;
     cx<R> *sm = lines + g * G::BUF;
@@ -592,7 +614,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         __syncthreads();
         if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items)
             issue(it + gridDim.x);
-        fft_line<N, E, +1, R>(z, sm, tw, t);
+        transform_line<N, E, +1, R>(z, sm, tw, twr, t);
         R vmax = 0;
 #pragma unroll
         for (int r = 0; r < E; ++r) {
@@ -607,7 +629,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
             if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
                 atomicOr(&a.ctl->status, STATUS_CFL);
         }
-        fft_line<N, E, -1, R>(z, sm, tw, t);
+        transform_line<N, E, -1, R>(z, sm, tw, twr, t);
         // separate P^ and Q^ at kx = p from z(p) and conj z(N - p); only the partners of
         // retained kx are stored
         static_for<0, E>([&](auto rc) {

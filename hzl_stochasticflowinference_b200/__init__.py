@@ -130,6 +130,7 @@ def library() -> C.CDLL:
         "hzlb_set_forcing": (C.c_int, [vp, _dp, C.c_int, C.c_int]),
         "hzlb_step": (C.c_int, [vp, C.c_double, C.c_uint64]),
         "hzlb_step_checked": (C.c_int, [vp, C.c_double]),
+        "hzlb_test_inject_wait_timeout": (C.c_int, [vp]),
         "hzlb_step_host": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, C.c_int]),
         "hzlb_status": (C.c_int, [vp, _u32p]),
         "hzlb_synchronize": (C.c_int, [vp]),
@@ -404,6 +405,12 @@ class Ensemble:
     # -- stepping ---------------------------------------------------------------------
     def step(self, dt: float, steps: int = 1):
         _check(self._lib.hzlb_step(self._h, dt, steps))
+
+    def inject_wait_timeout(self):
+        """Test hook (hzlb_test_inject_wait_timeout): the next step's row pass leaves one
+        block's first tile copy unissued, its bounded wait runs out and the step reports
+        STATUS_TIMEOUT."""
+        _check(self._lib.hzlb_test_inject_wait_timeout(self._h))
 
     def step_checked(self, dt: float):
         """One step that is undone when its stage-1 CFL check fails (hzlb_step_checked);

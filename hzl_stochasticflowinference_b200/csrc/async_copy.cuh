@@ -63,12 +63,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
                  : "memory");
     return done != 0;
 }
-// Waits for the phase with the given parity to complete, at most `limit` polls.
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits for the phase with the given parity to complete; gives up (false) after `limit_ns`
+// nanoseconds of the global timer (one second by default), or at the latest after 2^26 polls,
+// so a phase that never completes costs about a second, never a hang.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
-                                                  uint32_t limit = 1u << 24) {
-    for (uint32_t i = 0; i < limit; ++i)
+                                                  uint64_t limit_ns = 1000000000ull) {
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const uint64_t start = global_ns();
+    for (uint32_t i = 0; i < (1u << 26); ++i) {
         if (mbar_try_wait(bar, parity))
             return true;
+        if ((i & 63) == 63 && global_ns() - start > limit_ns)
+            return false;
+    }
     return false;
 }
 

@@ -94,6 +94,9 @@ int hzlb_set_forcing(hzlb_ensemble *h, const double *spectra, int first, int cou
 int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps) {
     return guarded([&] { engine(h).step(dt, nsteps); });
 }
+int hzlb_test_inject_wait_timeout(hzlb_ensemble *h) {
+    return guarded([&] { engine(h).inject_wait_timeout(); });
+}
 int hzlb_step_checked(hzlb_ensemble *h, double dt) {
     return guarded([&] { engine(h).step_checked(dt); });
 }

@@ -570,7 +570,7 @@ template <typename R> class EngineT final : public Engine {
         chunk_ctl_.ensure(sizeof(StepControl) * chunks, "allocate chunk control");
         std::vector<StepControl> init(chunks);
         for (auto &c : init)
-            c = StepControl{step_index, 0u, 0u};
+            c = StepControl{step_index, 0u, 0u, 0u};
         cuda_check(cudaMemcpyAsync(chunk_ctl_.ptr, init.data(), sizeof(StepControl) * chunks,
                                    cudaMemcpyHostToDevice, stream_),
                    "initialise chunk control");
@@ -692,6 +692,14 @@ template <typename R> class EngineT final : public Engine {
                                    stream_),
                    "set step counter");
         cuda_check(cudaStreamSynchronize(stream_), "set step counter");
+    }
+    void inject_wait_timeout() override {
+        const unsigned one = 1;
+        cuda_check(cudaMemcpyAsync(&ctl_.as<StepControl>()->inject, &one, sizeof one,
+                                   cudaMemcpyHostToDevice, stream_),
+                   "arm wait-timeout test hook");
+        cuda_check(cudaStreamSynchronize(stream_), "arm wait-timeout test hook");
+        w_valid_ = false;
     }
     uint32_t status() override {
         StepControl c{};

@@ -96,6 +96,9 @@ class Engine {
     // out in member chunks that overlap copies with stepping
     virtual void step_host(const void *in, void *out, double dt, uint64_t nsteps, int chunk) = 0;
     virtual uint32_t status() = 0;
+    // test hook: the next row pass leaves one block's first tile copy unissued (its bounded
+    // wait runs out and the step reports STATUS_TIMEOUT)
+    virtual void inject_wait_timeout() = 0;
     virtual void synchronize() = 0;
     virtual void diagnostics(double *out) = 0;
     virtual void physical(double *out) = 0;

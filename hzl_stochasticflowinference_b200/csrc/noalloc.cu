@@ -52,6 +52,7 @@ __global__ void noalloc_init(StepControl *ctl, unsigned long long first_step) {
     ctl->step = first_step;
     ctl->arrivals = 0;
     ctl->status = 0;
+    ctl->inject = 0;
 }
 
 size_t align256(size_t b) { return (b + 255) / 256 * 256; }

@@ -94,6 +94,8 @@ struct StepControl {
     unsigned long long step;   // index of the step being taken (noise counter)
     unsigned int arrivals;     // column-kernel block arrivals on the final stage
     unsigned int status;       // STATUS_* bits
+    unsigned int inject;       // test hook (hzlb_test_inject_wait_timeout): nonzero makes the
+                               // next row pass leave block 0's first tile copy unissued
 };
 
 template <typename R> struct ColumnArgs {
@@ -556,8 +558,11 @@ template <int N, int E> struct LowSlots {
     static constexpr int value = K / T + 1 < E ? K / T + 1 : E;
 };
 
+// FP32: at most 80 registers, so that 6 blocks fit an SM (95 unconstrained: 5 blocks; measured
+// 0.368 against 0.383 ms per launch at 2048 members, 256^2).
 template <typename R, int N>
-__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowArgs<R> a, int items) {
+__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1)
+    row_kernel(const RowArgs<R> a, int items) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -586,8 +591,14 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
         mbar_arrive_expect(&bar, tile_bytes);
         bulk_copy_g2s(tile, a.w + (static_cast<size_t>(m) * N + y0) * 2 * G::CW, tile_bytes, &bar);
     };
-    if (threadIdx.x == 0 && static_cast<int>(blockIdx.x) < items)
-        issue(blockIdx.x);
+    if (threadIdx.x == 0 && static_cast<int>(blockIdx.x) < items) {
+        // test hook: a pending injection (consumed here) leaves this block's first copy
+        // unissued, so its bounded wait below runs out with no copy in flight
+        const bool skip = blockIdx.x == 0 && *static_cast<volatile unsigned *>(&a.ctl->inject) != 0 &&
+                          atomicExch(&a.ctl->inject, 0u) != 0;
+        if (!skip)
+            issue(blockIdx.x);
+    }
 
     const int g = threadIdx.x / T, t = threadIdx.x % T;
     // FP32: this thread's between-pass twiddles in registers (see column_kernel)
@@ -630,19 +641,21 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS) row_kernel(const RowAr
                 atomicOr(&a.ctl->status, STATUS_CFL);
         }
         transform_line<N, E, -1, R>(z, sm, tw, twr, t);
-        // separate P^ and Q^ at kx = p from z(p) and conj z(N - p); only the partners of
-        // retained kx are stored
-        static_for<0, E>([&](auto rc) {
-            constexpr int r = decltype(rc)::value;
-            if constexpr (!Band<N, T, r>::zero)
-                sm[pad<E>(t + r * T)] = z[r];
-        });
-        __syncwarp();
+        // separate P^ and Q^ at kx = p from z(p) and conj z(N - p).  Position N - p of this
+        // row is held by lane T - t at register E - 1 - r (t > 0), or by this lane at register
+        // (E - r) mod E (t = 0): two shuffles per value, no trip through shared memory
+        const int lane = threadIdx.x & 31;
+        const int src = (lane & ~(T - 1)) + ((T - t) & (T - 1));
         cx<R> ph[RL], qh[RL];
         static_for<0, RL>([&](auto rc) {
             constexpr int r = decltype(rc)::value;
-            const int p = t + r * T;
-            const cx<R> zk = z[r], zc = conj(sm[pad<E>((N - p) & (N - 1))]);
+            constexpr int rs = E - 1 - r, r0 = (E - r) & (E - 1);
+            cx<R> zp;
+            zp.x = __shfl_sync(0xffffffffu, z[rs].x, src);
+            zp.y = __shfl_sync(0xffffffffu, z[rs].y, src);
+            if (t == 0)
+                zp = z[r0];
+            const cx<R> zk = z[r], zc = conj(zp);
             const cx<R> sa = zk + zc, sb = zk - zc;
             ph[r] = mk<R>(sa.x / 2, sa.y / 2);
             qh[r] = mk<R>(sb.y / 2, -sb.x / 2);

@@ -143,6 +143,12 @@ HZLB_API int hzlb_step_host(hzlb_ensemble *h, const void *state_in, void *state_
                             uint64_t nsteps, int chunk_members);
 /* Waits for the handle's stream; returns the accumulated status bits and clears them. */
 HZLB_API int hzlb_status(hzlb_ensemble *h, uint32_t *status);
+/* Test hook, no counterpart in the reference: the next row pass of h leaves the first tile
+ * copy of one block unissued, so that block's bounded wait (one second of the device's global
+ * timer) runs out with no copy in flight; the block records HZLB_STATUS_TIMEOUT and returns,
+ * the step's result is not valid, and the context stays usable.  Tests the failure path of
+ * the device waits without faulting or hanging the GPU. */
+HZLB_API int hzlb_test_inject_wait_timeout(hzlb_ensemble *h);
 HZLB_API int hzlb_synchronize(hzlb_ensemble *h);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work or
  * record events against the library's kernels. */

@@ -131,6 +131,34 @@ def test_checked_step_leaves_state_on_cfl_violation(hzlb, precision):
     b.close()
 
 
+@pytest.mark.parametrize("precision", [4, 8])
+def test_bounded_wait_runs_out_and_the_context_stays_usable(hzlb, precision):
+    """Failure detection without a GPU fault: the test hook leaves one block's first tile copy
+    unissued, so its mbarrier never completes with nothing in flight; the bounded wait gives up
+    after about a second, the step reports STATUS_TIMEOUT, and the same context then steps
+    exactly as a fresh ensemble does."""
+    import time
+    n, members, seed, dt = 64, 8, 3, 1e-3
+    a = device_synthetic(hzlb, n, members, precision, 1e-3, 0.05, seed)
+    a.inject_wait_timeout()
+    t0 = time.perf_counter()
+    a.step(dt, 1)
+    status = a.status()
+    assert status & hzlb.STATUS_TIMEOUT, status
+    assert time.perf_counter() - t0 < 30
+    assert a.status() == 0   # read and cleared
+    # the ensemble that timed out, restarted, and a fresh one agree bit for bit
+    a.set_state(np.array([hzlb.grf_spectrum(n, seed, m) for m in range(members)]))
+    a.set_time(0.0, 0)
+    b = device_synthetic(hzlb, n, members, precision, 1e-3, 0.05, seed)
+    a.step(dt, 3)
+    b.step(dt, 3)
+    assert a.status() == 0 and b.status() == 0
+    np.testing.assert_array_equal(a.get_state_compact(), b.get_state_compact())
+    a.close()
+    b.close()
+
+
 def test_fp32_error_against_fp64_oracle(hzlb, oracle):
     """FP32 path (complex64 spectra): stated error bound against the FP64 oracle."""
     n, members, steps, dt, nu, sigma, seed = 128, 2, 100, 5e-4, 5e-4, 0.05, 11

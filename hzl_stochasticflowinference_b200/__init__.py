@@ -148,6 +148,10 @@ def library() -> C.CDLL:
                                          C.POINTER(C.c_uint8), C.POINTER(hzlb_pf_record), _u32p,
                                          _dp]),
         "hzlb_pf_get_weights": (C.c_int, [vp, _dp]),
+        "hzlb_enkf_weights": (C.c_int, [vp, vp, _dp, _dp, vp, C.c_int, C.c_size_t, vp, _dp]),
+        "hzlb_dgemm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, vp, C.c_longlong,
+                                 C.c_longlong, vp, C.c_longlong, C.c_longlong, C.c_double, vp,
+                                 C.c_longlong, vp]),
         "hzlb_systematic_resample": (C.c_int, [vp, _dp, C.c_size_t, C.c_double, _u32p]),
         "hzlb_gather_members": (C.c_int, [vp, _u32p]),
         "hzlb_inflate": (C.c_int, [vp, C.c_double]),
@@ -551,6 +555,23 @@ class Ensemble:
                                                 nis_limit, C.byref(nis), C.byref(applied)))
         return nis.value, bool(applied.value)
 
+    def enkf_weights(self, hx, values, sd, eps):
+        """Ensemble-space EnKF weights of gathered predicted observations (hzlb_enkf_weights):
+        hx, eps CUDA float64 tensors (members, p); returns (W as a CUDA float64 tensor
+        (members, members), innovation statistic)."""
+        import torch
+        hx = hx.contiguous().to(torch.float64)
+        eps = eps.contiguous().to(torch.float64)
+        members, p = hx.shape
+        w = torch.empty((members, members), dtype=torch.float64, device=hx.device)
+        v, s = _f64(values), _f64(sd)
+        nis = C.c_double()
+        torch.cuda.current_stream(hx.device).synchronize()   # hx and eps are written
+        _check(self._lib.hzlb_enkf_weights(self._h, C.c_void_p(hx.data_ptr()), _p(v), _p(s),
+                                           C.c_void_p(eps.data_ptr()), members, p,
+                                           C.c_void_p(w.data_ptr()), C.byref(nis)))
+        return w, nis.value
+
     def learned_forecast(self, pod: "Pod", mlp: "Mlp", dt: float, steps: int,
                          mean_increment=None) -> None:
         """One window of the learned reduced forecast (hzlb_learned_forecast);
@@ -597,6 +618,26 @@ class Ensemble:
         ptr = C.c_void_p()
         _check(self._lib.hzlb_state_device(self._h, C.byref(ptr)))
         return ptr.value
+
+
+def dgemm(a, b, c, alpha: float = 1.0, beta: float = 0.0, a_trans: bool = False,
+          b_trans: bool = False) -> None:
+    """c = alpha op(a) op(b) + beta c on the FP64 tensor cores (hzlb_dgemm), for contiguous
+    CUDA float64 matrices; op(x) = x.T when the flag is set.  Runs on torch's current stream."""
+    import torch
+    for t in (a, b, c):
+        if t.dtype != torch.float64 or not t.is_cuda or not t.is_contiguous() or t.dim() != 2:
+            raise HzlbInvalidArgument(HZLB_EINVAL, "dgemm takes contiguous CUDA float64 matrices")
+    m, k = (a.shape[1], a.shape[0]) if a_trans else (a.shape[0], a.shape[1])
+    kb, n = (b.shape[1], b.shape[0]) if b_trans else (b.shape[0], b.shape[1])
+    if kb != k or tuple(c.shape) != (m, n):
+        raise HzlbInvalidArgument(HZLB_EINVAL, "dgemm shape mismatch")
+    sam, sak = (1, a.shape[1]) if a_trans else (a.shape[1], 1)
+    sbk, sbn = (1, b.shape[1]) if b_trans else (b.shape[1], 1)
+    stream = torch.cuda.current_stream(c.device).cuda_stream
+    _check(library().hzlb_dgemm(m, n, k, alpha, C.c_void_p(a.data_ptr()), sam, sak,
+                                C.c_void_p(b.data_ptr()), sbk, sbn, beta, C.c_void_p(c.data_ptr()),
+                                n, C.c_void_p(stream)))
 
 
 def grf_spectrum(n: int, seed: int, member: int) -> np.ndarray:

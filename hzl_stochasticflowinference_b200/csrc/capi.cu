@@ -1,5 +1,6 @@
 // extern "C" boundary (include/hzlb.h): exception -> status code mapping around the engine.
 #include "engine.h"
+#include "dense64.cuh"
 
 #include <cmath>
 #include <exception>
@@ -262,6 +263,42 @@ int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const uint32_t *
             *nis = r.nis;
         if (applied)
             *applied = r.applied;
+    });
+}
+int hzlb_enkf_weights(hzlb_ensemble *h, const double *hx, const double *values, const double *sd,
+                      const double *eps, int members, size_t p, double *W, double *nis) {
+    return guarded([&] {
+        need(hx, "hx");
+        need(values, "values");
+        need(sd, "sd");
+        need(eps, "eps");
+        need(W, "W");
+        if (members < 2 || members > (1 << 16))
+            hzlb::raise(HZLB_EINVAL, "EnKF weights need between 2 and 65536 members");
+        const double v = engine(h).enkf_weights(hx, values, sd, eps, members, p, W);
+        if (nis)
+            *nis = v;
+    });
+}
+int hzlb_dgemm(int M, int N, int K, double alpha, const double *A, long long sam, long long sak,
+               const double *B, long long sbk, long long sbn, double beta, double *C, long long ldc,
+               void *stream) {
+    return guarded([&] {
+        if (M < 0 || N < 0 || K < 0)
+            hzlb::raise(HZLB_EINVAL, "GEMM sizes must be nonnegative");
+        if (M > 0 && N > 0) {
+            need(C, "C");
+            if (K > 0) {
+                need(A, "A");
+                need(B, "B");
+            }
+            if (ldc < N)
+                hzlb::raise(HZLB_EINVAL, "ldc must be at least N");
+        }
+        hzlb::cuda_check(hzlb::d64::gemm(hzlb::d64::GemmArgs{M, N, K, alpha, beta, A, sam, sak, B,
+                                                             sbk, sbn, C, ldc},
+                                         static_cast<cudaStream_t>(stream)),
+                         "launch FP64 GEMM");
     });
 }
 int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,

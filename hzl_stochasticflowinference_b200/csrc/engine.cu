@@ -1071,49 +1071,59 @@ template <typename R> class EngineT final : public Engine {
         w_valid_ = false;
         return omega_.ptr;
     }
-    EnkfResult enkf(const EnkfRequest &q) override {
-        if (M_ < 2)
+    // The FP64 ensemble-space solve of the perturbed-observation analysis for M members whose
+    // predicted observations hx (device, M x p, row m = member) are given: innovations and
+    // anomalies, S = HA^T HA/(M-1) + R, its Cholesky, the forward substitution of [HA; D; dbar],
+    // the innovation statistic and -- unless nis_limit > 0 and the statistic exceeds it --
+    // W = (L^-1 HA)^T-rows (L^-1 D)-rows / (M-1) (M x M, rows: contributing member) in the
+    // workspace, *W_dev pointing at it.  eps: M x p standard normals on the host
+    // (eps_on_device false), on the device (true), or null for the Philox draws keyed by
+    // (seed, member_base + m) with counter `cycle`.
+    EnkfResult solve_weights(const double *hx, int M, size_t p, const double *values,
+                             const double *sd, const double *eps, bool eps_on_device,
+                             uint64_t seed, uint64_t cycle, uint32_t member_base,
+                             double nis_limit, double **W_dev) {
+        if (M < 2)
             raise(HZLB_EINVAL, "EnKF requires at least two ensemble members");
-        const size_t p = q.p;
-        if (p == 0)
-            return EnkfResult{0.0, 0};
         for (size_t o = 0; o < p; ++o)
-            if (!std::isfinite(q.values[o]) || !std::isfinite(q.sd[o]) || q.sd[o] <= 0)
+            if (!std::isfinite(values[o]) || !std::isfinite(sd[o]) || sd[o] <= 0)
                 raise(HZLB_EINVAL, "observations must be finite and have positive uncertainty");
         if (p > (1u << 20))
             raise(HZLB_EINVAL, "too many observations for one analysis");
-        observe_device(q.x, q.y, p);
         const int pi = static_cast<int>(p);
-        const size_t mp = static_cast<size_t>(M_) * p, m1p = mp + p;
+        const size_t mp = static_cast<size_t>(M) * p, m1p = mp + p;
         const size_t nblk = (p + d64::NB - 1) / d64::NB;
-        const size_t eps_n = q.perturbations ? mp : 0;
+        const size_t eps_n = (eps && !eps_on_device) ? mp : 0;
         // ha (M rows) and d (M + 1 rows) are adjacent: one forward substitution covers both
         const size_t doubles = 3 * p + eps_n + mp + m1p + (mp + m1p) + p * p +
-                               nblk * d64::NB * d64::NB + static_cast<size_t>(M_) * M_ + 1;
+                               nblk * d64::NB * d64::NB + static_cast<size_t>(M) * M + 1;
         enkf_.ensure(sizeof(double) * doubles + 64, "allocate EnKF workspace");
         double *ybuf = enkf_.as<double>(), *sdbuf = ybuf + p, *hmean = sdbuf + p,
                *eps_d = hmean + p, *ha = eps_d + eps_n, *d = ha + mp, *yw = d + m1p,
                *P = yw + mp + m1p, *inv = P + p * p, *W = inv + nblk * d64::NB * d64::NB,
-               *nis_d = W + static_cast<size_t>(M_) * M_;
+               *nis_d = W + static_cast<size_t>(M) * M;
         int *info = reinterpret_cast<int *>(nis_d + 1);
-        cuda_check(cudaMemcpyAsync(ybuf, q.values, sizeof(double) * p, cudaMemcpyHostToDevice,
+        cuda_check(cudaMemcpyAsync(ybuf, values, sizeof(double) * p, cudaMemcpyHostToDevice,
                                    stream_),
                    "upload observations");
-        cuda_check(cudaMemcpyAsync(sdbuf, q.sd, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
+        cuda_check(cudaMemcpyAsync(sdbuf, sd, sizeof(double) * p, cudaMemcpyHostToDevice, stream_),
                    "upload observation errors");
-        if (q.perturbations)
-            cuda_check(cudaMemcpyAsync(eps_d, q.perturbations, sizeof(double) * mp,
-                                       cudaMemcpyHostToDevice, stream_),
+        const double *eps_used = nullptr;
+        if (eps && !eps_on_device) {
+            cuda_check(cudaMemcpyAsync(eps_d, eps, sizeof(double) * mp, cudaMemcpyHostToDevice,
+                                       stream_),
                        "upload perturbations");
+            eps_used = eps_d;
+        } else if (eps) {
+            eps_used = eps;
+        }
         cuda_check(cudaMemsetAsync(info, 0, sizeof(int), stream_), "clear Cholesky status");
-        member_mean<double><<<(pi + 31) / 32, dim3(32, 8), 0, stream_>>>(obs_.as<double>(), pi, M_,
-                                                                       hmean);
-        enkf_innovations<<<1024, 256, 0, stream_>>>(
-            obs_.as<double>(), hmean, ybuf, sdbuf, q.perturbations ? eps_d : nullptr,
-            q.perturbation_seed, static_cast<uint32_t>(cfg_.member_base), q.cycle, M_, pi, ha, d);
+        member_mean<double><<<(pi + 31) / 32, dim3(32, 8), 0, stream_>>>(hx, pi, M, hmean);
+        enkf_innovations<<<1024, 256, 0, stream_>>>(hx, hmean, ybuf, sdbuf, eps_used, seed,
+                                                    member_base, cycle, M, pi, ha, d);
         cuda_check(cudaGetLastError(), "launch EnKF innovations");
         // S = HA^T HA / (M-1) + R (lower triangle), FP64
-        cuda_check(d64::gemm(d64::GemmArgs{pi, pi, M_, 1.0 / (M_ - 1), 0.0, ha, 1, pi, ha, pi, 1,
+        cuda_check(d64::gemm(d64::GemmArgs{pi, pi, M, 1.0 / (M - 1), 0.0, ha, 1, pi, ha, pi, 1,
                                            P, pi},
                              stream_, true),
                    "launch innovation covariance");
@@ -1122,7 +1132,7 @@ template <typename R> class EngineT final : public Engine {
         // L^{-1} applied to the anomalies HA, the M perturbed innovations and the mean
         // innovation at once (rows of [HA; D], written to yw): with S = L L^T,
         // W = (L^{-1} HA)^T-rows . (L^{-1} D)-rows / (M-1) and NIS = |L^{-1} dbar|^2 / p
-        cuda_check(d64::forward_rows(P, pi, inv, ha, yw, 2 * M_ + 1, stream_),
+        cuda_check(d64::forward_rows(P, pi, inv, ha, yw, 2 * M + 1, stream_),
                    "launch innovation solve");
         const double *yha = yw, *yd = yw + mp;
         innovation_statistic<<<1, 256, 0, stream_>>>(yd + mp, pi, nis_d);
@@ -1136,13 +1146,45 @@ template <typename R> class EngineT final : public Engine {
         cuda_check(cudaStreamSynchronize(stream_), "EnKF innovation solve");
         if (host_info != 0)
             raise(HZLB_ERUNTIME, "EnKF innovation covariance is not positive definite");
-        if (q.nis_limit > 0 && !(nis <= q.nis_limit))
+        *W_dev = W;
+        if (nis_limit > 0 && !(nis <= nis_limit))
             return EnkfResult{nis, 0};
         // W[a][m] = sum_o (L^{-1} HA)[a][o] (L^{-1} D)[m][o] / (M-1)
-        cuda_check(d64::gemm(d64::GemmArgs{M_, M_, pi, 1.0 / (M_ - 1), 0.0, yha, pi, 1, yd, 1, pi,
-                                           W, M_},
+        cuda_check(d64::gemm(d64::GemmArgs{M, M, pi, 1.0 / (M - 1), 0.0, yha, pi, 1, yd, 1, pi,
+                                           W, M},
                              stream_),
                    "launch ensemble weights");
+        return EnkfResult{nis, 1};
+    }
+    double enkf_weights(const double *hx, const double *values, const double *sd,
+                        const double *eps, int members, size_t p, double *W_out) override {
+        if (p == 0)
+            raise(HZLB_EINVAL, "EnKF weights need at least one observation");
+        double *W = nullptr;
+        const EnkfResult r = solve_weights(hx, members, p, values, sd, eps, true, 0, 0, 0, 0.0, &W);
+        cuda_check(cudaMemcpyAsync(W_out, W, sizeof(double) * members * members,
+                                   cudaMemcpyDeviceToDevice, stream_),
+                   "copy ensemble weights");
+        cuda_check(cudaStreamSynchronize(stream_), "EnKF weights");
+        return r.nis;
+    }
+    EnkfResult enkf(const EnkfRequest &q) override {
+        if (M_ < 2)
+            raise(HZLB_EINVAL, "EnKF requires at least two ensemble members");
+        const size_t p = q.p;
+        if (p == 0)
+            return EnkfResult{0.0, 0};
+        for (size_t o = 0; o < p; ++o)
+            if (!std::isfinite(q.values[o]) || !std::isfinite(q.sd[o]) || q.sd[o] <= 0)
+                raise(HZLB_EINVAL, "observations must be finite and have positive uncertainty");
+        observe_device(q.x, q.y, p);
+        double *W = nullptr;
+        const EnkfResult solved = solve_weights(
+            obs_.as<double>(), M_, p, q.values, q.sd, q.perturbations, false, q.perturbation_seed,
+            q.cycle, static_cast<uint32_t>(cfg_.member_base), q.nis_limit, &W);
+        if (!solved.applied)
+            return solved;
+        const double nis = solved.nis;
         cx<R> *mean = acc_.as<cx<R>>();   // free between steps
         member_mean<R><<<static_cast<unsigned>((2 * compact_ + 31) / 32), dim3(32, 8), 0, stream_>>>(
             reinterpret_cast<const R *>(omega_.ptr), static_cast<long long>(2 * compact_), M_,

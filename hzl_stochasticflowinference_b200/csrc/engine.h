@@ -118,6 +118,11 @@ class Engine {
     virtual void gather(const uint32_t *ancestors) = 0;
     virtual void inflate(double inflation) = 0;
     virtual EnkfResult enkf(const EnkfRequest &request) = 0;
+    // ensemble-space weights W (M x M, device out) of the perturbed-observation analysis of
+    // `members` members with predicted observations hx and perturbations eps (device,
+    // members x p); returns the innovation statistic
+    virtual double enkf_weights(const double *hx, const double *values, const double *sd,
+                                const double *eps, int members, size_t p, double *W) = 0;
     // device address of the compact state (members x compact_size complex entries); the
     // caller may modify it until its next call on this ensemble
     virtual void *state_device() = 0;

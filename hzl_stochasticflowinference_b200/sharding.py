@@ -15,8 +15,12 @@ src/inference.cpp:555-590).  Exchanges happen only in the analysis:
   X_a[:, mine] = X[:, mine] + sum_r A_r W[rows of r, mine] is one reduce-scatter of the
   per-rank partial products A_r W[rows of r, :].
 
-The functions take torch tensors (CUDA tensors over NCCL in production, CPU tensors over gloo
-in the tests) and an optional process group.
+The arithmetic of both runs on the rank's GPU through the library (`DeviceAnalysis`: the
+particle weights and resampling in FP64, the FP64 Cholesky and solve of the innovation system,
+the FP64 anomaly products on the tensor cores); this module only moves data between ranks.
+The collective functions take torch tensors (CUDA tensors over NCCL) and an analysis object
+with the methods of `DeviceAnalysis`, which tests may replace to check the communication
+logic on CPU ranks over gloo.
 """
 from __future__ import annotations
 
@@ -78,46 +82,47 @@ def _gather_concat(local: torch.Tensor, group=None) -> torch.Tensor:
     return torch.cat([p[: int(s.item())] for p, s in zip(parts, all_sizes)], dim=0)
 
 
-def pf_weights(log_weights: np.ndarray):
-    """Normalised weights, log-likelihood increment, ESS and max weight in the reference's
-    order of operations (filter.cpp:76-92)."""
-    logs = np.asarray(log_weights, dtype=np.float64)
-    maximum = logs[0]
-    for v in logs[1:]:
-        if maximum < v:
-            maximum = v
-    total = 0.0
-    for v in logs:
-        total += np.exp(v - maximum)
-    increment = maximum + np.log(total)
-    w = np.exp(logs - increment)
-    squared = 0.0
-    for x in w:
-        squared += x * x
-    return w, increment, 1 / squared, float(w.max())
+class DeviceAnalysis:
+    """The analysis arithmetic of a sharded filter on this rank's GPU, through the library:
+    particle weights and systematic resampling (hzlb_pf_weights, hzlb_systematic_resample:
+    FP64 in the reference's order), the ensemble-space EnKF solve of the gathered predicted
+    observations (hzlb_enkf_weights: FP64 Cholesky and forward substitution) and the anomaly
+    products (hzlb_dgemm, FP64 tensor cores).  `ensemble` is this rank's handle; the solves run
+    on its device and stream."""
+
+    def __init__(self, ensemble):
+        from . import dgemm
+        self.ensemble = ensemble
+        self._dgemm = dgemm
+
+    def pf_weights(self, logs: np.ndarray):
+        """(weights, increment, ess, max weight) of all M log-weights (filter.cpp:76-92)."""
+        return self.ensemble.pf_weights(logs)
+
+    def resample(self, weights: np.ndarray, u: float) -> np.ndarray:
+        """Ancestors of systematic resampling with uniform u (filter.cpp:102-112)."""
+        return self.ensemble.resample(weights, u)
+
+    def enkf_weights(self, hx: torch.Tensor, y, sd, eps: torch.Tensor) -> torch.Tensor:
+        """W (M x M, rows: contributing member) of the gathered HX and perturbations."""
+        w, _ = self.ensemble.enkf_weights(hx, y, sd, eps)
+        return w
+
+    def anomaly_products(self, anomalies: torch.Tensor, w_rows: torch.Tensor) -> torch.Tensor:
+        """w_rows^T anomalies: (total, dim) from this rank's (count, dim) anomalies and its
+        (count, total) rows of W."""
+        out = torch.empty((w_rows.shape[1], anomalies.shape[1]), dtype=torch.float64,
+                          device=anomalies.device)
+        self._dgemm(w_rows.contiguous(), anomalies.contiguous(), out, a_trans=True)
+        return out
 
 
-def systematic_resample(weights: np.ndarray, u: float) -> np.ndarray:
-    """filter.cpp:102-112, sequential cumulative sum."""
-    count = len(weights)
-    anc = np.zeros(count, np.uint32)
-    ancestor, cumulative = 0, weights[0]
-    start = u / count
-    for i in range(count):
-        position = start + i / count
-        while position > cumulative and ancestor + 1 < count:
-            ancestor += 1
-            cumulative += weights[ancestor]
-        anc[i] = ancestor
-    return anc
-
-
-def pf_resample_distributed(local_log_weights: torch.Tensor, u: float, group=None):
+def pf_resample_distributed(local_log_weights: torch.Tensor, u: float, analysis, group=None):
     """All-gathers the log-weights; returns (weights, increment, ess, max weight, ancestors),
     identical on every rank."""
     logs = _gather_concat(local_log_weights.to(torch.float64), group).cpu().numpy()
-    w, inc, ess, mw = pf_weights(logs)
-    return w, inc, ess, mw, systematic_resample(w, u)
+    w, inc, ess, mw = analysis.pf_weights(logs)
+    return w, inc, ess, mw, analysis.resample(w, u)
 
 
 def migration_plan(ancestors: np.ndarray, world: int) -> list[list[tuple[int, int, int]]]:
@@ -162,34 +167,21 @@ def exchange_members(local_states: torch.Tensor, ancestors: np.ndarray, group=No
     return out
 
 
-def enkf_weight_matrix(hx: np.ndarray, y: np.ndarray, sd: np.ndarray, eps: np.ndarray) -> np.ndarray:
-    """W = HA^T (HA HA^T/(M-1) + R)^-1 (y + sd eps - HX) / (M-1) for the perturbed-observation
-    EnKF in ensemble space (rows: contributing member, columns: updated member)."""
-    m = hx.shape[0]
-    ha = hx - hx.mean(axis=0)
-    p = ha.T @ ha / (m - 1) + np.diag(sd * sd)
-    d = (y[None, :] + sd[None, :] * eps - hx).T
-    l = np.linalg.cholesky(p)
-    z = np.linalg.solve(l.T, np.linalg.solve(l, d))
-    return ha @ z / (m - 1)
-
-
 def enkf_distributed(local_x: torch.Tensor, local_hx: torch.Tensor, y: np.ndarray,
-                     sd: np.ndarray, local_eps: torch.Tensor, group=None) -> torch.Tensor:
+                     sd: np.ndarray, local_eps: torch.Tensor, analysis, group=None) -> torch.Tensor:
     """Batched EnKF analysis of member-sharded states.  local_x: (local members, state dim)
     real; local_hx, local_eps: (local members, p).  Returns the analysed local states."""
     world, rank = dist.get_world_size(group), dist.get_rank(group)
-    hx = _gather_concat(local_hx.to(torch.float64), group).cpu().numpy()
-    eps = _gather_concat(local_eps.to(torch.float64), group).cpu().numpy()
+    hx = _gather_concat(local_hx.to(torch.float64), group)
+    eps = _gather_concat(local_eps.to(torch.float64), group)
     total = hx.shape[0]
-    w = torch.from_numpy(enkf_weight_matrix(hx, np.asarray(y), np.asarray(sd), eps)).to(
-        local_x.device, torch.float64)
+    w = analysis.enkf_weights(hx, np.asarray(y), np.asarray(sd), eps)
     first, count = shard_range(total, world, rank)
     xs = local_x.to(torch.float64)
     mean = xs.sum(dim=0, keepdim=True)
     dist.all_reduce(mean, group=group)
     mean /= total
-    partial = ((xs - mean).T @ w[first:first + count, :]).T.contiguous()   # (total, dim)
+    partial = analysis.anomaly_products(xs - mean, w[first:first + count, :])   # (total, dim)
     chunks = [partial[a:a + c] for a, c in (shard_range(total, world, r) for r in range(world))]
     mine = torch.empty((count,) + tuple(partial.shape[1:]), dtype=partial.dtype, device=partial.device)
     if world == 1:

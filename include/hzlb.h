@@ -250,6 +250,26 @@ HZLB_API int hzlb_enkf_analysis_nis(hzlb_ensemble *h, const uint32_t *x, const u
                                     const double *values, const double *sd, size_t p,
                                     const double *perturbations, uint64_t perturbation_seed,
                                     uint64_t cycle, double nis_limit, double *nis, int *applied);
+/* No counterpart entry point in the reference (it runs one process): the ensemble-space
+ * weights of the perturbed-observation EnKF (filter.cpp:265-321, batched) for `members`
+ * members whose predicted observations were gathered from several ranks,
+ *   W = HA^T (HA HA^T/(M-1) + R)^{-1} (y + sd eps - HX) / (M-1)
+ * (M x M, row-major, rows: contributing member, columns: updated member), with the FP64
+ * innovation system factorised and solved on h's device (the solve of hzlb_enkf_analysis).
+ * hx, eps: device arrays, members x p (row m = member); values, sd: host arrays of p;
+ * W: device array members x members (out); nis (may be NULL) receives dbar^T S^{-1} dbar / p.
+ * Synchronous on h's stream; the caller orders its own writes of hx and eps before the call. */
+HZLB_API int hzlb_enkf_weights(hzlb_ensemble *h, const double *hx, const double *values,
+                               const double *sd, const double *eps, int members, size_t p,
+                               double *W, double *nis);
+/* FP64 product on the device's FP64 tensor cores (the analysis's mma.sync kernel):
+ *   C[m][n] = alpha sum_k A(m,k) B(k,n) + beta C[m][n],
+ *   A(m,k) = A[m*sam + k*sak], B(k,n) = B[k*sbk + n*sbn], C row-major with leading dimension ldc.
+ * Device pointers; C must not overlap A or B.  Asynchronous on `stream` (a cudaStream_t or
+ * NULL).  No counterpart in the reference. */
+HZLB_API int hzlb_dgemm(int M, int N, int K, double alpha, const double *A, long long sam,
+                        long long sak, const double *B, long long sbk, long long sbn, double beta,
+                        double *C, long long ldc, void *stream);
 /* No counterpart in the reference.  Device address of the compact state (members x
  * hzlb_compact_size complex entries of the configured precision, member-major), for device
  * code that reads or modifies the ensemble in place (the learned reduced forecast).  Valid

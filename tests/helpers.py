@@ -49,3 +49,40 @@ def device_synthetic(hzlb, n, members, precision, nu, sigma, seed, alpha=0.0, am
     e.set_forcing(hzlb.kolmogorov_forcing(n, amplitude, wavenumber)[None])
     e.set_time(0.0, 0)
     return e
+
+
+def enkf_weight_matrix(hx: np.ndarray, y: np.ndarray, sd: np.ndarray, eps: np.ndarray) -> np.ndarray:
+    """W = HA^T (HA HA^T/(M-1) + R)^-1 (y + sd eps - HX) / (M-1), the perturbed-observation
+    EnKF in ensemble space (rows: contributing member, columns: updated member), in numpy FP64:
+    the formula the batched device analysis is checked against."""
+    m = hx.shape[0]
+    ha = hx - hx.mean(axis=0)
+    p = ha.T @ ha / (m - 1) + np.diag(sd * sd)
+    d = (y[None, :] + sd[None, :] * eps - hx).T
+    l = np.linalg.cholesky(p)
+    z = np.linalg.solve(l.T, np.linalg.solve(l, d))
+    return ha @ z / (m - 1)
+
+
+class HostAnalysis:
+    """The analysis arithmetic of the sharded filters on the host, for CPU ranks over gloo:
+    the oracle's particle weights and resampling (the reference's order) and the numpy EnKF
+    formula.  Stands in for sharding.DeviceAnalysis where no GPU is present."""
+
+    def __init__(self):
+        from oracle.oracle import Oracle
+        self.oracle = Oracle()
+
+    def pf_weights(self, logs):
+        return self.oracle.pf_weights(np.asarray(logs, np.float64))
+
+    def resample(self, weights, u):
+        return self.oracle.systematic_resample(np.asarray(weights, np.float64), u)
+
+    def enkf_weights(self, hx, y, sd, eps):
+        import torch
+        w = enkf_weight_matrix(hx.cpu().numpy(), np.asarray(y), np.asarray(sd), eps.cpu().numpy())
+        return torch.from_numpy(w).to(hx.device)
+
+    def anomaly_products(self, anomalies, w_rows):
+        return (w_rows.T @ anomalies).contiguous()

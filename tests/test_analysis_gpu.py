@@ -8,8 +8,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from helpers import device_synthetic, rel_l2
-from hzl_stochasticflowinference_b200 import sharding
+from helpers import device_synthetic, enkf_weight_matrix, rel_l2
 from oracle.oracle import params6
 
 pytestmark = pytest.mark.gpu
@@ -203,7 +202,7 @@ def test_enkf_batch_many_observations(hzlb, precision, tol, members, p):
     eps = rng.normal(size=(members, p))
     hx = e.observe(xs, ys)
     x = e.get_state_compact().astype(np.complex128)
-    W = sharding.enkf_weight_matrix(hx, vals, sd, eps)
+    W = enkf_weight_matrix(hx, vals, sd, eps)
     expect = x + ((x - x.mean(axis=0)).T @ W).T
     e.enkf_analysis(xs, ys, vals, sd, eps)
     got = e.get_state_compact().astype(np.complex128)

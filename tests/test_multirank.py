@@ -49,34 +49,49 @@ def test_mixed_resolution_balance():
         assert max(loads) <= 1.2 * (sum(loads) / world) + 512.0 ** 2
 
 
+# 64 members of 16^2 states in the compact layout (2 x 66 reals each), 20 observations
+TOTAL, DIM, P = 64, 132, 20
+
+
+def _problem():
+    rng = np.random.default_rng(5)
+    logs = rng.normal(-20, 4, TOTAL)
+    states = rng.normal(size=(TOTAL, DIM))
+    hx = rng.normal(size=(TOTAL, P))
+    eps = rng.normal(size=(TOTAL, P))
+    y, sd = rng.normal(size=P), np.full(P, 0.3)
+    return logs, states, hx, eps, y, sd
+
+
 def _worker(rank, world, port, q):
+    from helpers import HostAnalysis
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        rng = np.random.default_rng(5)
-        total, dim, p = 10, 12, 3
-        logs = rng.normal(-20, 4, total)
-        states = rng.normal(size=(total, dim))
-        hx = rng.normal(size=(total, p))
-        eps = rng.normal(size=(total, p))
-        y, sd = rng.normal(size=p), np.full(p, 0.3)
-        first, count = sharding.shard_range(total, world, rank)
+        logs, states, hx, eps, y, sd = _problem()
+        analysis = HostAnalysis()
+        first, count = sharding.shard_range(TOTAL, world, rank)
         sl = slice(first, first + count)
         # particle filter: identical weights and ancestors on every rank, then migration
-        w, inc, ess, mw, anc = sharding.pf_resample_distributed(torch.from_numpy(logs[sl]), 0.37)
+        w, inc, ess, mw, anc = sharding.pf_resample_distributed(torch.from_numpy(logs[sl]), 0.37,
+                                                                analysis)
         moved = sharding.exchange_members(torch.from_numpy(states[sl].copy()), anc)
         # EnKF: all-gather of HX, redundant solve, reduce-scatter of partial products
         xa = sharding.enkf_distributed(torch.from_numpy(states[sl].copy()),
                                        torch.from_numpy(hx[sl]), y, sd,
-                                       torch.from_numpy(eps[sl]))
+                                       torch.from_numpy(eps[sl]), analysis)
         q.put((rank, first, anc, inc, ess, moved.numpy(), xa.numpy()))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2])
-def test_distributed_filters_match_single_process(world):
+@pytest.mark.parametrize("world", [2, 3])
+def test_distributed_filters_match_single_process(world, oracle):
+    """The sharded filters on `world` gloo ranks (member blocks of 32/32 and 22/21/21) equal
+    the single-process computation: identical weights and ancestors on every rank, migrated
+    members equal to their ancestors, and the analysed states of the reduce-scatter update."""
+    from helpers import enkf_weight_matrix
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
@@ -87,16 +102,11 @@ def test_distributed_filters_match_single_process(world):
     for pr in procs:
         pr.join(timeout=60)
         assert pr.exitcode == 0
-    rng = np.random.default_rng(5)
-    total, dim, p = 10, 12, 3
-    logs = rng.normal(-20, 4, total)
-    states = rng.normal(size=(total, dim))
-    hx = rng.normal(size=(total, p))
-    eps = rng.normal(size=(total, p))
-    y, sd = rng.normal(size=p), np.full(p, 0.3)
-    w, inc, ess, mw = sharding.pf_weights(logs)
-    anc = sharding.systematic_resample(w, 0.37)
-    W = sharding.enkf_weight_matrix(hx, y, sd, eps)
+    logs, states, hx, eps, y, sd = _problem()
+    w, inc, ess, mw = oracle.pf_weights(logs)
+    anc = oracle.systematic_resample(w, 0.37)
+    assert len(set(anc.tolist())) < TOTAL   # the weights are uneven enough to resample
+    W = enkf_weight_matrix(hx, y, sd, eps)
     xa = states + (states - states.mean(axis=0)).T.dot(W).T
     moved_all, xa_all = np.zeros_like(states), np.zeros_like(states)
     for rank, first, a, i, e, moved, xa_local in results:

@@ -244,6 +244,8 @@ def library() -> C.CDLL:
         "hzlb_mixed_destroy": (None, [vp]),
         "hzlb_mixed_group": (vp, [vp, C.c_int]),
         "hzlb_mixed_step": (C.c_int, [vp, _dp, C.c_uint64]),
+        "hzlb_mixed_set_mode": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "hzlb_mixed_mode": (C.c_int, [vp, C.POINTER(C.c_int), _dp]),
         "hzlb_mixed_tune": (C.c_int, [vp, _dp, C.c_int, _dp]),
         "hzlb_mixed_schedule": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                           C.POINTER(C.c_int)]),
@@ -1150,12 +1152,26 @@ class Mixed:
         _check(self._lib.hzlb_mixed_tune(self._h, _p(d), repeats, C.byref(ms)))
         return ms.value
 
+    MODES = ("serial", "concurrent", "fused", "fused_branch")
+
     def schedule(self) -> dict:
         k = len(self.configs)
         serial = C.c_int()
         col, row = (C.c_int * k)(), (C.c_int * k)()
         _check(self._lib.hzlb_mixed_schedule(self._h, C.byref(serial), col, row))
-        return dict(serial=bool(serial.value), column_caps=list(col), row_caps=list(row))
+        mode = C.c_int()
+        tried = (C.c_double * 4)()
+        _check(self._lib.hzlb_mixed_mode(self._h, C.byref(mode), tried))
+        return dict(serial=bool(serial.value), mode=self.MODES[mode.value],
+                    column_caps=list(col), row_caps=list(row),
+                    tuned_ms={m: t for m, t in zip(self.MODES, tried) if t > 0})
+
+    def set_mode(self, mode: str, column_caps=None, row_caps=None) -> None:
+        """One of MODES (hzlb_mixed_set_mode); caps per group as in set_schedule."""
+        k = len(self.configs)
+        col = (C.c_int * k)(*column_caps) if column_caps is not None else None
+        row = (C.c_int * k)(*row_caps) if row_caps is not None else None
+        _check(self._lib.hzlb_mixed_set_mode(self._h, self.MODES.index(mode), col, row))
 
     def set_schedule(self, serial: bool, column_caps=None, row_caps=None) -> None:
         k = len(self.configs)

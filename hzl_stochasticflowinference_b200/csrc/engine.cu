@@ -471,6 +471,11 @@ template <typename R> class EngineT final : public Engine {
                 enqueue_ou(dt, 1, s);
         }
     }
+    void stage_args(double dt, void *col_out, void *row_out) const override {
+        *static_cast<ColumnArgs<R> *>(col_out) = column_args(dt);
+        *static_cast<RowArgs<R> *>(row_out) = row_args();
+    }
+    bool ou_enabled() const override { return ou_; }
     void finish_steps(double dt, uint64_t nsteps) override {
         w_valid_ = true;
         time += dt * static_cast<double>(nsteps);

@@ -140,6 +140,11 @@ class Engine {
     // enqueue `steps` RK4 steps on stream s, persistent grids capped at col_cap / row_cap
     // blocks (0: every resident block); allowed during stream capture
     virtual void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap) = 0;
+    // the stage kernels' arguments of this handle (ColumnArgs<R> / RowArgs<R> of its
+    // precision, stage and CFL scale unset) for a caller that launches the passes itself (the
+    // mixed-resolution kernels); OU forcing transitions are not part of them
+    virtual void stage_args(double dt, void *column_args, void *row_args) const = 0;
+    virtual bool ou_enabled() const = 0;
     // account for nsteps steps enqueued that way (clock, step counter, cached velocities)
     virtual void finish_steps(double dt, uint64_t nsteps) = 0;
     // member mean of the compact state into `out` (device, compact_size entries, own precision)

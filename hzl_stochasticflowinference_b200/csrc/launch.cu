@@ -251,3 +251,100 @@ HZLB_INSTANTIATE(float)
 HZLB_INSTANTIATE(double)
 
 } // namespace hzlb
+
+// ---- mixed-resolution kernels ----------------------------------------------------------
+namespace hzlb {
+namespace {
+// The fused kernels of a pack of resolutions: shared memory is the largest over the pack;
+// CMINB column blocks per SM (6, or 5 with 512^2 in the pack, whose 40.2 KB per block allow
+// no more) bound the registers of the column kernel; the row kernel keeps 6 blocks.
+template <int CMINB, int... Ns> struct MixedL {
+    static constexpr size_t row_smem = std::max({hzlb::row_smem<float, Ns>()...});
+    static constexpr size_t col_smem = std::max({hzlb::column_smem<float, Ns>()...});
+    static inline int row_res[64] = {}, col_res[64] = {};
+    static constexpr void (*cols[5])(const MixedColumnArgs<float>) = {
+        mixed_column_kernel<float, 0, CMINB, Ns...>, mixed_column_kernel<float, 1, CMINB, Ns...>,
+        mixed_column_kernel<float, 2, CMINB, Ns...>, mixed_column_kernel<float, 3, CMINB, Ns...>,
+        mixed_column_kernel<float, 4, CMINB, Ns...>};
+    static constexpr void (*rowk)(const MixedRowArgs<float>) = mixed_row_kernel<float, 6, Ns...>;
+    static cudaError_t prepare(int *cres, int *rres) {
+        cudaError_t e = cudaSuccess;
+        for (int st = 0; st < 5 && e == cudaSuccess; ++st)
+            e = cudaFuncSetAttribute(cols[st], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(col_smem));
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(rowk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(row_smem));
+        int dev = 0, sms = 0, cb = 1 << 30, rb = 0;
+        if (e == cudaSuccess)
+            e = cudaGetDevice(&dev);
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        for (int st = 0; st < 5 && e == cudaSuccess; ++st) {
+            int b = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, cols[st], 64, col_smem);
+            cb = std::min(cb, b);
+        }
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rb, rowk, 128, row_smem);
+        if (e == cudaSuccess && (cb < 1 || rb < 1))
+            e = cudaErrorInvalidConfiguration;
+        if (e == cudaSuccess && dev >= 0 && dev < 64) {
+            col_res[dev] = cb * sms;
+            row_res[dev] = rb * sms;
+        }
+        if (cres)
+            *cres = cb * sms;
+        if (rres)
+            *rres = rb * sms;
+        return e;
+    }
+    static int resident(const int *table) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        return dev >= 0 && dev < 64 && table[dev] > 0 ? table[dev] : 148;
+    }
+    static cudaError_t row(const MixedRowArgs<float> &a, int total, cudaStream_t s, int cap) {
+        const int res = cap > 0 ? std::min(cap, resident(row_res)) : resident(row_res);
+        const int grid = std::max(1, std::min(total, res));
+        rowk<<<grid, 128, row_smem, s>>>(a);
+        return cudaGetLastError();
+    }
+    static cudaError_t column(const MixedColumnArgs<float> &a, int stage, int total, cudaStream_t s,
+                              int cap) {
+        if (stage < 0 || stage > 4)
+            return cudaErrorInvalidValue;
+        const int res = cap > 0 ? std::min(cap, resident(col_res)) : resident(col_res);
+        const int grid = std::max(1, std::min(total, res));
+        cols[stage]<<<grid, 64, col_smem, s>>>(a);
+        return cudaGetLastError();
+    }
+};
+using Mixed3 = MixedL<6, 256, 128, 64>;
+using Mixed4 = MixedL<5, 512, 256, 128, 64>;
+} // namespace
+
+cudaError_t prepare_mixed(int classes, int *column_resident, int *row_resident) {
+    if (classes == 3)
+        return Mixed3::prepare(column_resident, row_resident);
+    if (classes == 4)
+        return Mixed4::prepare(column_resident, row_resident);
+    return cudaErrorInvalidValue;
+}
+cudaError_t launch_mixed_row(const MixedRowArgs<float> &a, int classes, int total_items,
+                             cudaStream_t s, int cap) {
+    if (classes == 3)
+        return Mixed3::row(a, total_items, s, cap);
+    if (classes == 4)
+        return Mixed4::row(a, total_items, s, cap);
+    return cudaErrorInvalidValue;
+}
+cudaError_t launch_mixed_column(const MixedColumnArgs<float> &a, int stage, int classes,
+                                int total_items, cudaStream_t s, int cap) {
+    if (classes == 3)
+        return Mixed3::column(a, stage, total_items, s, cap);
+    if (classes == 4)
+        return Mixed4::column(a, stage, total_items, s, cap);
+    return cudaErrorInvalidValue;
+}
+} // namespace hzlb

@@ -54,4 +54,14 @@ cudaError_t launch_observe_rows(int n, const cx<R> *field, long long stride, cx<
                                 double *out, cudaStream_t s);
 template <typename R> KernelShape kernel_shape(int n);
 
+// One persistent kernel per RK stage over a mixed-resolution work list (FP32, class c at
+// resolution 64 << c): `classes` 3 (64..256) or 4 (64..512).  prepare_mixed sets the kernels'
+// shared memory and returns their resident grids; the launchers take the total items of the
+// pass (every class's items) for the grid's cap.
+cudaError_t prepare_mixed(int classes, int *column_resident, int *row_resident);
+cudaError_t launch_mixed_row(const MixedRowArgs<float> &a, int classes, int total_items,
+                             cudaStream_t s, int cap = 0);
+cudaError_t launch_mixed_column(const MixedColumnArgs<float> &a, int stage, int classes,
+                                int total_items, cudaStream_t s, int cap = 0);
+
 } // namespace hzlb

@@ -18,6 +18,7 @@
 #include "launch.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <memory>
 #include <string>
@@ -28,6 +29,14 @@ namespace hzlb {
 struct GroupCaps {
     int col = 0, row = 0;   // 0: every resident block
 };
+
+// How a batch's steps are laid out in its graph: each resolution's own kernels one after
+// another (serial) or on concurrent branches with capped grids (concurrent); or one persistent
+// row kernel and one column kernel per RK stage over the whole mixed work list (fused); or the
+// fused kernels over 64^2..256^2 with the 512^2 resolution's kernels on a concurrent branch
+// (fused_branch: the 512^2 column pass needs 232 registers, which would cap every resolution's
+// residency in one kernel).
+enum class Mode : int { Serial = 0, Concurrent = 1, Fused = 2, FusedBranch = 3 };
 
 class Mixed {
   public:
@@ -137,11 +146,66 @@ class Mixed {
                         best = trial;
                     }
                 }
+        // the fused kernels over the mixed work list, and with the 512^2 resolution on a branch
+        // whose grid cap is searched too
+        Mode best_mode = Mode::Concurrent;
+        std::vector<GroupCaps> best_caps = best;
+        GroupCaps best_fused{};
+        tried_.clear();
+        tried_.push_back({Mode::Serial, serial});
+        tried_.push_back({Mode::Concurrent, best_ms});
+        if (fusable()) {
+            set_mode(Mode::Fused, std::vector<GroupCaps>(count()));
+            const double f = measure(dt, repeats);
+            tried_.push_back({Mode::Fused, f});
+            if (f < best_ms) {
+                best_ms = f;
+                best_mode = Mode::Fused;
+                best_caps = std::vector<GroupCaps>(count());
+            }
+            const int g5 = group_512();
+            if (g5 >= 0) {
+                // the branch's grid, then the fused kernels' grid, each as a fraction of its
+                // resident blocks
+                double fb_best = 0;
+                std::vector<GroupCaps> fb_caps(count());
+                GroupCaps fb_fused{};
+                auto try_fb = [&](const std::vector<GroupCaps> &caps, GroupCaps fused) {
+                    set_mode(Mode::FusedBranch, caps, fused);
+                    const double ms = measure(dt, repeats);
+                    if (fb_best == 0 || ms < fb_best) {
+                        fb_best = ms;
+                        fb_caps = caps;
+                        fb_fused = fused;
+                    }
+                };
+                for (double frac : {0.125, 0.25, 0.5, 1.0}) {
+                    std::vector<GroupCaps> trial(count());
+                    trial[g5].col = std::max(1, static_cast<int>(std::lround(resident_[g5].col * frac)));
+                    trial[g5].row = std::max(1, static_cast<int>(std::lround(resident_[g5].row * frac)));
+                    try_fb(trial, GroupCaps{});
+                }
+                const std::vector<GroupCaps> branch_caps = fb_caps;
+                for (double frac : {0.9, 0.8, 0.7}) {
+                    GroupCaps f;
+                    f.col = std::max(1, static_cast<int>(std::lround(fused_resident_.col * frac)));
+                    f.row = std::max(1, static_cast<int>(std::lround(fused_resident_.row * frac)));
+                    try_fb(branch_caps, f);
+                }
+                tried_.push_back({Mode::FusedBranch, fb_best});
+                if (fb_best < best_ms) {
+                    best_ms = fb_best;
+                    best_mode = Mode::FusedBranch;
+                    best_caps = fb_caps;
+                    best_fused = fb_fused;
+                }
+            }
+        }
         if (serial <= best_ms) {
-            set_schedule(true, std::vector<GroupCaps>(count()));
+            set_mode(Mode::Serial, std::vector<GroupCaps>(count()));
             best_ms = serial;
         } else {
-            set_schedule(false, best);
+            set_mode(best_mode, best_caps, best_fused);
         }
         tuned_serial_ms_ = serial;
         for (int g = 0; g < count(); ++g) {
@@ -164,10 +228,32 @@ class Mixed {
         }
     }
     void set_schedule(bool serial, const std::vector<GroupCaps> &caps) {
-        serial_ = serial;
+        set_mode(serial ? Mode::Serial : Mode::Concurrent, caps);
+    }
+    // caps: per group, used by the concurrent schedule and by the 512^2 branch of fused_branch
+    // fused: the grid caps of the fused kernels (0: every resident block)
+    void set_mode(Mode mode, const std::vector<GroupCaps> &caps, GroupCaps fused = GroupCaps{}) {
+        fused_caps_ = fused;
+        if ((mode == Mode::Fused || mode == Mode::FusedBranch) && !fusable())
+            raise(HZLB_EINVAL, "fused schedules need FP32 resolutions among 64, 128, 256 and 512 "
+                               "(one ensemble each, no device OU forcing)");
+        if (mode == Mode::FusedBranch && group_512() < 0)
+            raise(HZLB_EINVAL, "the fused schedule with a branch needs a 512^2 ensemble");
+        if (mode == Mode::Fused || mode == Mode::FusedBranch) {
+            int cres = 0, rres = 0;
+            cuda_check(cudaSetDevice(device_), "select CUDA device");
+            cuda_check(prepare_mixed(3, &cres, &rres), "configure mixed kernels");
+            if (mode == Mode::Fused && group_512() >= 0)
+                cuda_check(prepare_mixed(4, &cres, &rres), "configure mixed kernels");
+            fused_resident_.col = cres;
+            fused_resident_.row = rres;
+        }
+        mode_ = mode;
+        serial_ = mode == Mode::Serial;
         caps_ = caps;
         drop();
     }
+    Mode mode() const { return mode_; }
 
   private:
     struct Graph {
@@ -205,7 +291,18 @@ class Mixed {
         cuda_check(cudaStreamBeginCapture(main_, cudaStreamCaptureModeThreadLocal),
                    "begin mixed capture");
         try {
-            if (serial_) {
+            if (mode_ == Mode::Fused) {
+                enqueue_fused(dt, steps, main_, -1);
+            } else if (mode_ == Mode::FusedBranch) {
+                const int g5 = group_512();
+                cuda_check(cudaEventRecord(fork_, main_), "fork");
+                cuda_check(cudaStreamWaitEvent(branch_[g5], fork_, 0), "branch wait");
+                groups_[g5]->engine->enqueue_steps_on(dt[g5], steps, branch_[g5], caps_[g5].col,
+                                                      caps_[g5].row);
+                cuda_check(cudaEventRecord(join_[g5], branch_[g5]), "join record");
+                enqueue_fused(dt, steps, main_, g5);
+                cuda_check(cudaStreamWaitEvent(main_, join_[g5], 0), "join wait");
+            } else if (serial_) {
                 for (int g = 0; g < count(); ++g)
                     groups_[g]->engine->enqueue_steps_on(dt[g], steps, main_, 0, 0);
             } else {
@@ -253,7 +350,74 @@ class Mixed {
         return ms / (static_cast<double>(repeats) * kSteps);
     }
 
+    // ---- fused kernels over the mixed work list ------------------------------------
+    // class of group g in the fused kernels (resolution 64 << class), or -1
+    int class_of(int g) const {
+        const int n = groups_[g]->engine->config().n;
+        return n == 64 ? 0 : n == 128 ? 1 : n == 256 ? 2 : n == 512 ? 3 : -1;
+    }
+    // every group FP32 without device OU forcing, resolutions 64..512, one group per resolution
+    bool fusable() const {
+        if (count() > MIXED_CLASSES)
+            return false;
+        bool seen[MIXED_CLASSES] = {};
+        for (int g = 0; g < count(); ++g) {
+            const Engine &e = *groups_[g]->engine;
+            const int c = class_of(g);
+            if (c < 0 || seen[c] || e.config().precision != 4 || e.ou_enabled())
+                return false;
+            seen[c] = true;
+        }
+        return true;
+    }
+    int group_512() const {
+        for (int g = 0; g < count(); ++g)
+            if (class_of(g) == 3)
+                return g;
+        return -1;
+    }
+    // `steps` RK4 steps of every group except `skip` through the fused kernels on stream s
+    void enqueue_fused(const double *dt, int steps, cudaStream_t s, int skip) {
+        const int ccap = fused_caps_.col, rcap = fused_caps_.row;
+        MixedRowArgs<float> ra{};
+        MixedColumnArgs<float> ca{};
+        std::array<double, MIXED_CLASSES> cfl{};
+        int rtot = 0, ctot = 0, classes = 3;
+        for (int g = 0; g < count(); ++g) {
+            if (g == skip)
+                continue;
+            const int c = class_of(g), n = 64 << c;
+            Engine &e = *groups_[g]->engine;
+            e.stage_args(dt[g], &ca.cls[c], &ra.cls[c]);
+            const KernelShape k = kernel_shape<float>(n);
+            ra.items[c] = e.members() * (n / k.rows_per_block);
+            ca.items[c] = e.members() * k.col_blocks_per_member;
+            cfl[c] = dt[g] * n / (2 * 3.141592653589793238462643383279502884);
+            if (c == 3)
+                classes = 4;
+        }
+        // the work list in the kernels' processing order, largest resolution first
+        for (int c = MIXED_CLASSES - 1; c >= 0; --c) {
+            ra.offset[c] = rtot;
+            ca.offset[c] = ctot;
+            rtot += ra.items[c];
+            ctot += ca.items[c];
+        }
+        for (int i = 0; i < steps; ++i)
+            for (int st = 1; st <= 4; ++st) {
+                for (int c = 0; c < MIXED_CLASSES; ++c)
+                    ra.cls[c].cfl_scale = st == 1 ? cfl[c] : 0.0;
+                cuda_check(launch_mixed_row(ra, classes, rtot, s, rcap), "launch mixed row pass");
+                for (int c = 0; c < MIXED_CLASSES; ++c)
+                    ca.cls[c].stage = st;
+                cuda_check(launch_mixed_column(ca, st, classes, ctot, s, ccap),
+                           "launch mixed column pass");
+            }
+    }
+
     int device_ = 0;
+    Mode mode_ = Mode::Concurrent;
+    GroupCaps fused_caps_, fused_resident_;   // grid cap of the fused kernels (0: all resident)
     std::vector<std::unique_ptr<hzlb_ensemble>> groups_;
     cudaStream_t main_ = nullptr;
     std::vector<cudaStream_t> branch_;
@@ -262,6 +426,18 @@ class Mixed {
     std::vector<GroupCaps> caps_, resident_;
     bool serial_ = false;
     double tuned_serial_ms_ = 0;
+    std::vector<std::pair<Mode, double>> tried_;   // best ms per step of each schedule kind
+
+  public:
+    // the tuner's best time per step for each schedule kind it measured (ms; 0 if not measured)
+    void tuned_times(double *out4) const {
+        for (int i = 0; i < 4; ++i)
+            out4[i] = 0;
+        for (const auto &t : tried_)
+            out4[static_cast<int>(t.first)] = t.second;
+    }
+
+  private:
     std::vector<Graph> graphs_;
 };
 
@@ -317,6 +493,29 @@ HZLB_API int hzlb_mixed_tune(hzlb_mixed *h, const double *dt, int repeats, doubl
 }
 HZLB_API int hzlb_mixed_schedule(hzlb_mixed *h, int *serial, int *col_caps, int *row_caps) {
     return guarded_mixed([&] { mixed(h).schedule(serial, col_caps, row_caps); });
+}
+HZLB_API int hzlb_mixed_set_mode(hzlb_mixed *h, int mode, const int *col_caps,
+                                 const int *row_caps) {
+    return guarded_mixed([&] {
+        auto &m = mixed(h);
+        if (mode < 0 || mode > 3)
+            hzlb::raise(HZLB_EINVAL, "mixed schedule mode must be 0..3");
+        std::vector<hzlb::GroupCaps> caps(m.count());
+        for (int g = 0; g < m.count(); ++g) {
+            caps[g].col = col_caps ? std::max(0, col_caps[g]) : 0;
+            caps[g].row = row_caps ? std::max(0, row_caps[g]) : 0;
+        }
+        m.set_mode(static_cast<hzlb::Mode>(mode), caps);
+    });
+}
+HZLB_API int hzlb_mixed_mode(hzlb_mixed *h, int *mode, double *tuned_ms) {
+    return guarded_mixed([&] {
+        auto &m = mixed(h);
+        if (mode)
+            *mode = static_cast<int>(m.mode());
+        if (tuned_ms)
+            m.tuned_times(tuned_ms);
+    });
 }
 HZLB_API int hzlb_mixed_set_schedule(hzlb_mixed *h, int serial, const int *col_caps,
                                      const int *row_caps) {

@@ -196,12 +196,15 @@ __device__ __forceinline__ void transform_line(cx<R> (&x)[E], cx<R> *xsm, const 
 
 // S is the RK stage (0: velocity of the initial state only, 1..3 intermediate, 4 final), a
 // compile-time constant so that each stage's epilogue is straight-line code.
+// The column pass over work items first, first + stride, ... < items (member x group of LPB
+// kx columns), with `smem_raw` as its dynamic shared memory; column_kernel runs one resolution,
+// the mixed kernels run several one after another in one launch.  Every block of the grid
+// calls it (also with no items), as the final stage's step counter counts one arrival a block.
 template <typename R, int N, int S>
-__global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
-    column_kernel(const ColumnArgs<R> a, int items) {
+__device__ __forceinline__ void column_pass(const ColumnArgs<R> &a, int items, int first,
+                                            int stride, unsigned char *smem_raw) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, LD = G::LD, K = G::K, LPB = G::LPB;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     // product input [2][LPB][LS]: each line's two input columns, padded, double as the
     // exchange buffers of its forward transforms once read; state window [3][ST_STRIDE],
     // reused once the epilogue has consumed it as the exchange buffers [LPB][LS] of the
@@ -290,11 +293,11 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     cx<R> twr[thread_twiddles<N, E>()];
     if constexpr (reg_tw)
         load_thread_twiddles<N, E, R>(twr, tw, t);
-    if (threadIdx.x < 32 && forward && static_cast<int>(blockIdx.x) < items)
-        issue_nl(blockIdx.x);
+    if (threadIdx.x < 32 && forward && first < items)
+        issue_nl(first);
     bool timed_out = false;
     int k = 0;
-    for (int it = blockIdx.x; it < items; it += gridDim.x, ++k) {
+    for (int it = first; it < items; it += stride, ++k) {
         const int m = it / G::NCG, kx0 = (it % G::NCG) * LPB;
         const int kx = kx0 + line;
         const bool valid = kx < C;
@@ -352,8 +355,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
             // every line is done with the product buffer: stream the next item's in
             fence_proxy_async_shared();
             __syncthreads();
-            if (threadIdx.x < 32 && it + static_cast<int>(gridDim.x) < items)
-                issue_nl(it + gridDim.x);
+            if (threadIdx.x < 32 && it + stride < items)
+                issue_nl(it + stride);
             if (!block_wait(&bars[2], k & 1, &flags[1])) {
                 timed_out = true;
                 break;
@@ -513,6 +516,14 @@ __global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
     }
 }
 
+template <typename R, int N, int S>
+__global__ void __launch_bounds__(Cfg<R, N>::COL_THREADS)
+    column_kernel(const ColumnArgs<R> a, int items) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    column_pass<R, N, S>(a, items, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x),
+                         smem_raw);
+}
+
 // Packs the x-spectra of two real fields as a + i b for the inverse row transform.  A and B
 // hold kx = 0..K of the row (column-pass output); negative kx follow from the fields being
 // real (A(-kx) = conj A(kx)), and the kx = 0 entries are real (imaginary roundoff dropped, as
@@ -558,14 +569,14 @@ template <int N, int E> struct LowSlots {
     static constexpr int value = K / T + 1 < E ? K / T + 1 : E;
 };
 
-// FP32: at most 80 registers, so that 6 blocks fit an SM (95 unconstrained: 5 blocks; measured
-// 0.368 against 0.383 ms per launch at 2048 members, 256^2).
+// The row pass over work items first, first + stride, ... < items (member x tile of TY rows),
+// with `smem_raw` as its dynamic shared memory; row_kernel runs one resolution, the mixed
+// kernels run several one after another in one launch.
 template <typename R, int N>
-__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1)
-    row_kernel(const RowArgs<R> a, int items) {
+__device__ __forceinline__ void row_pass(const RowArgs<R> &a, int items, int first, int stride,
+                                         unsigned char *smem_raw) {
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     // input tile [TY][2][CW], refilled with the next item's tile as soon as every row has read
     // its entries; FFT line buffers [GROUPS][BUF], reused once every row has finished its
     // transforms as the staging of the product spectra [2C][TY] (swizzled rows)
@@ -591,13 +602,13 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1
         mbar_arrive_expect(&bar, tile_bytes);
         bulk_copy_g2s(tile, a.w + (static_cast<size_t>(m) * N + y0) * 2 * G::CW, tile_bytes, &bar);
     };
-    if (threadIdx.x == 0 && static_cast<int>(blockIdx.x) < items) {
+    if (threadIdx.x == 0 && first < items) {
         // test hook: a pending injection (consumed here) leaves this block's first copy
         // unissued, so its bounded wait below runs out with no copy in flight
         const bool skip = blockIdx.x == 0 && *static_cast<volatile unsigned *>(&a.ctl->inject) != 0 &&
                           atomicExch(&a.ctl->inject, 0u) != 0;
         if (!skip)
-            issue(blockIdx.x);
+            issue(first);
     }
 
     const int g = threadIdx.x / T, t = threadIdx.x % T;
@@ -610,7 +621,7 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1
     const int ty = active ? g : 0;
     cx<R> *sm = lines + g * G::BUF;
     int k = 0;
-    for (int it = blockIdx.x; it < items; it += gridDim.x, ++k) {
+    for (int it = first; it < items; it += stride, ++k) {
         const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
         if (!block_wait(&bar, k & 1, &flag)) {
             if (threadIdx.x == 0)
@@ -623,8 +634,8 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1
         // every row holds its inputs in registers: stream the next item's tile in
         fence_proxy_async_shared();
         __syncthreads();
-        if (threadIdx.x == 0 && it + static_cast<int>(gridDim.x) < items)
-            issue(it + gridDim.x);
+        if (threadIdx.x == 0 && it + stride < items)
+            issue(it + stride);
         transform_line<N, E, +1, R>(z, sm, tw, twr, t);
         R vmax = 0;
 #pragma unroll
@@ -690,6 +701,15 @@ __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1
     }
 }
 
+// FP32: at most 80 registers, so that 6 blocks fit an SM (95 unconstrained: 5 blocks; measured
+// 0.368 against 0.383 ms per launch at 2048 members, 256^2).
+template <typename R, int N>
+__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1)
+    row_kernel(const RowArgs<R> a, int items) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    row_pass<R, N>(a, items, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), smem_raw);
+}
+
 template <typename R, int N> constexpr size_t column_smem() {
     using G = Cfg<R, N>;
     return sizeof(cx<R>) * (2 * G::LPB * G::LS + G::ST_WORDS + G::TWE);
@@ -697,6 +717,79 @@ template <typename R, int N> constexpr size_t column_smem() {
 template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
     return sizeof(cx<R>) * (G::TILE + G::GROUPS * G::BUF + G::TWE);
+}
+
+} // namespace hzlb
+
+namespace hzlb {
+
+// ---- one persistent kernel per RK stage over several resolutions ----------------------
+// The work list of a mixed-resolution batch: class c (resolution 64 << c) holds items[c] work
+// items of its pass, the global indices [offset[c], offset[c] + items[c]) of one list the
+// persistent grid strides over, block b taking the indices congruent to b modulo the grid.
+// Each block runs the classes' passes one after another, so the grid stays busy across the
+// resolution boundaries instead of draining one resolution's launch before the next begins.
+constexpr int MIXED_CLASSES = 4;
+template <typename R> struct MixedRowArgs {
+    RowArgs<R> cls[MIXED_CLASSES];
+    int items[MIXED_CLASSES], offset[MIXED_CLASSES];
+};
+template <typename R> struct MixedColumnArgs {
+    ColumnArgs<R> cls[MIXED_CLASSES];
+    int items[MIXED_CLASSES], offset[MIXED_CLASSES];
+};
+// first local item of this block in a class whose items start at global index `offset`
+__device__ __forceinline__ int mixed_first(int offset) {
+    const int g = static_cast<int>(gridDim.x);
+    const int r = (static_cast<int>(blockIdx.x) - offset) % g;
+    return r < 0 ? r + g : r;
+}
+// between two classes' passes: every thread is done with the shared memory, through both the
+// generic and the bulk-copy proxy, before the next pass writes it
+__device__ __forceinline__ void mixed_boundary() {
+    fence_proxy_async_shared();
+    __syncthreads();
+}
+template <typename R, int... Ns> __host__ __device__ constexpr bool mixed_shapes_agree() {
+    return ((Cfg<R, Ns>::ROW_THREADS == 128 && Cfg<R, Ns>::COL_THREADS == 64) && ...);
+}
+// one class's pass in a mixed kernel; a class without items (a resolution the batch does not
+// hold: its arguments are empty) is skipped by every block alike
+template <typename R, int N>
+__device__ __forceinline__ void mixed_row_class(const MixedRowArgs<R> &a, int c, unsigned char *smem) {
+    if (a.items[c] > 0) {
+        row_pass<R, N>(a.cls[c], a.items[c], mixed_first(a.offset[c]), static_cast<int>(gridDim.x),
+                       smem);
+        mixed_boundary();
+    }
+}
+template <typename R, int N, int S>
+__device__ __forceinline__ void mixed_column_class(const MixedColumnArgs<R> &a, int c,
+                                                   unsigned char *smem) {
+    if (a.items[c] > 0) {
+        column_pass<R, N, S>(a.cls[c], a.items[c], mixed_first(a.offset[c]),
+                             static_cast<int>(gridDim.x), smem);
+        mixed_boundary();
+    }
+}
+// class (argument slot) of resolution n
+__host__ __device__ constexpr int mixed_class(int n) {
+    return n == 64 ? 0 : n == 128 ? 1 : n == 256 ? 2 : 3;
+}
+// The passes run in the order of the pack, heaviest items first (512^2 .. 64^2), so a block's
+// last items are the lightest and the launch ends without a tail of one large item; the host
+// numbers the work list in the same order.
+template <typename R, int MINB, int... Ns>
+__global__ void __launch_bounds__(128, MINB) mixed_row_kernel(const MixedRowArgs<R> a) {
+    static_assert(mixed_shapes_agree<R, Ns...>(), "one block shape for every resolution");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    (mixed_row_class<R, Ns>(a, mixed_class(Ns), smem_raw), ...);
+}
+template <typename R, int S, int MINB, int... Ns>
+__global__ void __launch_bounds__(64, MINB) mixed_column_kernel(const MixedColumnArgs<R> a) {
+    static_assert(mixed_shapes_agree<R, Ns...>(), "one block shape for every resolution");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    (mixed_column_class<R, Ns, S>(a, mixed_class(Ns), smem_raw), ...);
 }
 
 } // namespace hzlb

@@ -608,6 +608,16 @@ HZLB_API int hzlb_mixed_tune(hzlb_mixed *h, const double *dt, int repeats, doubl
 HZLB_API int hzlb_mixed_schedule(hzlb_mixed *h, int *serial, int *col_caps, int *row_caps);
 HZLB_API int hzlb_mixed_set_schedule(hzlb_mixed *h, int serial, const int *col_caps,
                                      const int *row_caps);
+/* Schedule modes: 0 serial, 1 concurrent (each resolution's kernels on its own graph branch,
+ * grids capped by col_caps / row_caps, 0 = every resident block), 2 fused (one persistent row
+ * kernel and one column kernel per RK stage over the whole mixed work list: FP32, resolutions
+ * among 64, 128, 256 and 512 with one ensemble each, no device OU forcing), 3 fused with the
+ * 512^2 ensemble's own kernels on a concurrent branch (its caps apply).  hzlb_mixed_tune
+ * measures every mode that applies and keeps the fastest; hzlb_mixed_mode reports the mode in
+ * effect and the tuner's best ms per step of modes 0..3 (tuned_ms: 4 doubles, 0 where not
+ * measured; may be NULL). */
+HZLB_API int hzlb_mixed_set_mode(hzlb_mixed *h, int mode, const int *col_caps, const int *row_caps);
+HZLB_API int hzlb_mixed_mode(hzlb_mixed *h, int *mode, double *tuned_ms);
 
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */

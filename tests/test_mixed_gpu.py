@@ -1,6 +1,8 @@
 """Mixed-resolution batches (hzlb_mixed_*): every schedule (serial, concurrent with capped
-grids, the autotuner's choice) advances each resolution exactly as stepping it alone does —
-bit for bit, since each work item's arithmetic does not depend on the grid size."""
+grids, one fused persistent kernel per stage over the mixed work list, fused with a 512^2
+branch, the autotuner's choice) advances each resolution exactly as stepping it alone does --
+bit for bit, since each work item's arithmetic does not depend on the grid or on the other
+resolutions in the launch."""
 from __future__ import annotations
 
 import numpy as np
@@ -67,4 +69,49 @@ def test_autotuner_keeps_results_exact(hzlb):
     got = [g.get_state_compact() for g in m.groups]
     for k, ref in enumerate(_alone(hzlb, cfgs, dts, [5] * 3)):
         np.testing.assert_array_equal(got[k], ref)
+    m.close()
+
+
+def _fused_configs(hzlb, with512=True):
+    out = [hzlb.Config(n=64, members=37, precision=4, nu=1e-3, noise_sigma=0.05, seed=4,
+                       forcing_kmax=0),
+           hzlb.Config(n=128, members=11, precision=4, nu=5e-4, noise_sigma=0.05, seed=5,
+                       forcing_kmax=0),
+           hzlb.Config(n=256, members=3, precision=4, nu=2.5e-4, noise_sigma=0.05, seed=6,
+                       forcing_kmax=0, member_base=48)]
+    if with512:
+        out.append(hzlb.Config(n=512, members=2, precision=4, nu=1.25e-4, noise_sigma=0.05,
+                               seed=7, forcing_kmax=0))
+    return out
+
+
+@pytest.mark.parametrize("mode,with512", [("fused", True), ("fused", False),
+                                          ("fused_branch", True)])
+def test_fused_kernels_match_separate_stepping(hzlb, mode, with512):
+    """One persistent row kernel and one column kernel per RK stage over the whole mixed work
+    list (and with the 512^2 resolution on its own branch) equal each resolution stepped alone,
+    bit for bit, including the step counters that key the noise across graph batches."""
+    cfgs = _fused_configs(hzlb, with512)
+    dts = [2e-3, 1e-3, 5e-4, 2.5e-4][:len(cfgs)]
+    m = hzlb.Mixed(cfgs)
+    for k, (g, c) in enumerate(zip(m.groups, cfgs)):
+        _init(hzlb, g, c, k)
+    m.set_mode(mode)
+    assert m.schedule()["mode"] == mode
+    m.step(dts, 11)
+    assert all(g.status() == 0 for g in m.groups)
+    got = [g.get_state_compact() for g in m.groups]
+    for k, ref in enumerate(_alone(hzlb, cfgs, dts, [11] * len(cfgs))):
+        np.testing.assert_array_equal(got[k], ref)
+    m.close()
+
+
+def test_fused_modes_are_refused_where_they_do_not_apply(hzlb):
+    m = hzlb.Mixed(_configs(hzlb))   # FP64 and 16^2 / 32^2 groups
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        m.set_mode("fused")
+    m.close()
+    m = hzlb.Mixed(_fused_configs(hzlb, with512=False))
+    with pytest.raises(hzlb.HzlbInvalidArgument):
+        m.set_mode("fused_branch")
     m.close()

@@ -596,7 +596,8 @@ def learned_experiment() -> dict:
                                                            "val_mse_persistence", "val_skill",
                                                            "train_seconds", "train_steps")},
                "data_seconds": res["data_seconds"]}
-        for mode in ("spectral", "learned", "hybrid", "persistence", "hybrid_persistence"):
+        for mode in ("spectral", "learned", "hybrid", "complement", "persistence",
+                     "hybrid_persistence", "complement_persistence"):
             out[mode] = {k: res[mode][k] for k in keep if k in res[mode]}
         return out
     except Exception as exc:   # report, never lose the main line

@@ -238,7 +238,7 @@ def library() -> C.CDLL:
         "hzlb_pod_project": (C.c_int, [vp, vp, C.c_int, vp, C.c_longlong, vp]),
         "hzlb_noise_amplitudes": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
                                             C.c_uint64, C.c_int, vp, C.c_longlong, vp]),
-        "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, vp]),
+        "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, vp, C.c_int]),
         "hzlb_ensemble_mean_device": (C.c_int, [vp, vp]),
         "hzlb_mixed_create": (C.c_int, [C.POINTER(hzlb_config), C.c_int, C.POINTER(vp)]),
         "hzlb_mixed_destroy": (None, [vp]),
@@ -575,14 +575,17 @@ class Ensemble:
         return w, nis.value
 
     def learned_forecast(self, pod: "Pod", mlp: "Mlp", dt: float, steps: int,
-                         mean_increment=None) -> None:
+                         mean_increment=None, centre: bool = True) -> None:
         """One window of the learned reduced forecast (hzlb_learned_forecast);
-        mean_increment: optional CUDA float32 tensor (compact field) moving the ensemble mean."""
+        mean_increment: optional CUDA float32 tensor (compact field) added to every member;
+        centre: the network then moves the members only about their mean (the increment is the
+        mean's change), else its changes are kept whole (the increment carries the rest)."""
         ptr = None
         if mean_increment is not None:
             _torch_ready()
             ptr = C.c_void_p(mean_increment.data_ptr())
-        _check(self._lib.hzlb_learned_forecast(self._h, pod._h, mlp._h, dt, steps, ptr))
+        _check(self._lib.hzlb_learned_forecast(self._h, pod._h, mlp._h, dt, steps, ptr,
+                                               1 if centre else 0))
 
     def mean_device(self, out) -> None:
         """Member mean of the compact state into out (CUDA tensor of the state's precision)."""

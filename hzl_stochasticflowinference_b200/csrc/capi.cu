@@ -302,11 +302,12 @@ int hzlb_dgemm(int M, int N, int K, double alpha, const double *A, long long sam
     });
 }
 int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
-                          uint64_t steps, const void *mean_increment) {
+                          uint64_t steps, const void *mean_increment, int centre) {
     int rc = HZLB_OK;
     const int outer = guarded([&] {
         auto &e = engine(h);
-        rc = hzlb::learned_forecast(e, e.config(), pod, mlp, 8, dt, steps, mean_increment);
+        rc = hzlb::learned_forecast(e, e.config(), pod, mlp, 8, dt, steps, mean_increment,
+                                    centre != 0);
     });
     return outer != HZLB_OK ? outer : rc;
 }

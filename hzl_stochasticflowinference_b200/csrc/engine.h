@@ -186,7 +186,7 @@ cudaError_t gemm(const tc::GemmArgs &g, int dtype, cudaStream_t s);
 
 // One window of the learned reduced forecast (pod.cu) on an FP32 ensemble.
 int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp *mlp, int q,
-                     double dt, uint64_t steps, const void *mean_increment);
+                     double dt, uint64_t steps, const void *mean_increment, bool centre);
 
 // Message returned by hzlb_last_error() on this thread.
 void set_last_error(const std::string &message);

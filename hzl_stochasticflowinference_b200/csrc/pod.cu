@@ -592,12 +592,14 @@ class PodBasis {
     // contribution of the window's noise), add the change of the coefficients back, then add
     // the window's noise increments themselves on every noise mode.
     //
-    // With mean_increment (device, D floats: the change of the ensemble mean over the window
-    // from another forecast, e.g. the spectral solver run on the mean), the network only moves
+    // With mean_increment (device, D floats) that field is added to every member after the
+    // network's change.  With centre it is the change of the ensemble mean over the window from
+    // another forecast (e.g. the spectral solver run on the mean) and the network only moves
     // the members about their mean: the members' coefficient changes are centred over the
-    // ensemble and mean_increment is added to every member.
+    // ensemble.  Without centre the network's changes are kept whole and the increment carries
+    // what the network cannot (e.g. the motion outside the POD space).
     void learned_window(Engine &e, const hzlb_config &cfg, hzlb_mlp *mlp, int q, double dt,
-                        uint64_t steps, const float *mean_increment) {
+                        uint64_t steps, const float *mean_increment, bool centre) {
         ensure_fitted();
         const int M = e.members();
         cudaStream_t s = static_cast<cudaStream_t>(e.stream());
@@ -613,10 +615,11 @@ class PodBasis {
         cuda_check(cudaGetLastError(), "launch noise amplitudes");
         if (int rc = hzlb_mlp_forward(mlp, xin, M, y, s))
             raise(rc, std::string("learned forecast network: ") + hzlb_last_error());
-        if (mean_increment)
+        const bool centred = mean_increment && centre;
+        if (centred)
             delta_mean<<<(r + 63) / 64, 64, 0, s>>>(y, xin, in, M, r, dmean);
         delta_split<<<blocks_for(static_cast<long long>(M) * r), 256, 0, s>>>(
-            y, xin, in, M, r, mean_increment ? dmean : nullptr, d3);
+            y, xin, in, M, r, centred ? dmean : nullptr, d3);
         cuda_check(cudaGetLastError(), "launch coefficient change");
         update(state, M, d3, s);
         if (mean_increment) {
@@ -977,7 +980,7 @@ HZLB_API int hzlb_noise_amplitudes(const hzlb_config *config, double dt, uint64_
 namespace hzlb {
 // Defined here so the learned forecast can reach both the engine and the basis.
 int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp *mlp, int q,
-                     double dt, uint64_t steps, const void *mean_increment) {
+                     double dt, uint64_t steps, const void *mean_increment, bool centre) {
     return guarded_pod([&] {
         if (!mlp || q != 8 || !(dt > 0) || steps == 0)
             raise(HZLB_EINVAL, "learned forecast needs a network with 8 noise inputs, dt > 0, steps > 0");
@@ -992,7 +995,8 @@ int learned_forecast(Engine &e, const hzlb_config &cfg, hzlb_pod *pod, hzlb_mlp 
         if (nr != b.r || nq != q || batch < e.members())
             raise(HZLB_EINVAL, "network shape does not match the POD rank, 8 noise inputs and the "
                                "ensemble size");
-        b.learned_window(e, cfg, mlp, q, dt, steps, static_cast<const float *>(mean_increment));
+        b.learned_window(e, cfg, mlp, q, dt, steps, static_cast<const float *>(mean_increment),
+                         centre);
         b.check_status(static_cast<cudaStream_t>(e.stream()));
     });
 }

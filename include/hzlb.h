@@ -579,13 +579,15 @@ HZLB_API int hzlb_add_window_noise(const hzlb_config *config, double dt, uint64_
  * The network predicts the coefficients at the end of the window less the projection of the
  * window's noise; outside the POD space the state changes by the noise alone.  Advances the
  * ensemble's time and step counter by `steps`.  The network must have r = the POD rank, q = 8
- * and max_batch >= members.  mean_increment: NULL, or a device array (compact FP32 field) with
- * the change of the ensemble mean over the window from another forecast of the mean (the
- * spectral step of a one-member ensemble holding hzlb_ensemble_mean_device): then the network
- * moves the members only about their mean (its coefficient changes are centred over the
- * ensemble) and mean_increment is added to every member. */
+ * and max_batch >= members.  mean_increment: NULL, or a device array (compact FP32 field)
+ * added to every member after the network's change: with centre != 0 the change of the
+ * ensemble mean over the window from another forecast of the mean (the spectral step of a
+ * one-member ensemble holding hzlb_ensemble_mean_device), the network then moving the members
+ * only about their mean (its coefficient changes are centred over the ensemble); with
+ * centre == 0 an increment the network cannot carry (e.g. the motion outside the POD space),
+ * the network's changes kept whole. */
 HZLB_API int hzlb_learned_forecast(hzlb_ensemble *h, hzlb_pod *pod, hzlb_mlp *mlp, double dt,
-                                   uint64_t steps, const void *mean_increment);
+                                   uint64_t steps, const void *mean_increment, int centre);
 
 /* ---- mixed-resolution batches (no counterpart in the reference) -----------------------
  * Ensembles of different grid sizes (and precisions) on one device advanced together: one CUDA

@@ -5,6 +5,9 @@ generated by the solver, POD, network training, and the EnKF twin experiment.
   persistence (what the method does without the network) on held-out windows;
 * every forecast variant keeps the filter finite and consistent, and the hybrid (spectral
   mean, learned anomalies) stays close to the spectral filter;
+* in the complement variant (the network moves every POD coefficient, the spectral step of the
+  mean supplies only the motion outside the POD space) switching the network off makes the
+  filter worse: the network carries the forecast there;
 * with an innovation-statistic limit below every statistic, the learned filter falls back to
   the spectral forecast on every cycle and then reproduces the spectral filter exactly.
 """
@@ -43,12 +46,15 @@ def test_twin_variants_are_consistent(experiment):
     spectral = out["spectral"]
     assert np.all(np.isfinite(spectral["rmse"]))
     assert spectral["mean_rmse"] < 0.5 * spectral["initial_rmse"]
-    for mode in ("learned", "hybrid", "persistence", "hybrid_persistence"):
+    for mode in ("learned", "hybrid", "complement", "persistence", "hybrid_persistence",
+                 "complement_persistence"):
         o = out[mode]
         assert np.all(np.isfinite(o["rmse"])) and len(o["rmse"]) == tc.cycles
         assert 0 <= o["fallback_cycles"] <= tc.cycles
         assert np.all(np.asarray(o["nis"]) > 0)
     assert out["hybrid"]["mean_rmse"] < 1.25 * spectral["mean_rmse"]
+    assert out["complement"]["mean_rmse"] < out["complement_persistence"]["mean_rmse"]
+    assert out["rmse_ratio"] == out["complement"]["rmse_ratio"]
 
 
 def test_fallback_on_every_cycle_reproduces_the_spectral_filter(hzlb, experiment):

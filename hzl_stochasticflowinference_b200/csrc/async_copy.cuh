@@ -43,6 +43,14 @@ __device__ __forceinline__ void bulk_copy_s2g(void *dst, const void *src, uint32
                  "r"(smem_u32(src)), "r"(bytes)
                  : "memory");
 }
+// Tiled tensor copy shared -> global of one box of `map` at coordinates (x, y, z), in this
+// thread's current bulk async-group (the map lies in kernel-parameter space).
+__device__ __forceinline__ void tensor_store_3d(const void *map, const void *src, int x, int y,
+                                                int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];"
+                 ::"l"(map), "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
 __device__ __forceinline__ void bulk_commit() {
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }

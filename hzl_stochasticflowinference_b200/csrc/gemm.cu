@@ -26,29 +26,11 @@ template <typename TIn, int BN> cudaError_t launch(const tc::GemmArgs &g, cudaSt
     tc::umma_gemm_kernel<TIn, BN><<<grid, 128, smem, s>>>(g);
     return cudaGetLastError();
 }
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
-using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                 const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                 const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiled encoder() {
-    static EncodeTiled fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiled>(p);
-    });
-    return fn;
-}
 // Tensor map of a K-contiguous operand (rows x K, row stride ld elements): boxes of
 // box_rows x 128 bytes, 128-byte swizzle, zero fill out of range.
 template <typename TIn>
 bool make_map(CUtensorMap *map, const void *ptr, int rows, int K, long long ld, int box_rows) {
-    EncodeTiled fn = encoder();
+    EncodeTiled fn = tensor_map_encoder();
     if (!fn || (reinterpret_cast<uintptr_t>(ptr) & 15) || (ld * sizeof(TIn)) % 16)
         return false;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(K), static_cast<cuuint64_t>(rows)};

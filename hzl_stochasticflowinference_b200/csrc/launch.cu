@@ -4,9 +4,53 @@
 #include "physical.cuh"
 
 #include <algorithm>
+#include <mutex>
 
 namespace hzlb {
+
+EncodeTiled tensor_map_encoder() {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    });
+    return fn;
+}
+
 namespace {
+
+// The tensor map through which the row pass of resolution N stores a tile's product spectra
+// (RowArgs::nlmap); nothing to do for resolutions that store them with plain stores.
+template <typename R, int N> cudaError_t row_store_map(RowArgs<R> &a) {
+    using G = Cfg<R, N>;
+    if constexpr (!G::ROW_TMA) {
+        return cudaSuccess;
+    } else {
+        constexpr cuuint32_t W = sizeof(cx<R>) / 4;   // 4-byte words per complex entry
+        EncodeTiled fn = tensor_map_encoder();
+        if (!fn || a.members < 1 || (reinterpret_cast<uintptr_t>(a.nl) & 15))
+            return cudaErrorInvalidValue;
+        const cuuint64_t dims[3] = {static_cast<cuuint64_t>(N) * W, 2 * G::C,
+                                    static_cast<cuuint64_t>(a.members)};
+        const cuuint64_t strides[2] = {static_cast<cuuint64_t>(N) * sizeof(cx<R>),
+                                       static_cast<cuuint64_t>(2 * G::C) * N * sizeof(cx<R>)};
+        const cuuint32_t box[3] = {static_cast<cuuint32_t>(G::TY) * W, 2 * G::C, 1};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        const CUtensorMapSwizzle sw = G::ROW_SPAN == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                      : G::ROW_SPAN == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                          : CU_TENSOR_MAP_SWIZZLE_128B;
+        return fn(&a.nlmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, a.nl, dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS
+                   ? cudaSuccess
+                   : cudaErrorInvalidValue;
+    }
+}
 
 template <typename R, int N> struct L {
     using G = Cfg<R, N>;
@@ -70,7 +114,10 @@ template <typename R, int N> struct L {
         col_kernels[a.stage]<<<grid, G::COL_THREADS, col_smem, s>>>(a, items);
         return cudaGetLastError();
     }
-    static cudaError_t row(const RowArgs<R> &a, cudaStream_t s, int cap) {
+    static cudaError_t row(const RowArgs<R> &args, cudaStream_t s, int cap) {
+        RowArgs<R> a = args;
+        if (cudaError_t e = row_store_map<R, N>(a))
+            return e;
         const int items = a.members * (N / G::TY);
         const int res = resident(row_resident);
         const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
@@ -304,7 +351,15 @@ template <int CMINB, int... Ns> struct MixedL {
         cudaGetDevice(&dev);
         return dev >= 0 && dev < 64 && table[dev] > 0 ? table[dev] : 148;
     }
-    static cudaError_t row(const MixedRowArgs<float> &a, int total, cudaStream_t s, int cap) {
+    static cudaError_t row(const MixedRowArgs<float> &args, int total, cudaStream_t s, int cap) {
+        MixedRowArgs<float> a = args;
+        cudaError_t e = cudaSuccess;
+        ((e = e == cudaSuccess && a.items[mixed_class(Ns)] > 0
+                  ? row_store_map<float, Ns>(a.cls[mixed_class(Ns)])
+                  : e),
+         ...);
+        if (e != cudaSuccess)
+            return e;
         const int res = cap > 0 ? std::min(cap, resident(row_res)) : resident(row_res);
         const int grid = std::max(1, std::min(total, res));
         rowk<<<grid, 128, row_smem, s>>>(a);

@@ -26,6 +26,14 @@ template <typename R> std::vector<cx<R>> host_twiddles(int n) {
     return tw;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda);
+// null when the driver does not provide it.
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                 const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                 const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled tensor_map_encoder();
+
 template <typename R> cudaError_t prepare_kernels(int n);
 // cap > 0 limits the persistent grid to cap blocks (default: all resident blocks of the device)
 template <typename R>

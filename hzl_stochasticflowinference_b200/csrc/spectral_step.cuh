@@ -31,6 +31,7 @@
 #include "async_copy.cuh"
 #include "fft.cuh"
 
+#include <cuda.h>
 #include <type_traits>
 
 namespace hzlb {
@@ -77,6 +78,15 @@ template <typename R, int N> struct Cfg {
     static constexpr int GROUPS = TY * T >= 32 ? TY : 32 / T;
     static constexpr int ROW_THREADS = GROUPS * T;
     static constexpr int TILE = TY * 2 * CW;          // row tile, complex entries
+    // The row pass writes a tile's product spectra ([2C] columns x TY rows) with one tiled
+    // tensor store when a staged column is one hardware swizzle span (32, 64 or 128 bytes) and
+    // the 2C columns fit one box (N = 128, 256 in FP32; 256 in FP64); the staging area then
+    // starts on a 1024-byte boundary inside the line buffers.
+    static constexpr int ROW_SPAN = TY * static_cast<int>(2 * sizeof(R));
+    static constexpr bool ROW_TMA = N >= 128 &&
+                                    (ROW_SPAN == 32 || ROW_SPAN == 64 || ROW_SPAN == 128) &&
+                                    2 * C <= 256 &&
+                                    2 * C * ROW_SPAN + 1024 <= GROUPS * BUF * static_cast<int>(2 * sizeof(R));
     static constexpr int TWE = pass_twiddle_entries<N, E>() > 0 ? pass_twiddle_entries<N, E>() : 1;
 };
 
@@ -120,6 +130,10 @@ template <typename R> struct ColumnArgs {
 };
 
 template <typename R> struct RowArgs {
+    // tensor map of the product spectra as 4-byte words {N * sizeof(cx<R>) / 4, 2C, M}, box
+    // {TY * sizeof(cx<R>) / 4, 2C, 1}, swizzle of the row span (filled by launch_row when the
+    // resolution stores through it, Cfg::ROW_TMA)
+    CUtensorMap nlmap;
     const cx<R> *w;       // [M][N][2][CW]
     cx<R> *nl;            // [M][2][C][N]
     const cx<R> *tw;
@@ -569,6 +583,53 @@ template <int N, int E> struct LowSlots {
     static constexpr int value = K / T + 1 < E ? K / T + 1 : E;
 };
 
+// One row's work between its inputs and its product spectra, by the T lanes that hold the
+// row: inverse transform of u + i v, products P = v^2 - u^2, Q = u v (and, with a.cfl_scale > 0,
+// the CFL check on |u| + |v|), forward transform of P + i Q, then separation of P^ and Q^ at
+// kx = p = t + r T (r < RL) from z(p) and conj z(N - p).  Position N - p of this row is held by
+// lane T - t at register E - 1 - r (t > 0), or by this lane at register (E - r) mod E (t = 0):
+// two shuffles per value, no trip through shared memory.  Every lane of the warp calls it.
+template <typename R, int N>
+__device__ __forceinline__ void row_line(cx<R> (&z)[Cfg<R, N>::E], cx<R> *sm, const cx<R> *tw,
+                                         const cx<R> (&twr)[thread_twiddles<N, Cfg<R, N>::E>()],
+                                         int t, const RowArgs<R> &a,
+                                         cx<R> (&ph)[LowSlots<N, Cfg<R, N>::E>::value],
+                                         cx<R> (&qh)[LowSlots<N, Cfg<R, N>::E>::value]) {
+    using G = Cfg<R, N>;
+    constexpr int E = G::E, T = G::T, RL = LowSlots<N, E>::value;
+    transform_line<N, E, +1, R>(z, sm, tw, twr, t);
+    R vmax = 0;
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const R u = z[r].x, v = z[r].y;
+        vmax = fmax(vmax, fabs(u) + fabs(v));
+        z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
+    }
+    if (a.cfl_scale > 0) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+        if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
+            atomicOr(&a.ctl->status, STATUS_CFL);
+    }
+    transform_line<N, E, -1, R>(z, sm, tw, twr, t);
+    const int lane = threadIdx.x & 31;
+    const int src = (lane & ~(T - 1)) + ((T - t) & (T - 1));
+    static_for<0, RL>([&](auto rc) {
+        constexpr int r = decltype(rc)::value;
+        constexpr int rs = E - 1 - r, r0 = (E - r) & (E - 1);
+        cx<R> zp;
+        zp.x = __shfl_sync(0xffffffffu, z[rs].x, src);
+        zp.y = __shfl_sync(0xffffffffu, z[rs].y, src);
+        if (t == 0)
+            zp = z[r0];
+        const cx<R> zk = z[r], zc = conj(zp);
+        const cx<R> sa = zk + zc, sb = zk - zc;
+        ph[r] = mk<R>(sa.x / 2, sa.y / 2);
+        qh[r] = mk<R>(sb.y / 2, -sb.x / 2);
+    });
+}
+
 // The row pass over work items first, first + stride, ... < items (member x tile of TY rows),
 // with `smem_raw` as its dynamic shared memory; row_kernel runs one resolution, the mixed
 // kernels run several one after another in one launch.
@@ -624,54 +685,58 @@ __device__ __forceinline__ void row_pass(const RowArgs<R> &a, int items, int fir
     for (int it = first; it < items; it += stride, ++k) {
         const int m = it / tiles_per_member, y0 = (it % tiles_per_member) * TY;
         if (!block_wait(&bar, k & 1, &flag)) {
-            if (threadIdx.x == 0)
+            if (threadIdx.x == 0) {
                 atomicOr(&a.ctl->status, STATUS_TIMEOUT);
+                bulk_wait_all();   // the product stores in flight complete before the block leaves
+            }
             return;   // uniform across the block
         }
         const cx<R> *row = tile + ty * 2 * G::CW;
         cx<R> z[E];
         pack_row<N, E, R>(z, row, row + G::CW, t);
-        // every row holds its inputs in registers: stream the next item's tile in
+        // every row holds its inputs in registers: stream the next item's tile in; the previous
+        // item's product store has read the staging area before the transforms write it
         fence_proxy_async_shared();
+        if constexpr (G::ROW_TMA)
+            if (threadIdx.x == 0)
+                bulk_wait_read_all();
         __syncthreads();
         if (threadIdx.x == 0 && it + stride < items)
             issue(it + stride);
-        transform_line<N, E, +1, R>(z, sm, tw, twr, t);
-        R vmax = 0;
-#pragma unroll
-        for (int r = 0; r < E; ++r) {
-            const R u = z[r].x, v = z[r].y;
-            vmax = fmax(vmax, fabs(u) + fabs(v));
-            z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
-        }
-        if (a.cfl_scale > 0) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-            if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
-                atomicOr(&a.ctl->status, STATUS_CFL);
-        }
-        transform_line<N, E, -1, R>(z, sm, tw, twr, t);
-        // separate P^ and Q^ at kx = p from z(p) and conj z(N - p).  Position N - p of this
-        // row is held by lane T - t at register E - 1 - r (t > 0), or by this lane at register
-        // (E - r) mod E (t = 0): two shuffles per value, no trip through shared memory
-        const int lane = threadIdx.x & 31;
-        const int src = (lane & ~(T - 1)) + ((T - t) & (T - 1));
         cx<R> ph[RL], qh[RL];
-        static_for<0, RL>([&](auto rc) {
-            constexpr int r = decltype(rc)::value;
-            constexpr int rs = E - 1 - r, r0 = (E - r) & (E - 1);
-            cx<R> zp;
-            zp.x = __shfl_sync(0xffffffffu, z[rs].x, src);
-            zp.y = __shfl_sync(0xffffffffu, z[rs].y, src);
-            if (t == 0)
-                zp = z[r0];
-            const cx<R> zk = z[r], zc = conj(zp);
-            const cx<R> sa = zk + zc, sb = zk - zc;
-            ph[r] = mk<R>(sa.x / 2, sa.y / 2);
-            qh[r] = mk<R>(sb.y / 2, -sb.x / 2);
-        });
+        row_line<R, N>(z, sm, tw, twr, t, a, ph, qh);
         __syncthreads();   // every row is done with its line buffer: stage the products there
+        if constexpr (G::ROW_TMA) {
+            // staged [2C][TY] in the layout of the tensor map's swizzle (16-byte chunk bits
+            // 4.. of an offset XORed with its bits 7..); one tiled store writes the tile's 2C
+            // column segments.  The swizzle spreads a row's 16-byte entries (FP64) over every
+            // bank; 8-byte entries (FP32) share address bit 3 within a row and reach half the
+            // banks per half warp (pairing rows by shuffles into 16-byte chunks removed those
+            // conflicts but cost as many instructions as it saved wavefronts: measured equal)
+            constexpr unsigned SZ = sizeof(cx<R>), RB = G::ROW_SPAN;
+            constexpr unsigned SWM = (RB / 16 - 1) << 4;
+            unsigned char *stage = reinterpret_cast<unsigned char *>(lines) +
+                                   ((1024u - (smem_u32(lines) & 1023u)) & 1023u);
+            if (active) {
+                static_for<0, RL>([&](auto rc) {
+                    constexpr int r = decltype(rc)::value;
+                    const int p = t + r * T;
+                    if (Band<N, T, r>::low || p <= K) {
+                        unsigned o = static_cast<unsigned>(p) * RB + ty * SZ;
+                        *reinterpret_cast<cx<R> *>(stage + (o ^ ((o >> 3) & SWM))) = ph[r];   // P^
+                        o = static_cast<unsigned>(C + p) * RB + ty * SZ;
+                        *reinterpret_cast<cx<R> *>(stage + (o ^ ((o >> 3) & SWM))) = qh[r];   // Q^
+                    }
+                });
+            }
+            fence_proxy_async_shared();
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                tensor_store_3d(&a.nlmap, stage, y0 * static_cast<int>(SZ / 4), 0, m);
+                bulk_commit();
+            }
+            continue;
+        }
         cx<R> *nlt = lines;
         if (active) {
             static_for<0, RL>([&](auto rc) {
@@ -699,13 +764,16 @@ __device__ __forceinline__ void row_pass(const RowArgs<R> &a, int items, int fir
         // the next item's transforms write the line buffers only after its tile barrier and
         // the block barrier that follows it
     }
+    if constexpr (G::ROW_TMA)
+        if (threadIdx.x == 0)
+            bulk_wait_all();   // this block's product stores are complete before it leaves
 }
 
 // FP32: at most 80 registers, so that 6 blocks fit an SM (95 unconstrained: 5 blocks; measured
 // 0.368 against 0.383 ms per launch at 2048 members, 256^2).
 template <typename R, int N>
 __global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1)
-    row_kernel(const RowArgs<R> a, int items) {
+    row_kernel(const __grid_constant__ RowArgs<R> a, int items) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     row_pass<R, N>(a, items, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), smem_raw);
 }
@@ -718,7 +786,6 @@ template <typename R, int N> constexpr size_t row_smem() {
     using G = Cfg<R, N>;
     return sizeof(cx<R>) * (G::TILE + G::GROUPS * G::BUF + G::TWE);
 }
-
 } // namespace hzlb
 
 namespace hzlb {
@@ -780,7 +847,7 @@ __host__ __device__ constexpr int mixed_class(int n) {
 // last items are the lightest and the launch ends without a tail of one large item; the host
 // numbers the work list in the same order.
 template <typename R, int MINB, int... Ns>
-__global__ void __launch_bounds__(128, MINB) mixed_row_kernel(const MixedRowArgs<R> a) {
+__global__ void __launch_bounds__(128, MINB) mixed_row_kernel(const __grid_constant__ MixedRowArgs<R> a) {
     static_assert(mixed_shapes_agree<R, Ns...>(), "one block shape for every resolution");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     (mixed_row_class<R, Ns>(a, mixed_class(Ns), smem_raw), ...);

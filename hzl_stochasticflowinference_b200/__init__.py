@@ -238,6 +238,8 @@ def library() -> C.CDLL:
         "hzlb_pod_project": (C.c_int, [vp, vp, C.c_int, vp, C.c_longlong, vp]),
         "hzlb_noise_amplitudes": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
                                             C.c_uint64, C.c_int, vp, C.c_longlong, vp]),
+        "hzlb_set_step_schedule": (C.c_int, [vp, C.c_int]),
+        "hzlb_step_schedule": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, vp, C.c_int]),
         "hzlb_ensemble_mean_device": (C.c_int, [vp, vp]),
         "hzlb_mixed_create": (C.c_int, [C.POINTER(hzlb_config), C.c_int, C.POINTER(vp)]),
@@ -417,6 +419,20 @@ class Ensemble:
         block's first tile copy unissued, its bounded wait runs out and the step reports
         STATUS_TIMEOUT."""
         _check(self._lib.hzlb_test_inject_wait_timeout(self._h))
+
+    STEP_SCHEDULES = ("single", "parts", "offset_parts")
+
+    def set_step_schedule(self, schedule) -> None:
+        """How step graphs run the members (hzlb_set_step_schedule): "single" (one pass per
+        RK stage), "parts" (two member parts on two streams), "offset_parts" (the second part
+        one row pass behind); a name or its index."""
+        code = self.STEP_SCHEDULES.index(schedule) if isinstance(schedule, str) else int(schedule)
+        _check(self._lib.hzlb_set_step_schedule(self._h, code))
+
+    def step_schedule(self) -> str:
+        v = C.c_int()
+        _check(self._lib.hzlb_step_schedule(self._h, C.byref(v)))
+        return self.STEP_SCHEDULES[v.value]
 
     def step_checked(self, dt: float):
         """One step that is undone when its stage-1 CFL check fails (hzlb_step_checked);

@@ -101,6 +101,15 @@ int hzlb_test_inject_wait_timeout(hzlb_ensemble *h) {
 int hzlb_step_checked(hzlb_ensemble *h, double dt) {
     return guarded([&] { engine(h).step_checked(dt); });
 }
+int hzlb_set_step_schedule(hzlb_ensemble *h, int schedule) {
+    return guarded([&] { engine(h).set_step_schedule(schedule); });
+}
+int hzlb_step_schedule(hzlb_ensemble *h, int *schedule) {
+    return guarded([&] {
+        need(schedule, "schedule");
+        *schedule = engine(h).step_schedule();
+    });
+}
 int hzlb_step_host(hzlb_ensemble *h, const void *state_in, void *state_out, double dt,
                    uint64_t nsteps, int chunk_members) {
     return guarded([&] { engine(h).step_host(state_in, state_out, dt, nsteps, chunk_members); });

@@ -92,6 +92,9 @@ class Engine {
     virtual void step(double dt, uint64_t nsteps) = 0;
     // one step, undone (state, forcing, clock, counter) when its stage-1 CFL check fails
     virtual void step_checked(double dt) = 0;
+    // how the step graphs run the members (hzlb_set_step_schedule)
+    virtual void set_step_schedule(int schedule) = 0;
+    virtual int step_schedule() const = 0;
     // nsteps steps of a host-resident state (compact layout): copied in, stepped and copied
     // out in member chunks that overlap copies with stepping
     virtual void step_host(const void *in, void *out, double dt, uint64_t nsteps, int chunk) = 0;

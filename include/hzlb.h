@@ -131,12 +131,21 @@ HZLB_API int hzlb_step(hzlb_ensemble *h, double dt, uint64_t nsteps);
  * the state, forcing, clock and step counter are left as they were before the call and
  * HZLB_ERUNTIME ("GPU CFL limit exceeded") is returned.  Synchronous. */
 HZLB_API int hzlb_step_checked(hzlb_ensemble *h, double dt);
+/* No counterpart in the reference.  How hzlb_step's graphs run the members: 0, one row and one
+ * column pass per RK stage over the whole ensemble; 1, the members in two parts, each with its
+ * own passes on its own stream, side by side; 2, as 1 with the second part one row pass behind
+ * the first, so that one part's row passes (bound by arithmetic) overlap the other's column
+ * passes (bound by memory).  Parts need at least 256 members and no device OU forcing (else
+ * schedule 0 runs).  Default 1.  Results are identical bit for bit under every schedule. */
+HZLB_API int hzlb_set_step_schedule(hzlb_ensemble *h, int schedule);
+HZLB_API int hzlb_step_schedule(hzlb_ensemble *h, int *schedule);
 /* No counterpart in the reference (its CudaSolver copies each member's state in and out around
  * every step, cuda_solver.cu:173-235).  The ensemble state lives on the host: state_in is read
  * and state_out written (both all members, the compact layout of the configured precision, as
  * hzlb_set_state_compact; they may be the same buffer), nsteps steps in between.  The members
- * go in chunks of about chunk_members (0: an eighth of the ensemble), each chunk's copies
- * overlapping the stepping of the others; pinned host buffers are needed for the overlap.
+ * go in chunks of about chunk_members (0: a sixteenth of the ensemble, at least 32 members),
+ * each chunk's copies overlapping the stepping of the others; pinned host buffers are needed
+ * for the overlap.
  * Results equal hzlb_set_state_compact + hzlb_step + hzlb_get_state_compact bit for bit.
  * Asynchronous on the handle's stream; device OU forcing is not supported here. */
 HZLB_API int hzlb_step_host(hzlb_ensemble *h, const void *state_in, void *state_out, double dt,

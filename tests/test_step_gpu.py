@@ -376,3 +376,33 @@ def test_nonfinite_state_flagged(hzlb):
     e.set_state_compact(compact)
     e.step(1e-4, 1)
     assert e.status() & hzlb.STATUS_NONFINITE
+
+
+@pytest.mark.parametrize("precision,n,members", [(4, 64, 300), (8, 32, 258), (4, 256, 256)])
+def test_step_schedules_agree_bit_for_bit(hzlb, precision, n, members):
+    """hzlb_set_step_schedule: the ensemble in two member parts on two streams (side by side, or
+    the second part one row pass behind) steps exactly as the single pass does, through graph
+    batches of 8 steps and single steps alike; the clock, step counter and status come back
+    whole; a pending wait-timeout injection reaches the first part and is reported."""
+    dt, seed = 1e-3 if n < 256 else 2.5e-4, 5
+    runs = {}
+    for schedule in ("single", "parts", "offset_parts"):
+        e = device_synthetic(hzlb, n, members, precision, 1e-3, 0.05, seed)
+        e.set_step_schedule(schedule)
+        assert e.step_schedule() == schedule
+        e.step(dt, 8 + 3)
+        assert e.status() == 0
+        runs[schedule] = (e.get_state_compact(), e.time())
+        e.inject_wait_timeout()
+        e.step(dt, 1)
+        assert e.status() & hzlb.STATUS_TIMEOUT
+        e.close()
+    for schedule in ("parts", "offset_parts"):
+        np.testing.assert_array_equal(runs[schedule][0], runs["single"][0])
+        assert runs[schedule][1] == runs["single"][1]
+    with pytest.raises(hzlb.HzlbError):
+        e = device_synthetic(hzlb, 16, 4, 4, 1e-3, 0.05, seed)
+        try:
+            e.set_step_schedule(3)
+        finally:
+            e.close()

@@ -191,6 +191,21 @@ __device__ __forceinline__ float gelu(float x) {
     return 0.5f * x * (1.0f + tanhf(k0 * (x + k1 * x * x * x)));
 }
 
+// Warps 2 and 3 are idle while thread 0 feeds and thread 32 issues the MMAs: when the epilogue
+// will read C back (beta != 0, no split-K partials), they bring the tile's rows of C into L2
+// (one prefetch per 128-byte line), so that read overlaps the main loop instead of following it.
+template <int BN>
+__device__ __forceinline__ void prefetch_c_tile(const GemmArgs &g, int m0, int n0) {
+    if (threadIdx.x < 64 || g.splits > 1 || g.beta == 0.0f || !g.C)
+        return;
+    constexpr int LINES = BN / 32;   // 128-byte lines of a tile row
+    for (int i = static_cast<int>(threadIdx.x) - 64; i < BM * LINES; i += 64) {
+        const int row = m0 + i / LINES, col = n0 + (i % LINES) * 32;
+        if (row < g.M && col < g.N)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(g.C + static_cast<long long>(row) * g.ldc + col));
+    }
+}
+
 // Epilogue of a 128 x BN accumulator tile: each warp copies its 32 TMEM lanes (rows) to the
 // shared-memory tile `stage` (row stride BN + 1 floats, conflict-free), then writes its rows
 // back with lanes along the columns, so every global read and write is a contiguous 128-byte

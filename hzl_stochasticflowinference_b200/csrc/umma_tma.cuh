@@ -94,6 +94,7 @@ __global__ void __launch_bounds__(128) umma_tma_kernel(const __grid_constant__ C
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_base;
+    prefetch_c_tile<BN>(g, m0, n0);
 
     if (threadIdx.x == 0) {
         // producer

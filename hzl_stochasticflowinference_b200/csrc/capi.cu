@@ -32,6 +32,7 @@ template <class F> int guarded(F &&f) {
 hzlb::Engine &engine(hzlb_ensemble *h) {
     if (!h || !h->engine)
         hzlb::raise(HZLB_EINVAL, "null ensemble handle");
+    ++h->engine->api_calls;
     return *h->engine;
 }
 void need(const void *p, const char *what) {
@@ -114,7 +115,12 @@ int hzlb_step_host(hzlb_ensemble *h, const void *state_in, void *state_out, doub
                    uint64_t nsteps, int chunk_members) {
     return guarded([&] { engine(h).step_host(state_in, state_out, dt, nsteps, chunk_members); });
 }
-void *hzlb_stream(hzlb_ensemble *h) { return h && h->engine ? h->engine->stream() : nullptr; }
+void *hzlb_stream(hzlb_ensemble *h) {
+    if (!h || !h->engine)
+        return nullptr;
+    ++h->engine->api_calls;   // the caller may order its own work on the stream
+    return h->engine->stream();
+}
 int hzlb_step_profiled(hzlb_ensemble *h, double dt, uint64_t nsteps, double *row_ms,
                        double *column_ms) {
     return guarded([&] {

@@ -115,6 +115,8 @@ template <typename R> class EngineT final : public Engine {
                 cudaEventDestroy(e);
         for (auto &e : pipe_events_)
             cudaEventDestroy(e);
+        for (auto &e : d2h_events_)
+            cudaEventDestroy(e);
         for (auto &e : split_events_)
             if (e)
                 cudaEventDestroy(e);
@@ -553,6 +555,7 @@ template <typename R> class EngineT final : public Engine {
     }
     int step_schedule() const override { return schedule_; }
     void prepare_steps(double dt) override {
+        ++api_calls;   // a mixed batch steps this ensemble: no host-pipelined call chains across it
         const int largest = (n_ - 1) / 3;
         if (!std::isfinite(dt) || dt <= 0 ||
             dt * (2 * cfg_.nu * largest * largest + cfg_.alpha) > 2.5)
@@ -691,8 +694,19 @@ template <typename R> class EngineT final : public Engine {
                    "initialise chunk control");
         cudaEvent_t start = pipe_events_[2 * chunks], end = pipe_events_[2 * chunks + 1],
                     side = pipe_events_[2 * chunks + 2];
+        // A call that directly follows another with the same chunks (no other call on this
+        // handle in between) lets each chunk's upload wait only for the previous call's
+        // download of the same chunk, so the uploads overlap the previous call's last
+        // downloads; its steps and downloads still follow the whole previous call.
+        const bool chained = pipe_mark_ != 0 && api_calls == pipe_mark_ + 1 && chunks == pipe_chunks_;
+        while (d2h_events_.size() < static_cast<size_t>(chunks)) {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
+            d2h_events_.push_back(e);
+        }
         cuda_check(cudaEventRecord(start, stream_), "record event");
-        cuda_check(cudaStreamWaitEvent(copy_in_, start, 0), "order copy stream");
+        if (!chained)
+            cuda_check(cudaStreamWaitEvent(copy_in_, start, 0), "order copy stream");
         cuda_check(cudaStreamWaitEvent(compute2_, start, 0), "order compute stream");
         const auto *src = static_cast<const unsigned char *>(in);
         auto *dst = static_cast<unsigned char *>(out);
@@ -700,6 +714,8 @@ template <typename R> class EngineT final : public Engine {
         for (int i = 0; i < chunks; ++i) {
             const int f = i * chunk, k = std::min(chunk, M_ - f);
             const size_t off = static_cast<size_t>(f) * compact_, bytes = bytes_per * k;
+            if (chained)
+                cuda_check(cudaStreamWaitEvent(copy_in_, d2h_events_[i], 0), "order upload");
             cuda_check(cudaMemcpyAsync(omega_.as<cx<R>>() + off, src + bytes_per * f, bytes,
                                        cudaMemcpyHostToDevice, copy_in_),
                        "host state upload");
@@ -738,6 +754,7 @@ template <typename R> class EngineT final : public Engine {
             cuda_check(cudaMemcpyAsync(dst + bytes_per * f, omega_.as<cx<R>>() + off, bytes,
                                        cudaMemcpyDeviceToHost, copy_out_),
                        "host state download");
+            cuda_check(cudaEventRecord(d2h_events_[i], copy_out_), "record event");
         }
         cuda_check(cudaEventRecord(side, compute2_), "record event");
         cuda_check(cudaStreamWaitEvent(stream_, side, 0), "join compute streams");
@@ -749,6 +766,8 @@ template <typename R> class EngineT final : public Engine {
         w_valid_ = true;
         time += dt * static_cast<double>(nsteps);
         step_index += nsteps;
+        pipe_mark_ = api_calls;
+        pipe_chunks_ = chunks;
     }
     void step_profiled(double dt, uint64_t nsteps, double *row_ms, double *col_ms) override {
         const int largest = (n_ - 1) / 3;
@@ -1382,6 +1401,11 @@ template <typename R> class EngineT final : public Engine {
     cudaStream_t copy_in_ = nullptr, copy_out_ = nullptr, compute2_ = nullptr;
     std::vector<cudaEvent_t> pipe_events_;
     DeviceBuffer chunk_ctl_;
+    // host-pipelined stepping: per-chunk download events of the last call, the handle's call
+    // count at its end (0: none yet) and its chunk count
+    std::vector<cudaEvent_t> d2h_events_;
+    uint64_t pipe_mark_ = 0;
+    int pipe_chunks_ = 0;
     // step graphs in two parts (split_members); two parts side by side measured 285k against
     // 274k member-steps/s in FP64 and 614k against 606k in FP32 (2048 members, 256^2, graphs
     // of 8 steps), the offset parts 283k and 610k

@@ -84,6 +84,9 @@ struct EnkfResult {
 class Engine {
   public:
     virtual ~Engine() = default;
+    // calls that reach this ensemble through the C ABI (or a mixed batch); a host-pipelined
+    // step chains to the previous one only when nothing else came in between
+    uint64_t api_calls = 0;
     virtual void set_state(const double *spectra, int first, int count) = 0;
     virtual void get_state(double *spectra, int first, int count) = 0;
     virtual void set_state_compact(const void *data, int first, int count) = 0;

@@ -114,3 +114,25 @@ def test_per_member_forcing_offsets(hzlb):
             outs.append(np.ascontiguousarray(e.get_state_compact()).view(np.float64).reshape(-1))
         e.close()
     assert np.array_equal(outs[0].reshape(-1), outs[1].reshape(-1))
+
+
+def test_consecutive_calls_chain_and_stay_exact(hzlb):
+    """Back-to-back calls on one handle let each chunk's upload follow only the previous call's
+    download of that chunk; with the state in place (in = out) and a call of another kind
+    breaking the chain halfway, five calls still equal five device steps bit for bit."""
+    n, members, dt = 256, 512, 5e-4
+    a, b = _pair(hzlb, n, members, 4)
+    host, _ = _pinned_state(a, np.float32)
+    a.set_state_compact_ptr(host.data_ptr(), 0, members)
+    a.step(dt, 5)
+    want = a.get_state_compact()
+    for i in range(5):
+        b.step_host_ptr(host.data_ptr(), host.data_ptr(), dt, 1, 0)
+        if i == 2:
+            assert b.status() == 0   # another call in between: the next one starts afresh
+    b.synchronize()
+    got = host.numpy().view(want.dtype).reshape(want.shape)
+    assert np.array_equal(got, want)
+    assert b.status() == 0
+    a.close()
+    b.close()

@@ -598,19 +598,21 @@ __device__ __forceinline__ void row_line(cx<R> (&z)[Cfg<R, N>::E], cx<R> *sm, co
     using G = Cfg<R, N>;
     constexpr int E = G::E, T = G::T, RL = LowSlots<N, E>::value;
     transform_line<N, E, +1, R>(z, sm, tw, twr, t);
-    R vmax = 0;
+    if (a.cfl_scale > 0) {   // uniform: the stage-1 launch checks the velocities
+        R vmax = 0;
 #pragma unroll
-    for (int r = 0; r < E; ++r) {
-        const R u = z[r].x, v = z[r].y;
-        vmax = fmax(vmax, fabs(u) + fabs(v));
-        z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
-    }
-    if (a.cfl_scale > 0) {
+        for (int r = 0; r < E; ++r)
+            vmax = fmax(vmax, fabs(z[r].x) + fabs(z[r].y));
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
             vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
         if ((threadIdx.x & 31) == 0 && static_cast<double>(vmax) * a.cfl_scale > 0.5)
             atomicOr(&a.ctl->status, STATUS_CFL);
+    }
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const R u = z[r].x, v = z[r].y;
+        z[r] = mk<R>(v * v - u * u, u * v);   // P + i Q
     }
     transform_line<N, E, -1, R>(z, sm, tw, twr, t);
     const int lane = threadIdx.x & 31;

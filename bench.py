@@ -707,6 +707,9 @@ def main():
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--step-schedule", choices=["single", "parts", "offset_parts"],
+                    help="hzlb_set_step_schedule for the main and FP64 legs (default: the "
+                         "library's, two member parts from 256 members)")
     ap.add_argument("--case", choices=["gemm", "enkf", "learned", "likelihood", "tangent"])
     args = ap.parse_args()
     if args.case:
@@ -745,12 +748,16 @@ def main():
 
     # ---- the headline: FP32 at 256^2 --------------------------------------------------
     ens = build_ensemble(hz, 4, M, rank * M, local)
+    if args.step_schedule:
+        ens.set_step_schedule(args.step_schedule)
     clocks = ClockSampler(local)
     main_leg = measure(hz, torch, ens, 4, args.steps, args.warmup, world, barrier, max_over_ranks,
                        clocks)
     ens.close()
     # ---- the same workload in FP64 (the reference's precision), same members and steps ----
     ens = build_ensemble(hz, 8, M, rank * M, local)
+    if args.step_schedule:
+        ens.set_step_schedule(args.step_schedule)
     fp64 = measure(hz, torch, ens, 8, args.steps, args.warmup, world, barrier, max_over_ranks)
     ens.close()
 

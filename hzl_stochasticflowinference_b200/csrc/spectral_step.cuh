@@ -109,7 +109,7 @@ struct StepControl {
 };
 
 template <typename R> struct ColumnArgs {
-    const cx<R> *nl;        // [M][2][C][N]
+    const cx<R> *nl;        // [M][2][C][N]: 2 P^, 2 Q^ (x-transformed products, doubled)
     cx<R> *w;               // [M][N][2][CW]
     cx<R> *omega;           // [M][C][LD]
     cx<R> *ystage;          // [M][C][LD]
@@ -375,7 +375,8 @@ __device__ __forceinline__ void column_pass(const ColumnArgs<R> &a, int items, i
                 timed_out = true;
                 break;
             }
-            const R inv_n2 = static_cast<R>(1.0 / (static_cast<double>(N) * N));
+            // 1/N^2 of the unnormalised transforms, halved: the row pass stores 2 P^ and 2 Q^
+            const R inv_n2 = static_cast<R>(0.5 / (static_cast<double>(N) * N));
             const R nu = static_cast<R>(a.nu), alpha = static_cast<R>(a.alpha),
                     dt = static_cast<R>(a.dt);
             bool bad = false;
@@ -586,7 +587,9 @@ template <int N, int E> struct LowSlots {
 // One row's work between its inputs and its product spectra, by the T lanes that hold the
 // row: inverse transform of u + i v, products P = v^2 - u^2, Q = u v (and, with a.cfl_scale > 0,
 // the CFL check on |u| + |v|), forward transform of P + i Q, then separation of P^ and Q^ at
-// kx = p = t + r T (r < RL) from z(p) and conj z(N - p).  Position N - p of this row is held by
+// kx = p = t + r T (r < RL) from z(p) and conj z(N - p), both stored doubled (the column pass
+// folds the halving into its 1/N^2: power-of-two scalings commute with rounding, so the
+// results are those of halving here).  Position N - p of this row is held by
 // lane T - t at register E - 1 - r (t > 0), or by this lane at register (E - r) mod E (t = 0):
 // two shuffles per value, no trip through shared memory.  Every lane of the warp calls it.
 template <typename R, int N>
@@ -627,8 +630,8 @@ __device__ __forceinline__ void row_line(cx<R> (&z)[Cfg<R, N>::E], cx<R> *sm, co
             zp = z[r0];
         const cx<R> zk = z[r], zc = conj(zp);
         const cx<R> sa = zk + zc, sb = zk - zc;
-        ph[r] = mk<R>(sa.x / 2, sa.y / 2);
-        qh[r] = mk<R>(sb.y / 2, -sb.x / 2);
+        ph[r] = sa;                   // 2 P^
+        qh[r] = mk<R>(sb.y, -sb.x);   // 2 Q^
     });
 }
 

@@ -26,8 +26,8 @@ namespace {
 
 // The tensor map through which the row pass of resolution N stores a tile's product spectra
 // (RowArgs::nlmap); nothing to do for resolutions that store them with plain stores.
-template <typename R, int N> cudaError_t row_store_map(RowArgs<R> &a) {
-    using G = Cfg<R, N>;
+template <typename R, int N, int RT = 128> cudaError_t row_store_map(RowArgs<R> &a) {
+    using G = Cfg<R, N, RT>;
     if constexpr (!G::ROW_TMA) {
         return cudaSuccess;
     } else {
@@ -55,7 +55,10 @@ template <typename R, int N> cudaError_t row_store_map(RowArgs<R> &a) {
 template <typename R, int N> struct L {
     using G = Cfg<R, N>;
     static constexpr size_t col_smem = hzlb::column_smem<R, N>();
-    static constexpr size_t row_smem = hzlb::row_smem<R, N>();
+    // the standalone row kernel's block shape (RT threads)
+    static constexpr int RT = row_kernel_threads<R, N>();
+    using GR = Cfg<R, N, RT>;
+    static constexpr size_t row_smem = hzlb::row_smem<R, N, RT>();
     static constexpr size_t prow_smem = sizeof(cx<R>) * (G::TWE + G::GROUPS * G::BUF);
     static constexpr size_t pcol_smem = sizeof(cx<R>) * (G::TWE + G::LPB * G::BUF);
     static_assert(row_smem <= 227 * 1024, "row kernel shared memory");
@@ -89,7 +92,7 @@ template <typename R, int N> struct L {
         }
         if (e == cudaSuccess)
             e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rb, row_kernel<R, N>,
-                                                              G::ROW_THREADS, row_smem);
+                                                              GR::ROW_THREADS, row_smem);
         if (e == cudaSuccess && (cb < 1 || rb < 1))
             e = cudaErrorInvalidConfiguration;
         if (e == cudaSuccess && dev < 64) {
@@ -116,12 +119,12 @@ template <typename R, int N> struct L {
     }
     static cudaError_t row(const RowArgs<R> &args, cudaStream_t s, int cap) {
         RowArgs<R> a = args;
-        if (cudaError_t e = row_store_map<R, N>(a))
+        if (cudaError_t e = row_store_map<R, N, RT>(a))
             return e;
-        const int items = a.members * (N / G::TY);
+        const int items = a.members * (N / GR::TY);
         const int res = resident(row_resident);
         const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
-        row_kernel<R, N><<<grid, G::ROW_THREADS, row_smem, s>>>(a, items);
+        row_kernel<R, N><<<grid, GR::ROW_THREADS, row_smem, s>>>(a, items);
         return cudaGetLastError();
     }
     static cudaError_t physical(const cx<R> *field, long long stride, cx<R> *cols, R *phys,

@@ -52,7 +52,9 @@ template <typename R> __host__ __device__ constexpr int velocity_row_stride(int 
 // E (elements per thread) keeps a line inside one warp.  16 elements (two radix-16 passes at
 // 256) beat 8 (three passes, twice the threads per line) in both precisions: measured at 256^2,
 // FP32 0.63 against 1.00 ms per column launch, FP64 252k against 221k member-steps/s.
-template <typename R, int N> struct Cfg {
+// RT: threads of a row-pass block (128 for every kernel but the standalone FP32 256^2 row
+// kernel, row_kernel_threads below).
+template <typename R, int N, int RT = 128> struct Cfg {
     static constexpr int E = N < 16 ? N : 16;
     static constexpr int T = N / E;
     static constexpr int K = (N - 1) / 3;
@@ -72,8 +74,8 @@ template <typename R, int N> struct Cfg {
     // padded FFT line buffer rounded up to whole 16-byte chunks
     static constexpr int LS = (BUF + PER16 - 1) / PER16 * PER16;
     static constexpr int ST_WORDS = 3 * ST_STRIDE > LPB * (LS + N) ? 3 * ST_STRIDE : LPB * (LS + N);
-    // row kernel: TY rows per block, one row per group of T threads, 128 threads at least
-    static constexpr int TY_RAW = 128 / T;
+    // row kernel: TY rows per block, one row per group of T threads, RT threads at least
+    static constexpr int TY_RAW = RT / T;
     static constexpr int TY = TY_RAW > N ? N : (TY_RAW < 2 ? 2 : TY_RAW);
     static constexpr int GROUPS = TY * T >= 32 ? TY : 32 / T;
     static constexpr int ROW_THREADS = GROUPS * T;
@@ -638,10 +640,10 @@ __device__ __forceinline__ void row_line(cx<R> (&z)[Cfg<R, N>::E], cx<R> *sm, co
 // The row pass over work items first, first + stride, ... < items (member x tile of TY rows),
 // with `smem_raw` as its dynamic shared memory; row_kernel runs one resolution, the mixed
 // kernels run several one after another in one launch.
-template <typename R, int N>
+template <typename R, int N, int RT = 128>
 __device__ __forceinline__ void row_pass(const RowArgs<R> &a, int items, int first, int stride,
                                          unsigned char *smem_raw) {
-    using G = Cfg<R, N>;
+    using G = Cfg<R, N, RT>;
     constexpr int E = G::E, T = G::T, C = G::C, K = G::K, TY = G::TY;
     // input tile [TY][2][CW], refilled with the next item's tile as soon as every row has read
     // its entries; FFT line buffers [GROUPS][BUF], reused once every row has finished its
@@ -774,21 +776,28 @@ __device__ __forceinline__ void row_pass(const RowArgs<R> &a, int items, int fir
             bulk_wait_all();   // this block's product stores are complete before it leaves
 }
 
-// FP32: at most 80 registers, so that 6 blocks fit an SM (95 unconstrained: 5 blocks; measured
-// 0.368 against 0.383 ms per launch at 2048 members, 256^2).
+// Threads of a standalone row-kernel block: 64 (4-row tiles, 12 blocks per SM) for FP32 at
+// 256^2, else 128 (the shape the mixed kernels share).
+template <typename R, int N> __host__ __device__ constexpr int row_kernel_threads() {
+    return sizeof(R) == 4 && N == 256 ? 64 : 128;
+}
+// FP32: at most 80 registers, so that 6 blocks of 128 (12 of 64) threads fit an SM (95
+// unconstrained: 5 blocks; measured 0.368 against 0.383 ms per launch at 2048 members, 256^2).
 template <typename R, int N>
-__global__ void __launch_bounds__(Cfg<R, N>::ROW_THREADS, sizeof(R) == 4 ? 6 : 1)
+__global__ void __launch_bounds__(Cfg<R, N, row_kernel_threads<R, N>()>::ROW_THREADS,
+                                  sizeof(R) == 4 ? (row_kernel_threads<R, N>() == 64 ? 12 : 6) : 1)
     row_kernel(const __grid_constant__ RowArgs<R> a, int items) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    row_pass<R, N>(a, items, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), smem_raw);
+    row_pass<R, N, row_kernel_threads<R, N>()>(a, items, static_cast<int>(blockIdx.x),
+                                               static_cast<int>(gridDim.x), smem_raw);
 }
 
 template <typename R, int N> constexpr size_t column_smem() {
     using G = Cfg<R, N>;
     return sizeof(cx<R>) * (2 * G::LPB * G::LS + G::ST_WORDS + G::TWE);
 }
-template <typename R, int N> constexpr size_t row_smem() {
-    using G = Cfg<R, N>;
+template <typename R, int N, int RT = 128> constexpr size_t row_smem() {
+    using G = Cfg<R, N, RT>;
     return sizeof(cx<R>) * (G::TILE + G::GROUPS * G::BUF + G::TWE);
 }
 } // namespace hzlb

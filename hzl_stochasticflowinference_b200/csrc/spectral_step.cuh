@@ -776,10 +776,10 @@ __device__ __forceinline__ void row_pass(const RowArgs<R> &a, int items, int fir
             bulk_wait_all();   // this block's product stores are complete before it leaves
 }
 
-// Threads of a standalone row-kernel block: 64 (4-row tiles, 12 blocks per SM) for FP32 at
-// 256^2, else 128 (the shape the mixed kernels share).
+// Threads of a standalone row-kernel block: 64 at 128^2 and 256^2 (FP32 256^2: 4-row tiles,
+// 12 blocks per SM; FP64 256^2: 6 blocks), else 128 (the shape the mixed kernels share).
 template <typename R, int N> __host__ __device__ constexpr int row_kernel_threads() {
-    return sizeof(R) == 4 && N == 256 ? 64 : 128;
+    return N == 256 || (sizeof(R) == 4 && N == 128) ? 64 : 128;
 }
 // FP32: at most 80 registers, so that 6 blocks of 128 (12 of 64) threads fit an SM (95
 // unconstrained: 5 blocks; measured 0.368 against 0.383 ms per launch at 2048 members, 256^2).

@@ -239,6 +239,8 @@ def library() -> C.CDLL:
         "hzlb_noise_amplitudes": (C.c_int, [C.POINTER(hzlb_config), C.c_double, C.c_uint64,
                                             C.c_uint64, C.c_int, vp, C.c_longlong, vp]),
         "hzlb_set_step_schedule": (C.c_int, [vp, C.c_int]),
+        "hzlb_mixed_row_threads": (C.c_int, [vp, C.POINTER(C.c_int)]),
+        "hzlb_mixed_set_row_threads": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "hzlb_step_schedule": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "hzlb_learned_forecast": (C.c_int, [vp, vp, vp, C.c_double, C.c_uint64, vp, C.c_int]),
         "hzlb_ensemble_mean_device": (C.c_int, [vp, vp]),
@@ -1181,9 +1183,17 @@ class Mixed:
         mode = C.c_int()
         tried = (C.c_double * 4)()
         _check(self._lib.hzlb_mixed_mode(self._h, C.byref(mode), tried))
+        threads = (C.c_int * k)()
+        _check(self._lib.hzlb_mixed_row_threads(self._h, threads))
         return dict(serial=bool(serial.value), mode=self.MODES[mode.value],
-                    column_caps=list(col), row_caps=list(row),
+                    column_caps=list(col), row_caps=list(row), row_threads=list(threads),
                     tuned_ms={m: t for m, t in zip(self.MODES, tried) if t > 0})
+
+    def set_row_threads(self, threads) -> None:
+        """Row-kernel block shape per group, 64 or 128 threads (0: the resolution's default;
+        hzlb_mixed_set_row_threads)."""
+        arr = (C.c_int * len(self.configs))(*threads)
+        _check(self._lib.hzlb_mixed_set_row_threads(self._h, arr))
 
     def set_mode(self, mode: str, column_caps=None, row_caps=None) -> None:
         """One of MODES (hzlb_mixed_set_mode); caps per group as in set_schedule."""

@@ -380,7 +380,7 @@ template <typename R> class EngineT final : public Engine {
     }
     // The eight launches of one RK4 step; the final column pass also emits the derivative
     // columns of the new state, so consecutive steps chain without a separate start pass.
-    void enqueue_step(double dt) { enqueue_steps_on(dt, 1, stream_, 0, 0); }
+    void enqueue_step(double dt) { enqueue_steps_on(dt, 1, stream_, 0, 0, 0); }
     // the OU half-step transition (ou.cuh) before (half 0) or after (half 1) a step's stages
     void enqueue_ou(double dt, int half, cudaStream_t s) {
         const double h = dt / 2;
@@ -566,7 +566,8 @@ template <typename R> class EngineT final : public Engine {
             w_valid_ = true;
         }
     }
-    void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap) override {
+    void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap,
+                          int row_threads) override {
         ColumnArgs<R> a = column_args(dt);
         RowArgs<R> r = row_args();
         for (int i = 0; i < steps; ++i) {
@@ -574,7 +575,7 @@ template <typename R> class EngineT final : public Engine {
                 enqueue_ou(dt, 0, s);
             for (int st = 1; st <= 4; ++st) {
                 r.cfl_scale = st == 1 ? dt * n_ / (2 * kPi) : 0.0;
-                cuda_check(launch_row<R>(n_, r, s, row_cap), "launch row pass");
+                cuda_check(launch_row<R>(n_, r, s, row_cap, row_threads), "launch row pass");
                 a.stage = st;
                 cuda_check(launch_column<R>(n_, a, s, col_cap), "launch column pass");
             }

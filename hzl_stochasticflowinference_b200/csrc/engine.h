@@ -144,8 +144,10 @@ class Engine {
     // validate dt and run the start pass if the velocity columns are stale (waits for it)
     virtual void prepare_steps(double dt) = 0;
     // enqueue `steps` RK4 steps on stream s, persistent grids capped at col_cap / row_cap
-    // blocks (0: every resident block); allowed during stream capture
-    virtual void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap) = 0;
+    // blocks (0: every resident block), row kernel blocks of row_threads threads (64 or 128;
+    // 0: the resolution's default); allowed during stream capture
+    virtual void enqueue_steps_on(double dt, int steps, cudaStream_t s, int col_cap, int row_cap,
+                                  int row_threads) = 0;
     // the stage kernels' arguments of this handle (ColumnArgs<R> / RowArgs<R> of its
     // precision, stage and CFL scale unset) for a caller that launches the passes itself (the
     // mixed-resolution kernels); OU forcing transitions are not part of them

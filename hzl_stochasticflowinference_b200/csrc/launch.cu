@@ -52,19 +52,53 @@ template <typename R, int N, int RT = 128> cudaError_t row_store_map(RowArgs<R> 
     }
 }
 
+// The standalone row kernel of resolution N in blocks of RT threads: shared memory, resident
+// grid per device, launch.
+template <typename R, int N, int RT> struct RowShape {
+    using GR = Cfg<R, N, RT>;
+    static constexpr size_t smem = hzlb::row_smem<R, N, RT>();
+    static_assert(smem <= 227 * 1024, "row kernel shared memory");
+    static inline int resident[64] = {};
+    static cudaError_t prepare(int dev, int sms) {
+        cudaError_t e = cudaFuncSetAttribute(row_kernel<R, N, RT>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(smem));
+        int rb = 0;
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rb, row_kernel<R, N, RT>,
+                                                              GR::ROW_THREADS, smem);
+        if (e == cudaSuccess && rb < 1)
+            e = cudaErrorInvalidConfiguration;
+        if (e == cudaSuccess && dev >= 0 && dev < 64)
+            resident[dev] = rb * sms;
+        return e;
+    }
+    static int resident_blocks() {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        return dev >= 0 && dev < 64 && resident[dev] > 0 ? resident[dev] : 148;
+    }
+    static cudaError_t run(const RowArgs<R> &args, cudaStream_t s, int cap) {
+        RowArgs<R> a = args;
+        if (cudaError_t e = row_store_map<R, N, RT>(a))
+            return e;
+        const int items = a.members * (N / GR::TY);
+        const int res = resident_blocks();
+        const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
+        row_kernel<R, N, RT><<<grid, GR::ROW_THREADS, smem, s>>>(a, items);
+        return cudaGetLastError();
+    }
+};
+
 template <typename R, int N> struct L {
     using G = Cfg<R, N>;
     static constexpr size_t col_smem = hzlb::column_smem<R, N>();
-    // the standalone row kernel's block shape (RT threads)
+    // the standalone row kernel's default block shape (RT threads)
     static constexpr int RT = row_kernel_threads<R, N>();
-    using GR = Cfg<R, N, RT>;
-    static constexpr size_t row_smem = hzlb::row_smem<R, N, RT>();
     static constexpr size_t prow_smem = sizeof(cx<R>) * (G::TWE + G::GROUPS * G::BUF);
     static constexpr size_t pcol_smem = sizeof(cx<R>) * (G::TWE + G::LPB * G::BUF);
-    static_assert(row_smem <= 227 * 1024, "row kernel shared memory");
-
-    // persistent grids: resident blocks per SM x SMs, per device
-    static inline int col_resident[64] = {}, row_resident[64] = {};
+    // persistent grid of the column pass: resident blocks per SM x SMs, per device
+    static inline int col_resident[64] = {};
     // one column kernel per RK stage
     static constexpr void (*col_kernels[5])(const ColumnArgs<R>, int) = {
         column_kernel<R, N, 0>, column_kernel<R, N, 1>, column_kernel<R, N, 2>,
@@ -74,10 +108,7 @@ template <typename R, int N> struct L {
         for (int st = 0; st < 5 && e == cudaSuccess; ++st)
             e = cudaFuncSetAttribute(col_kernels[st], cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(col_smem));
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(row_kernel<R, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(row_smem));
-        int dev = 0, sms = 0, cb = 0, rb = 0;
+        int dev = 0, sms = 0, cb = 0;
         if (e == cudaSuccess)
             e = cudaGetDevice(&dev);
         if (e == cudaSuccess)
@@ -90,15 +121,14 @@ template <typename R, int N> struct L {
                                                               col_smem);
             cb = std::min(cb, b);
         }
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rb, row_kernel<R, N>,
-                                                              GR::ROW_THREADS, row_smem);
-        if (e == cudaSuccess && (cb < 1 || rb < 1))
+        if (e == cudaSuccess && cb < 1)
             e = cudaErrorInvalidConfiguration;
-        if (e == cudaSuccess && dev < 64) {
+        if (e == cudaSuccess && dev < 64)
             col_resident[dev] = cb * sms;
-            row_resident[dev] = rb * sms;
-        }
+        if (e == cudaSuccess)
+            e = RowShape<R, N, 64>::prepare(dev, sms);
+        if (e == cudaSuccess)
+            e = RowShape<R, N, 128>::prepare(dev, sms);
         return e;
     }
     static int resident(const int *table) {
@@ -117,15 +147,15 @@ template <typename R, int N> struct L {
         col_kernels[a.stage]<<<grid, G::COL_THREADS, col_smem, s>>>(a, items);
         return cudaGetLastError();
     }
-    static cudaError_t row(const RowArgs<R> &args, cudaStream_t s, int cap) {
-        RowArgs<R> a = args;
-        if (cudaError_t e = row_store_map<R, N, RT>(a))
-            return e;
-        const int items = a.members * (N / GR::TY);
-        const int res = resident(row_resident);
-        const int grid = std::min(items, cap > 0 ? std::min(cap, res) : res);
-        row_kernel<R, N><<<grid, GR::ROW_THREADS, row_smem, s>>>(a, items);
-        return cudaGetLastError();
+    // threads: 64 or 128 (0: the default shape)
+    static int row_threads(int threads) { return threads == 64 || threads == 128 ? threads : RT; }
+    static cudaError_t row(const RowArgs<R> &args, cudaStream_t s, int cap, int threads) {
+        return row_threads(threads) == 64 ? RowShape<R, N, 64>::run(args, s, cap)
+                                          : RowShape<R, N, 128>::run(args, s, cap);
+    }
+    static int row_resident(int threads) {
+        return row_threads(threads) == 64 ? RowShape<R, N, 64>::resident_blocks()
+                                          : RowShape<R, N, 128>::resident_blocks();
     }
     static cudaError_t physical(const cx<R> *field, long long stride, cx<R> *cols, R *phys,
                                 const cx<R> *tw, int members, cudaStream_t s) {
@@ -155,7 +185,7 @@ template <typename R, int N> struct L {
         k.col_blocks_per_member = (G::C + G::LPB - 1) / G::LPB;
         k.row_blocks_per_member = N / G::TY;
         k.col_smem = col_smem;
-        k.row_smem = row_smem;
+        k.row_smem = hzlb::row_smem<R, N>();
         k.elements_per_thread = G::E;
         k.rows_per_block = G::TY;
     }
@@ -183,14 +213,20 @@ template <typename R, int N> struct DoColumn {
     }
 };
 template <typename R, int N> struct DoRow {
-    static cudaError_t run(const RowArgs<R> &a, cudaStream_t s, int cap) {
-        return L<R, N>::row(a, s, cap);
+    static cudaError_t run(const RowArgs<R> &a, cudaStream_t s, int cap, int threads) {
+        return L<R, N>::row(a, s, cap, threads);
     }
 };
 template <typename R, int N> struct DoResident {
-    static cudaError_t run(int *c, int *r) {
+    static cudaError_t run(int *c, int *r, int threads) {
         *c = L<R, N>::resident(L<R, N>::col_resident);
-        *r = L<R, N>::resident(L<R, N>::row_resident);
+        *r = L<R, N>::row_resident(threads);
+        return cudaSuccess;
+    }
+};
+template <typename R, int N> struct DoRowShape {
+    static cudaError_t run(int threads, int *out) {
+        *out = L<R, N>::row_threads(threads);
         return cudaSuccess;
     }
 };
@@ -225,11 +261,16 @@ template <typename R>
 cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s, int cap) {
     return dispatch<R, DoColumn>(n, a, s, cap);
 }
-template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s, int cap) {
-    return dispatch<R, DoRow>(n, a, s, cap);
+template <typename R>
+cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s, int cap, int threads) {
+    return dispatch<R, DoRow>(n, a, s, cap, threads);
 }
-template <typename R> cudaError_t resident_blocks(int n, int *column, int *row) {
-    return dispatch<R, DoResident>(n, column, row);
+template <typename R> cudaError_t resident_blocks(int n, int *column, int *row, int threads) {
+    return dispatch<R, DoResident>(n, column, row, threads);
+}
+template <typename R> int row_block_threads(int n, int threads) {
+    int out = 0;
+    return dispatch<R, DoRowShape>(n, threads, &out) == cudaSuccess ? out : 0;
 }
 template <typename R>
 cudaError_t launch_physical(int n, const cx<R> *field, long long stride, cx<R> *cols, R *phys,
@@ -282,8 +323,9 @@ template <typename R> KernelShape kernel_shape(int n) {
 #define HZLB_INSTANTIATE(R)                                                                        \
     template cudaError_t prepare_kernels<R>(int);                                                  \
     template cudaError_t launch_column<R>(int, const ColumnArgs<R> &, cudaStream_t, int);          \
-    template cudaError_t launch_row<R>(int, const RowArgs<R> &, cudaStream_t, int);                \
-    template cudaError_t resident_blocks<R>(int, int *, int *);                                    \
+    template cudaError_t launch_row<R>(int, const RowArgs<R> &, cudaStream_t, int, int);           \
+    template cudaError_t resident_blocks<R>(int, int *, int *, int);                               \
+    template int row_block_threads<R>(int, int);                                                   \
     template cudaError_t launch_physical<R>(int, const cx<R> *, long long, cx<R> *, R *,          \
                                             const cx<R> *, int, cudaStream_t);                     \
     template cudaError_t launch_velocity_max<R>(int, const cx<R> *, unsigned long long *,         \

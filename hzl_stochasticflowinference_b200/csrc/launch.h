@@ -38,9 +38,15 @@ template <typename R> cudaError_t prepare_kernels(int n);
 // cap > 0 limits the persistent grid to cap blocks (default: all resident blocks of the device)
 template <typename R>
 cudaError_t launch_column(int n, const ColumnArgs<R> &a, cudaStream_t s, int cap = 0);
-template <typename R> cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s, int cap = 0);
-// resident blocks of the column and row kernels on the current device (after prepare_kernels)
-template <typename R> cudaError_t resident_blocks(int n, int *column, int *row);
+// threads: the row kernel's block shape, 64 or 128 (0: the resolution's default,
+// row_kernel_threads); both are compiled for every resolution
+template <typename R>
+cudaError_t launch_row(int n, const RowArgs<R> &a, cudaStream_t s, int cap = 0, int threads = 0);
+// resident blocks of the column kernel and of the row kernel of that shape on the current
+// device (after prepare_kernels)
+template <typename R> cudaError_t resident_blocks(int n, int *column, int *row, int threads = 0);
+// the block shape `threads` resolves to at resolution n (64 or 128)
+template <typename R> int row_block_threads(int n, int threads);
 template <typename R>
 cudaError_t launch_physical(int n, const cx<R> *field, long long stride, cx<R> *cols, R *phys,
                             const cx<R> *tw, int members, cudaStream_t s);

@@ -9,7 +9,8 @@
 // The autotuner (hzlb_mixed_tune) measures the batch step time of candidate schedules on the
 // actual ensembles — the serial schedule, and the concurrent schedule with each resolution's
 // grid cap chosen by coordinate descent over fractions of its resident block count (largest
-// work first, two passes) — and keeps the fastest.  Each candidate is captured as a graph and
+// work first, two passes) and then each resolution's row-kernel block shape (64 or 128
+// threads) — and keeps the fastest.  Each candidate is captured as a graph and
 // timed with CUDA events after a warm-up launch.  The ensembles' states and clocks are saved
 // on the device before tuning and restored after it, so tuning leaves them as they were.
 //
@@ -28,6 +29,7 @@ namespace hzlb {
 
 struct GroupCaps {
     int col = 0, row = 0;   // 0: every resident block
+    int row_threads = 0;    // row kernel block shape, 64 or 128 threads (0: the default)
 };
 
 // How a batch's steps are laid out in its graph: each resolution's own kernels one after
@@ -146,6 +148,23 @@ class Mixed {
                         best = trial;
                     }
                 }
+        // the row kernel's block shape per resolution, 64 or 128 threads (both compiled), the
+        // grid cap carried over as the same fraction of that shape's resident blocks
+        for (int g : order) {
+            std::vector<GroupCaps> trial = best;
+            const int cur = row_threads(g, best[g].row_threads), alt = cur == 64 ? 128 : 64;
+            trial[g].row_threads = alt;
+            if (best[g].row > 0)
+                trial[g].row = std::max(1, static_cast<int>(std::lround(
+                                               static_cast<double>(best[g].row) *
+                                               row_resident(g, alt) / row_resident(g, cur))));
+            set_schedule(false, trial);
+            const double ms = measure(dt, repeats);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = trial;
+            }
+        }
         // the fused kernels over the mixed work list, and with the 512^2 resolution on a branch
         // whose grid cap is searched too
         Mode best_mode = Mode::Concurrent;
@@ -227,6 +246,32 @@ class Mixed {
                 row_caps[g] = caps_[g].row ? caps_[g].row : resident_[g].row;
         }
     }
+    // the row kernel block shape group g runs with `threads` (0: its default) resolves to
+    int row_threads(int g, int threads) const {
+        const hzlb_config &c = groups_[g]->engine->config();
+        return c.precision == 4 ? row_block_threads<float>(c.n, threads)
+                                : row_block_threads<double>(c.n, threads);
+    }
+    int row_threads(int g) const { return row_threads(g, caps_[g].row_threads); }
+    void set_row_threads(const int *threads) {
+        if (!threads)
+            raise(HZLB_EINVAL, "null row block shapes");
+        for (int g = 0; g < count(); ++g)
+            if (threads[g] != 0 && threads[g] != 64 && threads[g] != 128)
+                raise(HZLB_EINVAL, "row block shape must be 0 (default), 64 or 128 threads");
+        for (int g = 0; g < count(); ++g)
+            caps_[g].row_threads = threads[g];
+        drop();
+    }
+    // resident blocks of group g's row kernel in blocks of `threads`
+    int row_resident(int g, int threads) const {
+        const hzlb_config &c = groups_[g]->engine->config();
+        int col = 0, row = 0;
+        cuda_check(c.precision == 4 ? resident_blocks<float>(c.n, &col, &row, threads)
+                                    : resident_blocks<double>(c.n, &col, &row, threads),
+                   "query resident blocks");
+        return row > 0 ? row : 1;
+    }
     void set_schedule(bool serial, const std::vector<GroupCaps> &caps) {
         set_mode(serial ? Mode::Serial : Mode::Concurrent, caps);
     }
@@ -298,19 +343,20 @@ class Mixed {
                 cuda_check(cudaEventRecord(fork_, main_), "fork");
                 cuda_check(cudaStreamWaitEvent(branch_[g5], fork_, 0), "branch wait");
                 groups_[g5]->engine->enqueue_steps_on(dt[g5], steps, branch_[g5], caps_[g5].col,
-                                                      caps_[g5].row);
+                                                      caps_[g5].row, caps_[g5].row_threads);
                 cuda_check(cudaEventRecord(join_[g5], branch_[g5]), "join record");
                 enqueue_fused(dt, steps, main_, g5);
                 cuda_check(cudaStreamWaitEvent(main_, join_[g5], 0), "join wait");
             } else if (serial_) {
                 for (int g = 0; g < count(); ++g)
-                    groups_[g]->engine->enqueue_steps_on(dt[g], steps, main_, 0, 0);
+                    groups_[g]->engine->enqueue_steps_on(dt[g], steps, main_, 0, 0,
+                                                         caps_[g].row_threads);
             } else {
                 cuda_check(cudaEventRecord(fork_, main_), "fork");
                 for (int g = 0; g < count(); ++g) {
                     cuda_check(cudaStreamWaitEvent(branch_[g], fork_, 0), "branch wait");
                     groups_[g]->engine->enqueue_steps_on(dt[g], steps, branch_[g], caps_[g].col,
-                                                         caps_[g].row);
+                                                         caps_[g].row, caps_[g].row_threads);
                     cuda_check(cudaEventRecord(join_[g], branch_[g]), "join record");
                     cuda_check(cudaStreamWaitEvent(main_, join_[g], 0), "join wait");
                 }
@@ -507,6 +553,18 @@ HZLB_API int hzlb_mixed_set_mode(hzlb_mixed *h, int mode, const int *col_caps,
         }
         m.set_mode(static_cast<hzlb::Mode>(mode), caps);
     });
+}
+HZLB_API int hzlb_mixed_row_threads(hzlb_mixed *h, int *threads) {
+    return guarded_mixed([&] {
+        auto &m = mixed(h);
+        if (!threads)
+            hzlb::raise(HZLB_EINVAL, "null output");
+        for (int g = 0; g < m.count(); ++g)
+            threads[g] = m.row_threads(g);
+    });
+}
+HZLB_API int hzlb_mixed_set_row_threads(hzlb_mixed *h, const int *threads) {
+    return guarded_mixed([&] { mixed(h).set_row_threads(threads); });
 }
 HZLB_API int hzlb_mixed_mode(hzlb_mixed *h, int *mode, double *tuned_ms) {
     return guarded_mixed([&] {

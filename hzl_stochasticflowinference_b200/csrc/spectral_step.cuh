@@ -783,13 +783,13 @@ template <typename R, int N> __host__ __device__ constexpr int row_kernel_thread
 }
 // FP32: at most 80 registers, so that 6 blocks of 128 (12 of 64) threads fit an SM (95
 // unconstrained: 5 blocks; measured 0.368 against 0.383 ms per launch at 2048 members, 256^2).
-template <typename R, int N>
-__global__ void __launch_bounds__(Cfg<R, N, row_kernel_threads<R, N>()>::ROW_THREADS,
-                                  sizeof(R) == 4 ? (row_kernel_threads<R, N>() == 64 ? 12 : 6) : 1)
+// RT: the block shape (64 or 128 threads); both are compiled for every resolution, the
+// default is row_kernel_threads and a mixed batch's tuner may choose the other.
+template <typename R, int N, int RT>
+__global__ void __launch_bounds__(Cfg<R, N, RT>::ROW_THREADS, sizeof(R) == 4 ? (RT == 64 ? 12 : 6) : 1)
     row_kernel(const __grid_constant__ RowArgs<R> a, int items) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    row_pass<R, N, row_kernel_threads<R, N>()>(a, items, static_cast<int>(blockIdx.x),
-                                               static_cast<int>(gridDim.x), smem_raw);
+    row_pass<R, N, RT>(a, items, static_cast<int>(blockIdx.x), static_cast<int>(gridDim.x), smem_raw);
 }
 
 template <typename R, int N> constexpr size_t column_smem() {

@@ -629,6 +629,14 @@ HZLB_API int hzlb_mixed_set_schedule(hzlb_mixed *h, int serial, const int *col_c
  * measured; may be NULL). */
 HZLB_API int hzlb_mixed_set_mode(hzlb_mixed *h, int mode, const int *col_caps, const int *row_caps);
 HZLB_API int hzlb_mixed_mode(hzlb_mixed *h, int *mode, double *tuned_ms);
+/* Row-kernel block shape per group in the serial and concurrent modes (and the 512^2 branch of
+ * mode 3): 64 or 128 threads, both compiled for every resolution (a block of 64 holds half the
+ * rows of one of 128).  hzlb_mixed_row_threads reports the shapes in effect (one int per group);
+ * set_row_threads sets them (0: the resolution's default); hzlb_mixed_tune chooses them after
+ * the grid caps; set_mode and set_schedule return them to the defaults.  The shape changes no
+ * result bit. */
+HZLB_API int hzlb_mixed_row_threads(hzlb_mixed *h, int *threads);
+HZLB_API int hzlb_mixed_set_row_threads(hzlb_mixed *h, const int *threads);
 
 /* ---- seeded synthetic inputs (no counterpart in the reference, which has only built-in
  * analytic initial fields, solver.cpp:145-161) -------------------------------------- */

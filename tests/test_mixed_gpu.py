@@ -115,3 +115,32 @@ def test_fused_modes_are_refused_where_they_do_not_apply(hzlb):
     with pytest.raises(hzlb.HzlbInvalidArgument):
         m.set_mode("fused_branch")
     m.close()
+
+
+@pytest.mark.parametrize("serial,threads", [(False, [64, 64, 64]), (False, [128, 128, 128]),
+                                            (True, [64, 128, 0])])
+def test_row_block_shapes_match_separate_stepping(hzlb, serial, threads):
+    """hzlb_mixed_set_row_threads: the row kernel in blocks of 64 or 128 threads (both compiled
+    for every resolution) gives the same bits as each resolution stepped alone; the shapes in
+    effect are reported, 0 resolving to the resolution's default."""
+    cfgs = _configs(hzlb) + [hzlb.Config(n=256, members=3, precision=4, nu=2.5e-4, seed=6,
+                                         forcing_kmax=0),
+                             hzlb.Config(n=512, members=2, precision=4, nu=1.25e-4, seed=7,
+                                         forcing_kmax=0)]
+    dts = [1e-3, 5e-4, 2e-3, 2.5e-4, 1.25e-4]
+    threads = threads + [threads[0], threads[1]]
+    m = hzlb.Mixed(cfgs)
+    for k, (g, c) in enumerate(zip(m.groups, cfgs)):
+        _init(hzlb, g, c, k)
+    m.set_schedule(serial)
+    m.set_row_threads(threads)
+    shapes = m.schedule()["row_threads"]
+    assert all(s in (64, 128) for s in shapes)
+    assert all(s == t for s, t in zip(shapes, threads) if t)
+    m.step(dts, 9)
+    got = [g.get_state_compact() for g in m.groups]
+    for k, ref in enumerate(_alone(hzlb, cfgs, dts, [9] * 5)):
+        np.testing.assert_array_equal(got[k], ref)
+    with pytest.raises(hzlb.HzlbError):
+        m.set_row_threads([96, 0, 0, 0, 0])
+    m.close()
